@@ -1,0 +1,122 @@
+"""ctypes front end of the oracle (TEST INFRASTRUCTURE ONLY).
+
+Loads ``oracle/liboracle.so`` (this repository's C restatement of the
+reference time step, mhd_oracle.c) and runs the host-compiled reference
+binaries in ``oracle/_ref`` (built by ``make -C oracle ref`` where the
+reference sources are present).  Only tests/, ``__graft_entry__.smoke()`` and
+bench.py's CPU-baseline leg use this module, as the checker or the timed CPU
+baseline.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+REF_DIR = os.path.join(HERE, "_ref")
+
+_lib = None
+
+
+def build():
+    """Compile liboracle.so (gcc only; works on any box with this image)."""
+    subprocess.run(["make", "-s", "-C", HERE, "oracle"], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = ctypes.CDLL(LIB_PATH)
+        f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+        f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+        for suf, rp in (("f32", f32p), ("f64", f64p)):
+            fn = getattr(L, "oracle_proceed_" + suf)
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_void_p, rp, ctypes.POINTER(ctypes.c_double),
+                           ctypes.POINTER(ctypes.c_int64), ctypes.c_double, ctypes.c_int,
+                           ctypes.c_void_p, ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+            fn = getattr(L, "oracle_shear_fill_" + suf)
+            fn.restype = None
+            fn.argtypes = [ctypes.c_void_p, rp, ctypes.c_double]
+        L.oracle_hlld_f32.restype = None
+        L.oracle_hlld_f32.argtypes = [ctypes.c_float, ctypes.c_float, f32p, f32p]
+        L.oracle_hlld_f64.restype = None
+        L.oracle_hlld_f64.argtypes = [ctypes.c_double, ctypes.c_double, f64p, f64p]
+        L.oracle_cfl_f32.restype = ctypes.c_float
+        L.oracle_cfl_f32.argtypes = [ctypes.c_void_p, f32p, ctypes.c_float]
+        L.oracle_cfl_f64.restype = ctypes.c_double
+        L.oracle_cfl_f64.argtypes = [ctypes.c_void_p, f64p, ctypes.c_double]
+        _lib = L
+    return _lib
+
+
+def proceed(cfg, state, steps, goal_time=1.0e30, time=0.0, generation=0, dtype=np.float32):
+    """Advance ``state`` (8, Sz, Sy, Sx) by ``steps`` steps; returns a dict with
+    the new state, times (steps+1), dts, time, generation, goal_reached."""
+    suf = "f32" if dtype == np.float32 else "f64"
+    st = np.ascontiguousarray(state, dtype=dtype).copy()
+    c = cfg.to_ctypes()
+    t = ctypes.c_double(time)
+    g = ctypes.c_int64(generation)
+    times = np.zeros(steps + 1, np.float64)
+    dts = np.zeros(max(steps, 1), dtype)
+    reached = ctypes.c_int(0)
+    n = getattr(lib(), "oracle_proceed_" + suf)(
+        ctypes.byref(c), st, ctypes.byref(t), ctypes.byref(g), goal_time, steps,
+        times.ctypes.data, dts.ctypes.data, ctypes.byref(reached))
+    return {"state": st, "steps": n, "times": times[:n + 1], "dts": dts[:n], "time": t.value,
+            "generation": g.value, "goal_reached": bool(reached.value)}
+
+
+def hlld(gamma, bx, lr, dtype=np.float32):
+    suf = "f32" if dtype == np.float32 else "f64"
+    out = np.zeros(7, dtype)
+    getattr(lib(), "oracle_hlld_" + suf)(gamma, bx, np.ascontiguousarray(lr, dtype), out)
+    return out
+
+
+def cfl(cfg, state, goal=1.0e30):
+    c = cfg.to_ctypes()
+    return float(lib().oracle_cfl_f32(ctypes.byref(c), np.ascontiguousarray(state, np.float32), goal))
+
+
+def shear_fill(cfg, state, time, dtype=np.float32):
+    suf = "f32" if dtype == np.float32 else "f64"
+    st = np.ascontiguousarray(state, dtype=dtype).copy()
+    c = cfg.to_ctypes()
+    getattr(lib(), "oracle_shear_fill_" + suf)(ctypes.byref(c), st, time)
+    return st
+
+
+def ref_binary(name):
+    """Path of a host-compiled reference binary, or None when not built."""
+    p = os.path.join(REF_DIR, "ref_" + name)
+    return p if os.path.exists(p) else None
+
+
+def run_ref(name, state, steps, goal_time=1.0e30, threads=None, dtype=np.float32):
+    """Run the reference binary ``name`` on ``state``; returns (state, times, info)."""
+    from nmhd_b200.binio import read_bin, write_bin
+    exe = ref_binary(name)
+    if exe is None:
+        raise FileNotFoundError(f"reference binary ref_{name} is not built")
+    env = dict(os.environ)
+    if threads:
+        env["OMP_NUM_THREADS"] = str(threads)
+    with tempfile.TemporaryDirectory() as d:
+        fin, fout, ftimes = (os.path.join(d, x) for x in ("in.bin", "out.bin", "t.txt"))
+        write_bin(fin, state, dtype=dtype)
+        r = subprocess.run([exe, fin, fout, str(steps), repr(float(goal_time)), ftimes],
+                           check=True, capture_output=True, text=True, env=env)
+        info = json.loads(r.stdout.strip().splitlines()[-1])
+        out = read_bin(fout, dtype=dtype)
+        times = np.loadtxt(ftimes, ndmin=1)
+    return out, times, info

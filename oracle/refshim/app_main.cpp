@@ -1,0 +1,65 @@
+// Driver for the host-compiled reference solver (test infrastructure only).
+// Appended after the reference's src/library/mhd_solver.inl by oracle/Makefile.
+//
+//   <binary> IN.bin OUT.bin NSTEPS [GOAL_TIME] [TIMES.txt]
+//
+// Reads the initial primitive state with MHDSolver::read, advances exactly
+// NSTEPS steps with MHDSolver::proceed (monitor() stops the loop, as in
+// src/library/mhd_solver.inlrb:859-860), writes the state with
+// MHDSolver::write, and prints one JSON line with the wallclock of the proceed()
+// call.  TIMES.txt receives current_time() before every step and after the
+// last, as %.17g.
+#include <sys/time.h>
+#include <omp.h>
+
+static int g_max_steps = 0;
+static std::vector<double> g_times;
+
+void MHDSolver::dump(std::string) {}
+int MHDSolver::monitor() {
+  g_times.push_back(current_time());
+  return generation() >= g_max_steps;
+}
+int MHDSolver::initial_event() { return 0; }
+int MHDSolver::final_event() { return 0; }
+
+static double nmhd_now() {
+  timeval tv;
+  gettimeofday(&tv, 0);
+  return tv.tv_sec + 1e-6 * tv.tv_usec;
+}
+
+int main(int argc, char **argv) {
+  if (argc < 4) {
+    std::fprintf(stderr, "usage: %s IN.bin OUT.bin NSTEPS [GOAL_TIME] [TIMES.txt]\n", argv[0]);
+    return 2;
+  }
+  g_max_steps = std::atoi(argv[3]);
+  double goal = argc > 4 ? std::atof(argv[4]) : 1.0e30;
+  MHDSolver solver;
+  if (!solver.read(argv[1])) {
+    std::fprintf(stderr, "cannot read %s (missing or size mismatch)\n", argv[1]);
+    return 1;
+  }
+  // The reference prints "t dt" to stderr every step; silence it for timing.
+  std::cerr.setstate(std::ios_base::failbit);
+  double t0 = nmhd_now();
+  bool reached = solver.proceed(Real(goal));
+  double t1 = nmhd_now();
+  std::cerr.clear();
+  if (!solver.write(argv[2])) {
+    std::fprintf(stderr, "cannot write %s\n", argv[2]);
+    return 1;
+  }
+  if (argc > 5) {
+    FILE *fp = std::fopen(argv[5], "w");
+    for (size_t i = 0; i < g_times.size(); ++i) std::fprintf(fp, "%.17g\n", g_times[i]);
+    std::fclose(fp);
+  }
+  std::printf(
+      "{\"steps\": %d, \"cells\": %zu, \"seconds\": %.6f, \"threads\": %d, \"goal_reached\": %d, "
+      "\"time\": %.17g, \"sizeof_real\": %d}\n",
+      solver.generation(), (size_t)kSize, t1 - t0, omp_get_max_threads(), reached ? 1 : 0,
+      solver.current_time(), (int)sizeof(Real));
+  return 0;
+}
