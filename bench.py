@@ -1,0 +1,300 @@
+"""Benchmark: Mcell-updates/s of the ideal-MHD time step on B200.
+
+Workload (default): the MRI shearing box, 128 (radial) x 256 (azimuthal) x 64
+cells, FP32, gamma 5/3, CFL 0.4, q 1.5, Omega 1, beta 400, seeded velocity
+noise (seed 1); reference axes X azimuthal, Y radial (+2x4 shearing margins),
+Z vertical.  A "step" is one RK2 time step of the whole box (two stages,
+margin fill, CFL reduction).  Metric: interior cells x steps / second
+(the reference's "mesh updates per sec",
+src/application/optimize_mhd/main_detail.curb:39-44, counted over interior
+cells).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nmhd|reference]
+
+N > 1 runs under torch.distributed (one rank per GPU): independent replicas of
+the box, one per GPU (the time step has no data-parallel exchange on one box;
+"scaling": "weak").  Rank 0 prints one JSON line.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOADS = {
+    "mri_shearing_box_128x256x64": dict(n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0,
+                                        l_azimuthal=4.0, l_vertical=1.0, seed=1),
+    "mri_shearing_box_512x1024x256": dict(n_radial=512, n_azimuthal=1024, n_vertical=256,
+                                          l_radial=1.0, l_azimuthal=4.0, l_vertical=1.0, seed=3),
+}
+REF_BINARY = {"mri_shearing_box_128x256x64": "shear256x128x64"}
+BYTES_PER_CELL_UPDATE = 160  # 8 FP32 state words: stage 1 read+write, stage 2 2x read + write
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons while running."""
+
+    Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        if shutil.which("nvidia-smi"):
+            self.out = tempfile.TemporaryFile(mode="w+")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.out:
+            return None
+        self.out.seek(0)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.out:
+            f = [t.strip() for t in line.split(",")]
+            if len(f) < 7:
+                continue
+            try:
+                sm.append(float(f[0]))
+                mx = float(f[1])
+            except ValueError:
+                continue
+            for name, val in zip(names, f[3:7]):
+                if val.lower() == "active":
+                    reasons.add(name)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def cpu_reference_run(workload, steps, threads=None):
+    """Run the host-compiled reference solver (oracle/_ref) on the workload;
+    returns (interior cell-updates/s, steps, seconds, threads, kind)."""
+    from nmhd_b200.problems import shearing_box
+    from oracle import oracle
+    cfg, state = shearing_box(**WORKLOADS[workload])
+    name = REF_BINARY.get(workload)
+    threads = threads or os.cpu_count()
+    if name and oracle.ref_binary(name):
+        _, _, info = oracle.run_ref(name, state, steps, threads=threads)
+        secs = info["seconds"]
+        kind = "reference"
+    else:
+        os.environ["OMP_NUM_THREADS"] = str(threads)
+        t0 = time.perf_counter()
+        oracle.proceed(cfg, state, steps)
+        secs = time.perf_counter() - t0
+        kind = "port"
+    return cfg.interior_cells * steps / secs, steps, secs, threads, kind
+
+
+def cpu_sample(workload, budget_s=12.0):
+    """Bounded CPU sample: calibrate with one step, then run ~budget_s seconds."""
+    rate, _, secs, threads, kind = cpu_reference_run(workload, 1)
+    steps = max(1, min(200, int(budget_s / max(secs, 1e-3))))
+    rate, steps, secs, threads, kind = cpu_reference_run(workload, steps)
+    return {"value": rate / 1e6, "unit": "Mcell-updates/s", "cores": threads, "kind": kind,
+            "sample": f"{steps} full RK2 steps of {workload} ({secs:.1f} s, OpenMP {threads} threads)"}
+
+
+def dist_setup(n_gpus):
+    import torch
+    import torch.distributed as dist
+    if n_gpus > 1 or "RANK" in os.environ:
+        os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+        rank = int(os.environ.get("RANK", 0))
+        world = int(os.environ.get("WORLD_SIZE", 1))
+        local = int(os.environ.get("LOCAL_RANK", rank))
+        if torch.cuda.is_available():
+            torch.cuda.set_device(local)
+        from datetime import timedelta
+        dist.init_process_group("nccl" if torch.cuda.is_available() else "gloo",
+                                timeout=timedelta(seconds=120))
+        return rank, world, local, dist
+    return 0, 1, 0, None
+
+
+def run_reference_arm(args):
+    rank, world, _, dist = dist_setup(args.gpus)
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+    wl = args.workload
+    cpu_reference_run(wl, max(1, min(args.warmup, 2)))
+    # bounded: at most ~90 s of timed CPU work
+    _, _, secs1, _, _ = cpu_reference_run(wl, 1)
+    steps = max(1, min(args.steps, int(90.0 / max(secs1, 1e-3))))
+    rate, steps, secs, threads, kind = cpu_reference_run(wl, steps)
+    v = rate / 1e6
+    line = {"metric": "Mcell-updates/s", "value": v, "unit": "Mcell-updates/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * secs / steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing-box noise)",
+            "config": {"workload": wl, "parallelism": "replicas"},
+            "cpu_baseline": {"value": v, "unit": "Mcell-updates/s", "cores": threads, "kind": kind,
+                             "sample": f"{steps} full RK2 steps ({secs:.1f} s)"},
+            "e2e": {"value": v, "unit": "Mcell-updates/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def run_gpu_arm(args):
+    import torch
+    from nmhd_b200.problems import shearing_box
+    from nmhd_b200.solver import MHDSolver
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    wl = args.workload
+    cfg, state = shearing_box(**WORKLOADS[wl])
+    stream = torch.cuda.Stream(device=dev)
+    sol = MHDSolver(cfg)
+    sol.set_stream(stream.cuda_stream)
+    sol.set_state(state)
+    sol.step(args.warmup)
+    torch.cuda.synchronize(dev)
+
+    def barrier():
+        if dist:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # -- device-timed steps, state resident in HBM ---------------------------
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev.index) as clocks:
+        start.record(stream)
+        sol.step(args.steps)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    barrier()
+    ms = max_over_ranks(start.elapsed_time(end))
+    ms_per_step = ms / args.steps
+    cells = cfg.interior_cells
+    value = world * cells * args.steps / (ms * 1e-3) / 1e6
+
+    # -- per-kernel times (CUDA events around each launch, same stream) -------
+    prof = sol.profile(max(3, min(20, args.steps)))
+    kernel_ms_step = sum(t * k for t, k in prof.values())
+
+    # -- end to end through the C ABI with pinned host buffers ---------------
+    host_in = torch.empty((8,) + cfg.shape, dtype=torch.float32, pin_memory=True).numpy()
+    host_in[...] = state
+    host_out = torch.empty((8,) + cfg.shape, dtype=torch.float32, pin_memory=True).numpy()
+    e2e_steps = args.steps
+    barrier()
+    torch.cuda.synchronize(dev)
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sol.set_state(host_in)
+    sol.step(e2e_steps)
+    sol.get_state(host_out)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
+    state_bytes = 8 * 4 * cfg.cells
+    e2e = {"value": world * cells * e2e_steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+           "h2d_bytes_per_step": state_bytes / e2e_steps, "d2h_bytes_per_step": state_bytes / e2e_steps,
+           "note": "set_state(pinned host) + proceed(K steps) + get_state(pinned host), per step"}
+
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        # the RK2 step is the unit: 160 algorithmic bytes per cell-update
+        achieved = BYTES_PER_CELL_UPDATE * cells / (kernel_ms_step * 1e-3) / 1e9
+        traffic = None
+        tf = os.path.join(ROOT, "profiles", "traffic_" + wl + ".json")
+        if os.path.exists(tf):
+            traffic = json.load(open(tf)).get("dram_bytes_per_step")
+        launches_per_step = sum(k for _, k in prof.values())
+        line = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing-box noise)",
+            "config": {"workload": wl, "cells_interior": cells, "cells_with_margins": cfg.cells,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set per step (state x3 + fluxes) > 126 MB L2"},
+            "e2e": e2e,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "peak_kind": peak_kind,
+                         "unit_of_work": "one RK2 step (all kernels); 160 B per cell-update",
+                         "kernels_ms_per_step": {k: round(t * n, 5) for k, (t, n) in prof.items()}},
+            "gpu_launches": int(round(launches_per_step * args.steps)),
+            "clocks": clocks.summary(),
+        }
+        if world == 1 and not args.no_cpu:
+            line["cpu_baseline"] = cpu_sample(wl)
+        print(json.dumps(line), flush=True)
+    sol.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=400)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="nmhd", choices=["nmhd", "reference"])
+    ap.add_argument("--workload", default="mri_shearing_box_128x256x64", choices=sorted(WORKLOADS))
+    ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    args = ap.parse_args()
+    args.warmup = max(args.warmup, 3)
+    if args.impl == "reference":
+        run_reference_arm(args)
+    else:
+        run_gpu_arm(args)
+
+
+if __name__ == "__main__":
+    main()

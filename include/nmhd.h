@@ -1,0 +1,146 @@
+/* nmhd.h - C ABI of the B200-native ideal-MHD time step (libnmhd.so).
+ *
+ * Drop-in boundary for the reference's solver interface, class MHDSolver
+ * (src/library/mhd_solver.hrb:150-276; generated src/library/mhd_solver.h:514-640).
+ * Each entry point names the reference member it replaces.  Plain C types only:
+ * sizes, pointers, status codes; no exceptions cross this boundary.
+ *
+ * Conventions
+ *  - State is the reference's primitive state: 8 float32 fields of
+ *    Sx*Sy*Sz values, x fastest, in the order of its .bin dump
+ *    (density, vx, vy, vz, pressure, Bx, By, Bz).  B component d at index
+ *    (x,y,z) is the field on the lower d-face of cell (x,y,z).
+ *  - Sizes include margins (the reference's kSize{X,Y,Z}); every cell,
+ *    margins included, is advanced, as in the reference.
+ *  - The library owns device memory; the caller owns host buffers.
+ *  - Calls are synchronous with respect to the host unless stated; a handle
+ *    is not thread-safe.
+ *  - Every call returns nmhd_status; nmhd_last_error() describes the last
+ *    failure of a handle.
+ */
+#ifndef NMHD_H
+#define NMHD_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum nmhd_status {
+  NMHD_OK = 0,
+  NMHD_GOAL_REACHED = 1,        /* proceed(): goal time reached (reference returns true) */
+  NMHD_TIMEOUT = 2,             /* proceed(): wallclock limit hit (reference returns false) */
+  NMHD_STEP_LIMIT = 3,          /* proceed(): max_steps done before the goal */
+  NMHD_ERR_INVALID_ARGUMENT = -1,
+  NMHD_ERR_CUDA = -2,
+  NMHD_ERR_IO = -3,             /* file cannot be opened, read or written */
+  NMHD_ERR_SIZE_MISMATCH = -4,  /* .bin sizes differ from the solver's */
+  NMHD_ERR_NUMERICAL = -5,      /* non-finite state, density <= 0 or pressure <= 0 */
+  NMHD_ERR_OUT_OF_MEMORY = -6,
+  NMHD_ERR_NOT_SUPPORTED = -7
+} nmhd_status;
+
+typedef enum nmhd_problem {
+  NMHD_PROBLEM_NONE = 0,         /* no external acceleration */
+  NMHD_PROBLEM_SHEARING_BOX = 1  /* Coriolis + tidal acceleration, shearing-periodic Y margins */
+} nmhd_problem;
+
+/* Runtime form of the reference's compile-time simulation_config.h
+ * (src/library/simulation_config_default.h, application overrides). */
+typedef struct nmhd_config {
+  int32_t size_x, size_y, size_z; /* kSize{X,Y,Z}: cells including margins */
+  int32_t margin_y, margin_z;     /* kMarginSize{Y,Z}; X has no margin */
+  float extent_x, extent_y, extent_z; /* kGlobalExtent{X,Y,Z} of the interior */
+  float gamma;                    /* kGamma */
+  float cfl;                      /* kCflFactor */
+  int32_t problem;                /* nmhd_problem */
+  float q, omega;                 /* kDifferentialRotationIndex, kOmega (shearing box) */
+  int32_t space_order;            /* 2: minbee (reference default), 1: piecewise constant */
+  int32_t time_order;             /* 2: midpoint RK2 (reference default), 1: Euler */
+  int32_t flags;                  /* reserved, 0 */
+} nmhd_config;
+
+/* Conservation and field diagnostics, accumulated in FP64 over the interior
+ * (monitor() of src/application/kepler_disk_demo/mhd_solver.curb:107-130 and
+ * src/application/convergence_demo/mhd_solver.curb:61-100). */
+typedef struct nmhd_diag {
+  double mass;                   /* sum rho dV */
+  double momentum[3];            /* sum rho v dV */
+  double kinetic_energy;         /* sum rho v^2/2 dV */
+  double internal_energy;        /* sum p/(gamma-1) dV */
+  double magnetic_energy;        /* sum (face-averaged B^2)/2 dV */
+  double total_energy;
+  double bx2_mean, by2_mean;     /* <Bx^2>, <By^2> over all faces (reference monitor) */
+  double maxwell_stress;         /* -<Bx By> with B at cell centres */
+  double max_div_b;              /* max |div B| over interior cells */
+  double volume;
+} nmhd_diag;
+
+typedef struct nmhd_solver nmhd_solver;
+
+/* MHDSolver::MHDSolver(LocalSetup&) - allocates device state for `cfg`. */
+nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out);
+/* ~MHDSolver */
+void nmhd_destroy(nmhd_solver *s);
+
+/* Replaces initialize_state()/set_initial_condition hooks: copy a primitive
+ * state in.  fields[i] points to Sx*Sy*Sz floats, on the host
+ * (on_device = 0) or on this solver's device (on_device = 1). */
+nmhd_status nmhd_set_state(nmhd_solver *s, const float *const fields[8], int on_device);
+/* Copy the primitive state out (the arrays MHDSolver::write dumps). */
+nmhd_status nmhd_get_state(nmhd_solver *s, float *const fields[8], int on_device);
+
+/* MHDSolver::read(std::string): sizes must match (else NMHD_ERR_SIZE_MISMATCH,
+ * where the reference returns false). */
+nmhd_status nmhd_read(nmhd_solver *s, const char *path);
+/* MHDSolver::write(std::string): byte-identical to the reference's dump. */
+nmhd_status nmhd_write(nmhd_solver *s, const char *path);
+
+/* MHDSolver::proceed(goal_time, wallclock_time_limit)
+ * (src/library/mhd_solver.inlrb:850-993).  Advances until current_time reaches
+ * goal_time (rounded to float, as the reference's `Real goal_time`), the
+ * wallclock limit in seconds passes (ignored if <= 0; checked between
+ * batches of steps), or max_steps steps are done (ignored if <= 0).
+ * Returns NMHD_GOAL_REACHED, NMHD_TIMEOUT, NMHD_STEP_LIMIT or an error;
+ * *steps_done (may be NULL) receives the number of steps taken. */
+nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limit,
+                         int64_t max_steps, int64_t *steps_done);
+
+/* MHDSolver::current_time(), generation(), and the GlobalSetup fields that
+ * load_state() restores. */
+double nmhd_current_time(const nmhd_solver *s);
+int64_t nmhd_generation(const nmhd_solver *s);
+nmhd_status nmhd_set_time(nmhd_solver *s, double current_time, int64_t generation);
+
+/* dt of the last `n` steps (most recent last); returns how many were stored.
+ * The reference prints "t dt" to stderr every step (mhd_solver.inlrb:895). */
+int64_t nmhd_dt_history(const nmhd_solver *s, float *out, int64_t n);
+
+/* FP64 diagnostics of the current state (nmhd_diag). */
+nmhd_status nmhd_diagnostics(nmhd_solver *s, nmhd_diag *out);
+
+/* Device id of this solver, the CUDA stream its work runs on (a
+ * cudaStream_t, may be set to the caller's stream), last error text. */
+int nmhd_device(const nmhd_solver *s);
+nmhd_status nmhd_set_stream(nmhd_solver *s, void *cuda_stream);
+const char *nmhd_last_error(const nmhd_solver *s);
+
+/* Per-kernel timing (no counterpart in the reference, which has no timers;
+ * replaces its wallclock bench, src/application/optimize_mhd/main_detail.curb:27-57).
+ * Runs `steps` steps launching every kernel separately with CUDA events around
+ * it on the solver's stream; ms_out[i] receives the mean duration of kernel
+ * class i and launches_out[i] (may be NULL) its launches per step.  Returns the
+ * number of classes written (at most max), or a negative nmhd_status. */
+int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max);
+/* Name of kernel class i of nmhd_profile (NULL when out of range). */
+const char *nmhd_kernel_name(int i);
+
+/* Library version string. */
+const char *nmhd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* NMHD_H */

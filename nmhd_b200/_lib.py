@@ -1,0 +1,75 @@
+"""Loader for libnmhd.so (the C ABI declared in include/nmhd.h).
+
+The compute path exists only as this CUDA library: there is no CPU fallback.
+If the library is missing or cannot load, :func:`lib` raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libnmhd.so")
+
+# nmhd_status codes
+OK = 0
+GOAL_REACHED = 1
+TIMEOUT = 2
+STEP_LIMIT = 3
+ERRORS = {
+    -1: "invalid argument", -2: "CUDA error", -3: "I/O error", -4: "size mismatch",
+    -5: "numerical error", -6: "out of device memory", -7: "not supported",
+}
+
+# Every entry point declared in include/nmhd.h: (name, restype, argtypes)
+_P = ctypes.c_void_p
+_SIGS = [
+    ("nmhd_version", ctypes.c_char_p, []),
+    ("nmhd_create", ctypes.c_int, [_P, ctypes.POINTER(_P)]),
+    ("nmhd_destroy", None, [_P]),
+    ("nmhd_set_state", ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_get_state", ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_read", ctypes.c_int, [_P, ctypes.c_char_p]),
+    ("nmhd_write", ctypes.c_int, [_P, ctypes.c_char_p]),
+    ("nmhd_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
+                                    ctypes.POINTER(ctypes.c_int64)]),
+    ("nmhd_current_time", ctypes.c_double, [_P]),
+    ("nmhd_generation", ctypes.c_int64, [_P]),
+    ("nmhd_set_time", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64]),
+    ("nmhd_dt_history", ctypes.c_int64, [_P, _P, ctypes.c_int64]),
+    ("nmhd_diagnostics", ctypes.c_int, [_P, _P]),
+    ("nmhd_device", ctypes.c_int, [_P]),
+    ("nmhd_set_stream", ctypes.c_int, [_P, _P]),
+    ("nmhd_last_error", ctypes.c_char_p, [_P]),
+    ("nmhd_profile", ctypes.c_int, [_P, ctypes.c_int, _P, _P, ctypes.c_int]),
+    ("nmhd_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+]
+EXPORTS = [s[0] for s in _SIGS]
+
+_lib = None
+
+
+def build(verbose=False):
+    """Compile libnmhd.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    subprocess.run(["make", "-s" if not verbose else "-w", "-C", HERE], check=True)
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RuntimeError(f"{LIB_PATH} is not built; run nmhd_b200._lib.build()")
+        L = ctypes.CDLL(LIB_PATH)
+        for name, res, args in _SIGS:
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+class NmhdError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"{ERRORS.get(code, code)}: {message}")
+        self.code = code

@@ -1,0 +1,544 @@
+// C ABI of the B200-native ideal-MHD solver: the host side of MHDSolver
+// (src/library/mhd_solver.hrb:150-276, mhd_solver.inlrb:69-97, 850-1050).
+//
+// One nmhd_solver owns the device state of one box: two primitive-state
+// buffers (current / next, swapped on the device every step), the RK
+// predictor, the face-flux scratch and a device-resident step control block.
+// proceed() enqueues whole steps without any host round trip; batches of
+// steps are captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nmhd.h"
+#include "step.cuh"
+
+using nmhd::GridParams;
+using nmhd::StepCtl;
+
+struct nmhd_solver {
+  nmhd_config cfg;
+  GridParams g;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  float *w0 = nullptr, *w1 = nullptr, *wp = nullptr, *flux = nullptr, *dt_hist = nullptr;
+  StepCtl *ctl = nullptr;
+  double *diag = nullptr;
+  bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
+  std::map<int, cudaGraphExec_t> graphs;
+  std::string err;
+};
+
+namespace {
+
+const char *kVersion = "nmhd_b200 0.1 (sm_100a)";
+thread_local std::string g_create_error;
+
+nmhd_status fail(nmhd_solver *s, nmhd_status st, const std::string &msg) {
+  if (s) s->err = msg;
+  else g_create_error = msg;
+  return st;
+}
+
+nmhd_status cuda_fail(nmhd_solver *s, cudaError_t e, const char *what) {
+  return fail(s, e == cudaErrorMemoryAllocation ? NMHD_ERR_OUT_OF_MEMORY : NMHD_ERR_CUDA,
+              std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+#define NMHD_CUDA(s, call)                                \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return cuda_fail(s, e_, #call); \
+  } while (0)
+
+// Derived constants exactly as the reference's float chains produce them
+// (simulation_config_default.h:56-103; relative_velocity of
+// src/application/kepler_disk_demo/mhd_solver.curb:50-52).
+GridParams derive(const nmhd_config &c) {
+  GridParams g;
+  g.sx = c.size_x;
+  g.sy = c.size_y;
+  g.sz = c.size_z;
+  g.n = c.size_x * c.size_y * c.size_z;
+  g.my = c.margin_y;
+  g.mz = c.margin_z;
+  const int s[3] = {c.size_x, c.size_y, c.size_z};
+  const int gi[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
+  volatile float comp[3], local[3], d[3];
+  for (int i = 0; i < 3; ++i) {
+    volatile float per = L[i] / (float)gi[i];
+    comp[i] = per * (float)s[i];
+    local[i] = per * (float)gi[i];
+    d[i] = comp[i] / (float)s[i];
+  }
+  g.dx = d[0];
+  g.dy = d[1];
+  g.dz = d[2];
+  g.extent_x = comp[0];
+  g.corner_y = -comp[1] / 2.0f;
+  g.gamma = c.gamma;
+  g.cfl = c.cfl;
+  g.q = c.q;
+  g.omega = c.omega;
+  volatile float qo = -c.q * c.omega;
+  volatile float rv = qo * local[1];
+  g.rel_vel = (double)rv;
+  g.shear = c.problem == NMHD_PROBLEM_SHEARING_BOX;
+  g.order2 = c.space_order != 1;
+  return g;
+}
+
+nmhd_status validate(const nmhd_config *c, std::string &why) {
+  if (!c) { why = "config is NULL"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->size_x < 1 || c->size_y < 1 || c->size_z < 1) { why = "sizes must be >= 1"; return NMHD_ERR_INVALID_ARGUMENT; }
+  const long long n = (long long)c->size_x * c->size_y * c->size_z;
+  if (n * 8 >= (1LL << 31)) { why = "box too large: 8*cells must fit in int32"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->margin_y < 0 || c->margin_z < 0) { why = "margins must be >= 0"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->size_y - 2 * c->margin_y < c->margin_y || (c->margin_y > 0 && c->size_y - 2 * c->margin_y < 1)) {
+    why = "interior Y rows must be at least margin_y"; return NMHD_ERR_INVALID_ARGUMENT;
+  }
+  if (c->margin_z > 0 && c->size_z - 2 * c->margin_z < c->margin_z) {
+    why = "interior Z planes must be at least margin_z"; return NMHD_ERR_INVALID_ARGUMENT;
+  }
+  if (!(c->extent_x > 0 && c->extent_y > 0 && c->extent_z > 0)) { why = "extents must be > 0"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (!(c->gamma > 1.0f) || !(c->cfl > 0.0f)) { why = "gamma must be > 1 and cfl > 0"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->problem != NMHD_PROBLEM_NONE && c->problem != NMHD_PROBLEM_SHEARING_BOX) { why = "unknown problem"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->space_order != 1 && c->space_order != 2) { why = "space_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->time_order != 1 && c->time_order != 2) { why = "time_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
+  return NMHD_OK;
+}
+
+nmhd_status read_ctl(nmhd_solver *s, StepCtl &h) {
+  NMHD_CUDA(s, cudaMemcpyAsync(&h, s->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  return NMHD_OK;
+}
+
+nmhd_status write_ctl(nmhd_solver *s, const StepCtl &h) {
+  NMHD_CUDA(s, cudaMemcpyAsync(s->ctl, &h, sizeof(StepCtl), cudaMemcpyHostToDevice, s->stream));
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  return NMHD_OK;
+}
+
+float *current_buffer(nmhd_solver *s, const StepCtl &h) { return h.parity ? s->w1 : s->w0; }
+
+// One time step, enqueued on the solver's stream (mhd_solver.inlrb:865-985).
+void enqueue_step(nmhd_solver *s) {
+  const GridParams &g = s->g;
+  cudaStream_t st = s->stream;
+  if (g.my > 0 || g.mz > 0) {
+    nmhd::launch_fill(g, s->ctl, s->w0, s->w1, st);
+    nmhd::launch_cfl_margin(g, s->ctl, s->w0, s->w1, st);
+  }
+  if (s->cfg.time_order == 1) {
+    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 1, 0, 1, st);
+  } else {
+    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 2, 1, 0, st);
+    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 2, 1, 0, 1, st);
+  }
+}
+
+nmhd_status graph_for(nmhd_solver *s, int steps, cudaGraphExec_t *out) {
+  auto it = s->graphs.find(steps);
+  if (it != s->graphs.end()) { *out = it->second; return NMHD_OK; }
+  cudaGraph_t graph;
+  NMHD_CUDA(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < steps; ++i) enqueue_step(s);
+  NMHD_CUDA(s, cudaStreamEndCapture(s->stream, &graph));
+  cudaGraphExec_t exec;
+  cudaError_t e = cudaGraphInstantiate(&exec, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return cuda_fail(s, e, "cudaGraphInstantiate");
+  s->graphs[steps] = exec;
+  *out = exec;
+  return NMHD_OK;
+}
+
+void drop_graphs(nmhd_solver *s) {
+  for (auto &kv : s->graphs) cudaGraphExecDestroy(kv.second);
+  s->graphs.clear();
+}
+
+nmhd_status copy_fields(nmhd_solver *s, float *dev_base, const float *const in[8], float *const out[8],
+                        int on_device) {
+  const size_t bytes = sizeof(float) * (size_t)s->g.n;
+  for (int v = 0; v < 8; ++v) {
+    if (in) {
+      if (!in[v]) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+      NMHD_CUDA(s, cudaMemcpyAsync(dev_base + (size_t)v * s->g.n, in[v], bytes,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, s->stream));
+    } else {
+      if (!out[v]) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+      NMHD_CUDA(s, cudaMemcpyAsync(out[v], dev_base + (size_t)v * s->g.n, bytes,
+                                   on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, s->stream));
+    }
+  }
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  return NMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *nmhd_version(void) { return kVersion; }
+
+nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
+  if (!out) return fail(nullptr, NMHD_ERR_INVALID_ARGUMENT, "out is NULL");
+  *out = nullptr;
+  std::string why;
+  nmhd_status st = validate(cfg, why);
+  if (st != NMHD_OK) return fail(nullptr, st, why);
+  nmhd_solver *s = new nmhd_solver();
+  s->cfg = *cfg;
+  s->g = derive(*cfg);
+  cudaError_t e = cudaGetDevice(&s->device);
+  const size_t n = (size_t)s->g.n;
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) s->own_stream = true;
+  if (e == cudaSuccess) e = cudaMalloc(&s->w0, sizeof(float) * 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&s->w1, sizeof(float) * 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&s->wp, sizeof(float) * 8 * n);
+  if (e == cudaSuccess) e = cudaMalloc(&s->flux, sizeof(float) * nmhd::kFluxFields * n);
+  if (e == cudaSuccess) e = cudaMalloc(&s->dt_hist, sizeof(float) * nmhd::kDtHistCap);
+  if (e == cudaSuccess) e = cudaMalloc(&s->ctl, sizeof(StepCtl));
+  if (e == cudaSuccess) e = cudaMalloc(&s->diag, sizeof(double) * nmhd::kDiagFields);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->w0, 0, sizeof(float) * 8 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->w1, 0, sizeof(float) * 8 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->wp, 0, sizeof(float) * 8 * n, s->stream);
+  if (e == cudaSuccess) e = cudaMemsetAsync(s->dt_hist, 0, sizeof(float) * nmhd::kDtHistCap, s->stream);
+  if (e != cudaSuccess) {
+    nmhd_status r = cuda_fail(nullptr, e, "nmhd_create");
+    nmhd_destroy(s);
+    return r;
+  }
+  StepCtl h;
+  std::memset(&h, 0, sizeof(h));
+  h.cfl_cur = h.cfl_next = 0x7f800000u;
+  h.goal = INFINITY;
+  h.hist_cap = nmhd::kDtHistCap;
+  st = write_ctl(s, h);
+  if (st != NMHD_OK) {
+    g_create_error = s->err;
+    nmhd_destroy(s);
+    return st;
+  }
+  *out = s;
+  return NMHD_OK;
+}
+
+void nmhd_destroy(nmhd_solver *s) {
+  if (!s) return;
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  drop_graphs(s);
+  cudaFree(s->w0);
+  cudaFree(s->w1);
+  cudaFree(s->wp);
+  cudaFree(s->flux);
+  cudaFree(s->dt_hist);
+  cudaFree(s->ctl);
+  cudaFree(s->diag);
+  if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+  delete s;
+}
+
+nmhd_status nmhd_set_state(nmhd_solver *s, const float *const fields[8], int on_device) {
+  if (!s || !fields) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  st = copy_fields(s, current_buffer(s, h), fields, nullptr, on_device);
+  if (st != NMHD_OK) return st;
+  // A new state: its CFL time must be recomputed and earlier errors no longer apply.
+  h.status = 0;
+  h.done = 0;
+  h.cfl_cur = h.cfl_next = 0x7f800000u;
+  s->cfl_ready = false;
+  return write_ctl(s, h);
+}
+
+nmhd_status nmhd_get_state(nmhd_solver *s, float *const fields[8], int on_device) {
+  if (!s || !fields) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  return copy_fields(s, current_buffer(s, h), nullptr, fields, on_device);
+}
+
+nmhd_status nmhd_read(nmhd_solver *s, const char *path) {
+  if (!s || !path) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  FILE *fp = std::fopen(path, "rb");
+  if (!fp) return fail(s, NMHD_ERR_IO, std::string("cannot open ") + path);
+  int32_t sz[3];
+  if (std::fread(sz, sizeof(int32_t), 3, fp) != 3) {
+    std::fclose(fp);
+    return fail(s, NMHD_ERR_IO, std::string("truncated header in ") + path);
+  }
+  if (sz[0] != s->g.sx || sz[1] != s->g.sy || sz[2] != s->g.sz) {
+    std::fclose(fp);
+    char buf[160];
+    std::snprintf(buf, sizeof buf, "size mismatch: file %dx%dx%d, solver %dx%dx%d", sz[0], sz[1], sz[2],
+                  s->g.sx, s->g.sy, s->g.sz);
+    return fail(s, NMHD_ERR_SIZE_MISMATCH, buf);
+  }
+  const size_t n = (size_t)s->g.n;
+  std::vector<float> host(8 * n);
+  const size_t got = std::fread(host.data(), sizeof(float), 8 * n, fp);
+  std::fclose(fp);
+  if (got != 8 * n) return fail(s, NMHD_ERR_IO, std::string("truncated data in ") + path);
+  const float *f[8];
+  for (int v = 0; v < 8; ++v) f[v] = host.data() + v * n;
+  return nmhd_set_state(s, f, 0);
+}
+
+nmhd_status nmhd_write(nmhd_solver *s, const char *path) {
+  if (!s || !path) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  const size_t n = (size_t)s->g.n;
+  std::vector<float> host(8 * n);
+  float *f[8];
+  for (int v = 0; v < 8; ++v) f[v] = host.data() + v * n;
+  nmhd_status st = nmhd_get_state(s, f, 0);
+  if (st != NMHD_OK) return st;
+  FILE *fp = std::fopen(path, "wb");
+  if (!fp) return fail(s, NMHD_ERR_IO, std::string("cannot open ") + path);
+  const int32_t sz[3] = {s->g.sx, s->g.sy, s->g.sz};
+  bool ok = std::fwrite(sz, sizeof(int32_t), 3, fp) == 3;
+  ok = ok && std::fwrite(host.data(), sizeof(float), 8 * n, fp) == 8 * n;
+  ok = (std::fclose(fp) == 0) && ok;
+  return ok ? NMHD_OK : fail(s, NMHD_ERR_IO, std::string("cannot write ") + path);
+}
+
+nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limit, int64_t max_steps,
+                         int64_t *steps_done) {
+  if (steps_done) *steps_done = 0;
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  const auto t0 = std::chrono::steady_clock::now();
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (h.status) return fail(s, NMHD_ERR_NUMERICAL, "state is not valid (set a new state)");
+  const long long gen0 = h.generation;
+  h.goal = (float)goal_time;
+  h.done = 0;
+  if (!s->cfl_ready) {
+    h.cfl_cur = h.cfl_next = 0x7f800000u;
+    h.blocks_done = 0;
+  }
+  st = write_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (!s->cfl_ready) {
+    // CFL time of the fresh state, after its margins are filled.
+    nmhd::launch_fill(s->g, s->ctl, s->w0, s->w1, s->stream);
+    nmhd::launch_cfl_all(s->g, s->ctl, s->w0, s->w1, s->stream);
+    NMHD_CUDA(s, cudaGetLastError());
+    s->cfl_ready = true;
+  }
+  const int kBatch = 16;
+  long long left = max_steps > 0 ? max_steps : -1;
+  nmhd_status result = NMHD_OK;
+  for (;;) {
+    int batch = kBatch;
+    if (left >= 0 && left < batch) batch = (int)left;
+    if (batch == 0) { result = NMHD_STEP_LIMIT; break; }
+    cudaGraphExec_t ge;
+    st = graph_for(s, batch, &ge);
+    if (st != NMHD_OK) return st;
+    NMHD_CUDA(s, cudaGraphLaunch(ge, s->stream));
+    st = read_ctl(s, h);
+    if (st != NMHD_OK) return st;
+    if (left > 0) left -= batch;
+    if (h.status) {
+      result = fail(s, NMHD_ERR_NUMERICAL,
+                    (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
+                                                    : "non-finite state, density <= 0 or pressure <= 0");
+      break;
+    }
+    if (h.done) { result = NMHD_GOAL_REACHED; break; }
+    if (wallclock_limit > 0) {
+      const double el = std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+      if (el > wallclock_limit) { result = NMHD_TIMEOUT; break; }
+    }
+  }
+  if (steps_done) *steps_done = h.generation - gen0;
+  return result;
+}
+
+double nmhd_current_time(const nmhd_solver *s) {
+  if (!s) return NAN;
+  StepCtl h;
+  if (read_ctl(const_cast<nmhd_solver *>(s), h) != NMHD_OK) return NAN;
+  return h.time;
+}
+
+int64_t nmhd_generation(const nmhd_solver *s) {
+  if (!s) return -1;
+  StepCtl h;
+  if (read_ctl(const_cast<nmhd_solver *>(s), h) != NMHD_OK) return -1;
+  return h.generation;
+}
+
+nmhd_status nmhd_set_time(nmhd_solver *s, double current_time, int64_t generation) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  h.time = current_time;
+  h.generation = generation;
+  // The shearing fill depends on the time: recompute margins and CFL.
+  s->cfl_ready = false;
+  return write_ctl(s, h);
+}
+
+int64_t nmhd_dt_history(const nmhd_solver *s, float *out, int64_t n) {
+  if (!s || !out || n <= 0) return 0;
+  nmhd_solver *m = const_cast<nmhd_solver *>(s);
+  StepCtl h;
+  if (read_ctl(m, h) != NMHD_OK) return 0;
+  std::vector<float> all(nmhd::kDtHistCap);
+  if (cudaMemcpy(all.data(), s->dt_hist, sizeof(float) * nmhd::kDtHistCap, cudaMemcpyDeviceToHost) !=
+      cudaSuccess)
+    return 0;
+  long long avail = h.generation < nmhd::kDtHistCap ? h.generation : nmhd::kDtHistCap;
+  long long k = n < avail ? n : avail;
+  for (long long i = 0; i < k; ++i) {
+    long long gen = h.generation - k + i;
+    out[i] = all[gen % nmhd::kDtHistCap];
+  }
+  return k;
+}
+
+nmhd_status nmhd_diagnostics(nmhd_solver *s, nmhd_diag *out) {
+  if (!s || !out) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  NMHD_CUDA(s, cudaMemsetAsync(s->diag, 0, sizeof(double) * nmhd::kDiagFields, s->stream));
+  nmhd::launch_diag(s->g, s->ctl, s->w0, s->w1, s->diag, s->stream);
+  NMHD_CUDA(s, cudaGetLastError());
+  double a[nmhd::kDiagFields];
+  NMHD_CUDA(s, cudaMemcpyAsync(a, s->diag, sizeof(a), cudaMemcpyDeviceToHost, s->stream));
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  std::memset(out, 0, sizeof(*out));
+  out->mass = a[0];
+  out->momentum[0] = a[1];
+  out->momentum[1] = a[2];
+  out->momentum[2] = a[3];
+  out->kinetic_energy = a[4];
+  out->internal_energy = a[5];
+  out->magnetic_energy = a[6];
+  out->total_energy = a[4] + a[5] + a[6];
+  out->volume = a[8];
+  out->maxwell_stress = a[8] > 0 ? a[7] / a[8] : 0.0;
+  out->bx2_mean = a[9] / (double)s->g.n;
+  out->by2_mean = a[10] / (double)s->g.n;
+  out->max_div_b = a[nmhd::kDiagFields - 1];
+  return NMHD_OK;
+}
+
+namespace {
+const char *kKernelNames[] = {"fill_margins", "cfl_margins", "flux_stage1", "update_stage1",
+                              "flux_stage2", "update_stage2"};
+constexpr int kKernelClasses = 6;
+}  // namespace
+
+const char *nmhd_kernel_name(int i) {
+  return (i >= 0 && i < kKernelClasses) ? kKernelNames[i] : nullptr;
+}
+
+int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max) {
+  if (!s || !ms_out || steps <= 0 || max <= 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  h.goal = INFINITY;
+  h.done = 0;
+  if (!s->cfl_ready) h.cfl_cur = h.cfl_next = 0x7f800000u;
+  st = write_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (!s->cfl_ready) {
+    nmhd::launch_fill(s->g, s->ctl, s->w0, s->w1, s->stream);
+    nmhd::launch_cfl_all(s->g, s->ctl, s->w0, s->w1, s->stream);
+    s->cfl_ready = true;
+  }
+  cudaEvent_t ev[kKernelClasses + 1];
+  for (auto &e : ev) NMHD_CUDA(s, cudaEventCreate(&e));
+  double acc[kKernelClasses] = {0};
+  double cnt[kKernelClasses] = {0};
+  const GridParams &g = s->g;
+  cudaStream_t q = s->stream;
+  const bool margins = g.my > 0 || g.mz > 0;
+  const bool midpoint = s->cfg.time_order != 1;
+  for (int it = 0; it < steps; ++it) {
+    NMHD_CUDA(s, cudaEventRecord(ev[0], q));
+    if (margins) nmhd::launch_fill(g, s->ctl, s->w0, s->w1, q);
+    NMHD_CUDA(s, cudaEventRecord(ev[1], q));
+    if (margins) nmhd::launch_cfl_margin(g, s->ctl, s->w0, s->w1, q);
+    NMHD_CUDA(s, cudaEventRecord(ev[2], q));
+    if (midpoint) {
+      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 0, 1, q);
+      NMHD_CUDA(s, cudaEventRecord(ev[3], q));
+      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 2, 1, 0, q);
+      NMHD_CUDA(s, cudaEventRecord(ev[4], q));
+      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 2, 0, q);
+      NMHD_CUDA(s, cudaEventRecord(ev[5], q));
+      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 2, 1, 0, 1, q);
+    } else {
+      NMHD_CUDA(s, cudaEventRecord(ev[3], q));
+      NMHD_CUDA(s, cudaEventRecord(ev[4], q));
+      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 0, 0, q);
+      NMHD_CUDA(s, cudaEventRecord(ev[5], q));
+      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 1, 0, 1, q);
+    }
+    NMHD_CUDA(s, cudaEventRecord(ev[6], q));
+    NMHD_CUDA(s, cudaEventSynchronize(ev[6]));
+    for (int k = 0; k < kKernelClasses; ++k) {
+      float ms = 0.f;
+      NMHD_CUDA(s, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
+      acc[k] += ms;
+    }
+    cnt[0] += margins;
+    cnt[1] += margins;
+    cnt[2] += midpoint;
+    cnt[3] += midpoint;
+    cnt[4] += 1;
+    cnt[5] += 1;
+  }
+  for (auto &e : ev) cudaEventDestroy(e);
+  NMHD_CUDA(s, cudaGetLastError());
+  st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (h.status) return fail(s, NMHD_ERR_NUMERICAL, "numerical error while profiling");
+  const int k = max < kKernelClasses ? max : kKernelClasses;
+  for (int i = 0; i < k; ++i) {
+    ms_out[i] = acc[i] / steps;
+    if (launches_out) launches_out[i] = cnt[i] / steps;
+  }
+  return k;
+}
+
+int nmhd_device(const nmhd_solver *s) { return s ? s->device : -1; }
+
+nmhd_status nmhd_set_stream(nmhd_solver *s, void *cuda_stream) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  if (s->own_stream) cudaStreamDestroy(s->stream);
+  s->own_stream = cuda_stream == nullptr;
+  if (s->own_stream) {
+    NMHD_CUDA(s, cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking));
+  } else {
+    s->stream = (cudaStream_t)cuda_stream;
+  }
+  return NMHD_OK;
+}
+
+const char *nmhd_last_error(const nmhd_solver *s) {
+  return s ? s->err.c_str() : g_create_error.c_str();
+}
+
+}  // extern "C"

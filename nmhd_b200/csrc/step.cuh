@@ -1,0 +1,63 @@
+// Internal interface between the C ABI (solver.cu) and the step kernels.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace nmhd {
+
+// Runtime constants of one box (the reference's simulation_config.h values).
+struct GridParams {
+  int sx, sy, sz;  // cells including margins
+  int n;           // sx*sy*sz
+  int my, mz;      // margins
+  float dx, dy, dz;
+  float gamma, cfl;
+  float q, omega;
+  float corner_y;  // origin of the Kepler radial coordinate (-kExtentY/2)
+  float extent_x;  // kExtentX
+  double rel_vel;  // relative_velocity(): -q*Omega*kLocalExtentY
+  int shear;       // shearing box: Kepler acceleration + shearing-periodic Y margins
+  int order2;      // minbee (2) vs piecewise-constant (1) reconstruction
+};
+
+// Device-resident step control.  The time step is a pure function of
+// (cfl_cur, time, goal), evaluated identically by every block that needs it, so
+// no host round trip is needed between steps.
+struct StepCtl {
+  double time;                // current_time (FP64, as the reference's PreciseReal)
+  long long generation;
+  unsigned cfl_cur;           // float bits: min over cells of the CFL time (this step)
+  unsigned cfl_next;          // accumulated by the final stage for the next step
+  float goal;                 // goal_time as float (the reference's `Real goal_time`)
+  int parity;                 // which of the two state buffers holds the current state
+  int done;                   // goal reached or run stopped: later kernels return at once
+  int status;                 // kStatus* bits
+  unsigned blocks_done;       // last-block detection in the final stage
+  int hist_cap;
+};
+
+enum : int { kStatusNumerical = 1, kStatusBadDt = 2 };
+constexpr int kDtHistCap = 4096;
+constexpr int kFluxFields = 21;  // 3 face directions x 7 flux components
+
+// Launchers (all asynchronous on `stream`).
+void launch_cfl_all(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
+void launch_cfl_margin(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
+void launch_fill(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
+// One RK stage: fluxes from buffer `in_sel`, conserved state from the current
+// buffer, result into `out_sel` (0 current, 1 next, 2 predictor); `half`
+// selects dt/2; `final_stage` reduces the next CFL time and advances the clock.
+void launch_stage(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                  float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                  cudaStream_t stream);
+// The two kernels of a stage, separately (for per-kernel timing).
+void launch_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                 int in_sel, int half, cudaStream_t stream);
+void launch_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                   float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                   cudaStream_t stream);
+void launch_diag(const GridParams &g, StepCtl *ctl, float *w0, float *w1, double *acc,
+                 cudaStream_t stream);
+constexpr int kDiagFields = 14;
+
+}  // namespace nmhd

@@ -1,0 +1,207 @@
+"""Host-side mirror of the reference's solver interface.
+
+:class:`MHDSolver` keeps the member names, argument meaning and error
+behaviour of the reference's ``class MHDSolver``
+(src/library/mhd_solver.hrb:150-276): ``read``/``write`` return ``False`` on
+failure, ``proceed`` returns ``True`` when the goal time was reached and
+``False`` on a wallclock timeout, ``current_time``/``generation`` report the
+clock.  Problem hooks cannot cross the C ABI, so ``initialize_state`` takes the
+initial primitive state as an array (see :mod:`nmhd_b200.problems`).
+
+Every call goes through libnmhd.so (include/nmhd.h); the compute runs only on
+the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+import json
+import math
+import os
+
+import numpy as np
+
+from . import _lib
+from .config import SolverConfig
+
+
+class NmhdDiag(ctypes.Structure):
+    _fields_ = [
+        ("mass", ctypes.c_double), ("momentum", ctypes.c_double * 3),
+        ("kinetic_energy", ctypes.c_double), ("internal_energy", ctypes.c_double),
+        ("magnetic_energy", ctypes.c_double), ("total_energy", ctypes.c_double),
+        ("bx2_mean", ctypes.c_double), ("by2_mean", ctypes.c_double),
+        ("maxwell_stress", ctypes.c_double), ("max_div_b", ctypes.c_double),
+        ("volume", ctypes.c_double),
+    ]
+
+
+def _check(L, handle, code):
+    if code < 0:
+        raise _lib.NmhdError(code, L.nmhd_last_error(handle).decode())
+    return code
+
+
+class MHDSolver:
+    """One box advanced by the B200 time step (MHDSolver::MHDSolver(LocalSetup&))."""
+
+    def __init__(self, config: SolverConfig):
+        self.config = config
+        self._L = _lib.lib()
+        self._c = config.to_ctypes()
+        h = ctypes.c_void_p()
+        code = self._L.nmhd_create(ctypes.byref(self._c), ctypes.byref(h))
+        if code != 0:
+            raise _lib.NmhdError(code, self._L.nmhd_last_error(None).decode())
+        self._h = h
+        self.last_status = _lib.OK
+
+    # -- lifetime --------------------------------------------------------
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.nmhd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- state -----------------------------------------------------------
+    def _ptrs(self, arr):
+        n = self.config.cells
+        base = arr.ctypes.data
+        return (ctypes.c_void_p * 8)(*[base + 4 * n * v for v in range(8)])
+
+    def initialize_state(self, state):
+        """Set the primitive state (8, Sz, Sy, Sx) float32 (replaces the
+        reference's set_initial_condition hook)."""
+        self.set_state(state)
+
+    def set_state(self, state):
+        st = np.ascontiguousarray(state, dtype=np.float32)
+        if st.shape != (8,) + self.config.shape:
+            raise ValueError(f"state shape {st.shape} != {(8,) + self.config.shape}")
+        _check(self._L, self._h, self._L.nmhd_set_state(self._h, self._ptrs(st), 0))
+
+    def set_state_device(self, tensor):
+        """Set the state from a CUDA tensor (8, Sz, Sy, Sx) float32 on this device."""
+        n = self.config.cells
+        t = tensor.contiguous()
+        base = t.data_ptr()
+        ptrs = (ctypes.c_void_p * 8)(*[base + 4 * n * v for v in range(8)])
+        _check(self._L, self._h, self._L.nmhd_set_state(self._h, ptrs, 1))
+
+    def get_state(self, out=None):
+        if out is None:
+            out = np.empty((8,) + self.config.shape, dtype=np.float32)
+        _check(self._L, self._h, self._L.nmhd_get_state(self._h, self._ptrs(out), 0))
+        return out
+
+    def get_state_device(self, tensor):
+        n = self.config.cells
+        base = tensor.data_ptr()
+        ptrs = (ctypes.c_void_p * 8)(*[base + 4 * n * v for v in range(8)])
+        _check(self._L, self._h, self._L.nmhd_get_state(self._h, ptrs, 1))
+        return tensor
+
+    def read(self, path) -> bool:
+        """MHDSolver::read: False when the file cannot be read or sizes differ."""
+        code = self._L.nmhd_read(self._h, os.fsencode(path))
+        self.last_status = code
+        return code == 0
+
+    def write(self, path) -> bool:
+        code = self._L.nmhd_write(self._h, os.fsencode(path))
+        self.last_status = code
+        return code == 0
+
+    # -- time stepping ---------------------------------------------------
+    def proceed(self, goal_time, wallclock_time_limit=-1.0, max_steps=0) -> bool:
+        """MHDSolver::proceed: integrate until ``goal_time`` (True) or until the
+        wallclock limit in seconds passes (False); ``max_steps`` > 0 also stops
+        after that many steps (False).  Raises on numerical or CUDA errors."""
+        done = ctypes.c_int64(0)
+        code = self._L.nmhd_proceed(self._h, float(goal_time), float(wallclock_time_limit),
+                                    int(max_steps), ctypes.byref(done))
+        self.last_status = code
+        self.last_steps = done.value
+        _check(self._L, self._h, code)
+        return code == _lib.GOAL_REACHED
+
+    def step(self, nsteps):
+        """Advance exactly ``nsteps`` steps (no goal time); returns steps done."""
+        self.proceed(math.inf, -1.0, nsteps)
+        return self.last_steps
+
+    def current_time(self) -> float:
+        return self._L.nmhd_current_time(self._h)
+
+    def generation(self) -> int:
+        return self._L.nmhd_generation(self._h)
+
+    def set_time(self, current_time, generation):
+        _check(self._L, self._h, self._L.nmhd_set_time(self._h, float(current_time), int(generation)))
+
+    def dt_history(self, n):
+        out = np.zeros(n, np.float32)
+        k = self._L.nmhd_dt_history(self._h, out.ctypes.data, n)
+        return out[:k]
+
+    def diagnostics(self):
+        d = NmhdDiag()
+        _check(self._L, self._h, self._L.nmhd_diagnostics(self._h, ctypes.byref(d)))
+        return {
+            "mass": d.mass, "momentum": list(d.momentum), "kinetic_energy": d.kinetic_energy,
+            "internal_energy": d.internal_energy, "magnetic_energy": d.magnetic_energy,
+            "total_energy": d.total_energy, "bx2_mean": d.bx2_mean, "by2_mean": d.by2_mean,
+            "maxwell_stress": d.maxwell_stress, "max_div_b": d.max_div_b, "volume": d.volume,
+        }
+
+    # -- checkpoint ------------------------------------------------------
+    def save_state(self, prefix) -> bool:
+        """MHDSolver::save_state: ``prefix.bin`` plus ``prefix_setup.json`` with
+        the clock (generation, current_time) and the configuration."""
+        if not self.write(str(prefix) + ".bin"):
+            return False
+        meta = {"generation": self.generation(), "current_time": self.current_time(),
+                "config": self.config.__dict__}
+        with open(str(prefix) + "_setup.json", "w") as fp:
+            json.dump(meta, fp)
+        return True
+
+    def load_state(self, prefix) -> bool:
+        """MHDSolver::load_state: restores the clock and the state; False (and
+        the state unchanged) when the files cannot be read."""
+        try:
+            with open(str(prefix) + "_setup.json") as fp:
+                meta = json.load(fp)
+        except OSError:
+            return False
+        if not self.read(str(prefix) + ".bin"):
+            return False
+        self.set_time(meta["current_time"], meta["generation"])
+        return True
+
+    def profile(self, steps):
+        """Mean device time (ms) and launches per step of every kernel class,
+        from CUDA events around separately launched kernels."""
+        ms = np.zeros(16, np.float64)
+        launches = np.zeros(16, np.float64)
+        k = _check(self._L, self._h, self._L.nmhd_profile(self._h, int(steps), ms.ctypes.data,
+                                                          launches.ctypes.data, 16))
+        return {self._L.nmhd_kernel_name(i).decode(): (float(ms[i]), float(launches[i]))
+                for i in range(k)}
+
+    @property
+    def device(self):
+        return self._L.nmhd_device(self._h)
+
+    def set_stream(self, stream_ptr):
+        _check(self._L, self._h, self._L.nmhd_set_stream(self._h, ctypes.c_void_p(stream_ptr)))

@@ -1,0 +1,59 @@
+"""Generate the golden fixtures in this directory from the reference itself.
+
+Runs the host-compiled reference solver (oracle/_ref/ref_*, built by
+``make -C oracle ref`` from the reference sources; see oracle/Makefile) on
+seeded inputs and stores its outputs.  The reference ships no golden vectors
+of its own, so these fixtures pin both the oracle (tests/test_oracle_pin.py)
+and, through it, the CUDA path.
+
+Usage:  python tests/golden/make_golden.py
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+from nmhd_b200.problems import orszag_tang_3d, shearing_box  # noqa: E402
+from oracle import oracle  # noqa: E402
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+# name -> (reference binary, problem builder, steps, goal_time, store input)
+CASES = {
+    "ot16": ("ot16", lambda: orszag_tang_3d(16), 10, 1.0e30, True),
+    "ot16_goal": ("ot16", lambda: orszag_tang_3d(16), 100, 0.05, True),
+    "ot24x20x12": ("ot24x20x12", lambda: orszag_tang_3d(24, ny=20, nz=12), 12, 1.0e30, True),
+    "shear32x16x8": ("shear32x16x8",
+                     lambda: shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0),
+                     20, 1.0e30, False),
+    "shear48x20x12": ("shear48x20x12",
+                      lambda: shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12, l_azimuthal=2.0),
+                      8, 1.0e30, False),
+}
+
+
+def digest(a):
+    return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
+
+
+def main():
+    for name, (binary, make, steps, goal, keep_input) in CASES.items():
+        cfg, state = make()
+        out, times, info = oracle.run_ref(binary, state, steps, goal_time=goal)
+        payload = {"output": out, "times": times, "steps": np.int64(info["steps"]),
+                   "goal_time": np.float64(goal), "input_sha256": np.bytes_(digest(state)),
+                   "goal_reached": np.int64(info["goal_reached"])}
+        if keep_input:
+            payload["input"] = state
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **payload)
+        print(name, info)
+
+
+if __name__ == "__main__":
+    main()

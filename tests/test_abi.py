@@ -1,0 +1,80 @@
+"""CPU checks of the drop-in boundary: libnmhd.so loads and exports exactly the
+entry points include/nmhd.h declares; host-side config and problem setup."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from nmhd_b200 import _lib
+from nmhd_b200.config import NmhdConfig, SolverConfig
+from nmhd_b200.problems import orszag_tang_3d, shearing_box
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def header_symbols():
+    text = open(os.path.join(ROOT, "include", "nmhd.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(nmhd_[a-z_0-9]+)\s*\(", text)))
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(_lib.LIB_PATH):
+        _lib.build()
+    L = ctypes.CDLL(_lib.LIB_PATH)
+    syms = header_symbols()
+    assert len(syms) >= 15
+    for name in syms:
+        assert hasattr(L, name), f"libnmhd.so does not export {name}"
+    assert sorted(_lib.EXPORTS) == syms, "Python binding and header disagree"
+
+
+def test_version_string():
+    assert b"sm_100a" in _lib.lib().nmhd_version()
+
+
+def test_create_rejects_bad_config_without_touching_the_gpu():
+    L = _lib.lib()
+    bad = SolverConfig(size_x=0, size_y=4, size_z=4).to_ctypes()
+    h = ctypes.c_void_p()
+    assert L.nmhd_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+    assert b"sizes" in L.nmhd_last_error(None)
+    bad = SolverConfig(size_x=8, size_y=10, size_z=4, margin_y=4).to_ctypes()
+    assert L.nmhd_create(ctypes.byref(bad), ctypes.byref(h)) == -1
+
+
+def test_config_struct_layout_matches_header():
+    # 16 four-byte fields, no padding
+    assert ctypes.sizeof(NmhdConfig) == 64
+
+
+def test_derived_constants_follow_reference_float_chains():
+    cfg, _ = shearing_box()
+    d = cfg.derived()
+    assert d["dy"] == np.float32(1.0 / 128)          # 1.0625 / 136
+    assert d["dx"] == np.float32(4.0 / 256)
+    assert d["extent_y"] == np.float32(1.0625)
+    assert d["relative_velocity"] == -1.5
+    c48 = SolverConfig(size_x=48, size_y=28, size_z=12, margin_y=4, extent_x=2.0)
+    dd = c48.derived()
+    f = np.float32
+    assert dd["dx"] == f(f(f(f(2.0) / f(48)) * f(48)) / f(48))
+
+
+def test_shearing_box_background_is_reference_equilibrium():
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, noise=0.0)
+    d = cfg.derived()
+    y = np.arange(cfg.size_y, dtype=np.float32)
+    ly = np.float32(d["corner_y"]) + np.float32(d["dy"]) * (y + np.float32(0.5))
+    assert np.array_equal(s[1, 0, :, 0], (np.float32(-1.5) * np.float32(1.0)) * ly)
+    assert np.all(s[2:4] == 0) and np.all(s[5:7] == 0)
+    assert np.allclose(s[7], np.sqrt(2.0 / 400.0))
+
+
+def test_orszag_tang_face_field_is_divergence_free():
+    cfg, s = orszag_tang_3d(32)
+    bx, by = s[5].astype(np.float64), s[6].astype(np.float64)
+    div = (np.roll(bx, -1, axis=2) - bx) * 32 + (np.roll(by, -1, axis=1) - by) * 32
+    assert np.max(np.abs(div)) < 1e-4

@@ -1,0 +1,164 @@
+"""Parity of the CUDA time step (libnmhd.so, called through the C ABI) with the
+reference.  Tolerance: bitwise equality of every state value after every
+tested number of steps, and identical step times; the CUDA path mirrors the
+reference's operation order and promotions, so anything else is a bug."""
+import math
+import os
+
+import numpy as np
+import pytest
+
+from nmhd_b200.binio import read_bin, write_bin
+from nmhd_b200.config import SolverConfig
+from nmhd_b200.problems import orszag_tang_3d, shearing_box
+from nmhd_b200.solver import MHDSolver
+from nmhd_b200 import _lib
+from oracle import oracle
+
+from test_oracle_pin import GOLDEN, load_golden
+
+pytestmark = pytest.mark.gpu
+
+
+def run_gpu(cfg, state, steps, goal=math.inf):
+    with MHDSolver(cfg) as s:
+        s.set_state(state)
+        reached = s.proceed(goal, -1.0, steps)
+        return {"state": s.get_state(), "time": s.current_time(), "generation": s.generation(),
+                "dts": s.dt_history(steps), "reached": reached}
+
+
+def assert_same(a, b):
+    diff = np.argwhere(a != b)
+    assert diff.size == 0, f"{len(diff)} values differ, first at {diff[:3].tolist()}"
+
+
+@pytest.mark.parametrize("name", sorted(GOLDEN))
+def test_gpu_matches_reference_golden(gpu, golden_dir, name):
+    cfg, state, fx = load_golden(golden_dir, name)
+    steps = int(fx["steps"])
+    goal = float(fx["goal_time"])
+    r = run_gpu(cfg, state, 1000 if goal < 1e29 else steps, goal if goal < 1e29 else math.inf)
+    assert r["generation"] == steps
+    assert_same(r["state"], fx["output"])
+    times = fx["times"]
+    assert r["time"] == (times[-1] if goal > 1e29 else float(np.float32(goal)))
+
+
+@pytest.mark.parametrize("case", ["ot32", "ot_2d", "shear64x40x16", "shear_mz", "euler", "order1"])
+def test_gpu_matches_oracle(gpu, case):
+    if case == "ot32":
+        cfg, s = orszag_tang_3d(32)
+        steps = 25
+    elif case == "ot_2d":
+        cfg, s = orszag_tang_3d(40, ny=24, nz=1)
+        steps = 30
+    elif case == "shear64x40x16":
+        cfg, s = shearing_box(n_radial=32, n_azimuthal=64, n_vertical=16, l_azimuthal=4.0, seed=7)
+        steps = 30
+    elif case == "shear_mz":
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=3)
+        cfg.margin_z, cfg.size_z = 4, 16
+        s = np.concatenate([s[:, -4:], s, s[:, :4]], axis=1)
+        steps = 15
+    elif case == "euler":
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=4)
+        cfg.time_order = 1
+        steps = 20
+    else:
+        cfg, s = orszag_tang_3d(24, ny=20, nz=12)
+        cfg.space_order = 1
+        steps = 20
+    o = oracle.proceed(cfg, s, steps)
+    r = run_gpu(cfg, s, steps)
+    assert r["generation"] == steps
+    assert r["time"] == o["time"]
+    assert np.array_equal(r["dts"], o["dts"])
+    assert_same(r["state"], o["state"])
+
+
+def test_gpu_full_size_mri_box_matches_oracle_and_keeps_div_b(gpu):
+    """128(radial) x 256(azimuthal) x 64 box of the MRI benchmark, a few steps."""
+    cfg, s = shearing_box()
+    o = oracle.proceed(cfg, s, 3)
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        d0 = sol.diagnostics()
+        sol.step(3)
+        assert_same(sol.get_state(), o["state"])
+        d1 = sol.diagnostics()
+    assert d1["max_div_b"] < 1e-4 * math.sqrt(2 / 400) * 128
+    assert abs(d1["mass"] - d0["mass"]) < 1e-6 * d0["mass"]
+
+
+def test_chunked_proceed_equals_single_call(gpu):
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=9)
+    with MHDSolver(cfg) as a, MHDSolver(cfg) as b:
+        a.set_state(s)
+        b.set_state(s)
+        a.step(37)
+        for k in (1, 16, 3, 17):
+            b.step(k)
+        assert a.generation() == b.generation() == 37
+        assert a.current_time() == b.current_time()
+        assert_same(a.get_state(), b.get_state())
+
+
+def test_read_write_bin_roundtrip(gpu, tmp_path):
+    cfg, s = orszag_tang_3d(16)
+    p_in, p_out = tmp_path / "in.bin", tmp_path / "out.bin"
+    write_bin(p_in, s)
+    with MHDSolver(cfg) as sol:
+        assert sol.read(p_in)
+        assert sol.write(p_out)
+        assert open(p_in, "rb").read() == open(p_out, "rb").read()
+        bad = tmp_path / "bad.bin"
+        write_bin(bad, np.zeros((8, 4, 4, 4), np.float32))
+        assert not sol.read(bad)
+        assert sol.last_status == -4
+        assert not sol.read(tmp_path / "missing.bin")
+
+
+def test_save_load_state_resumes_bitwise(gpu, tmp_path):
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=11)
+    with MHDSolver(cfg) as a:
+        a.set_state(s)
+        a.step(10)
+        assert a.save_state(tmp_path / "c")
+        a.step(10)
+        ref = a.get_state()
+        t_ref = a.current_time()
+    with MHDSolver(cfg) as b:
+        assert b.load_state(tmp_path / "c")
+        assert b.generation() == 10
+        b.step(10)
+        assert b.current_time() == t_ref
+        assert_same(b.get_state(), ref)
+
+
+def test_numerical_failure_is_reported_not_faulted(gpu):
+    """A state with negative pressure: the kernels produce NaN, the host sees
+    NMHD_ERR_NUMERICAL; the GPU context stays usable."""
+    cfg, s = orszag_tang_3d(16)
+    s = s.copy()
+    s[4, 3, 3, 3] = -1.0
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        with pytest.raises(_lib.NmhdError) as e:
+            sol.step(5)
+        assert e.value.code == -5
+        cfg2, good = orszag_tang_3d(16)
+        sol.set_state(good)
+        sol.step(2)
+        assert sol.generation() == 2
+
+
+def test_goal_time_semantics(gpu):
+    cfg, s = orszag_tang_3d(16)
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        assert sol.proceed(0.02)
+        assert sol.current_time() == float(np.float32(0.02))
+        g = sol.generation()
+        assert not sol.proceed(1.0, -1.0, 3)
+        assert sol.generation() == g + 3
