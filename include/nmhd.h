@@ -134,6 +134,12 @@ const char *nmhd_last_error(const nmhd_solver *s);
  * class i and launches_out[i] (may be NULL) its launches per step.  Returns the
  * number of classes written (at most max), or a negative nmhd_status. */
 int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max);
+/* Kernel selection (the reference picks launch shapes with its Ruby autotuner,
+ * src/application/optimize_mhd, kernel_call() in src/library/mhd_solver.inlrb:24-33).
+ * variant 0: tiled kernels (32 x tile_rows cells per CTA, tile_rows in
+ * {4, 8, 16}, z_chunk planes per CTA, 0 = whole height); variant 1: per-cell
+ * flux and update kernels.  Every variant gives bitwise identical results. */
+nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
 /* Name of kernel class i of nmhd_profile (NULL when out of range). */
 const char *nmhd_kernel_name(int i);
 

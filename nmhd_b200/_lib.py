@@ -44,6 +44,7 @@ _SIGS = [
     ("nmhd_last_error", ctypes.c_char_p, [_P]),
     ("nmhd_profile", ctypes.c_int, [_P, ctypes.c_int, _P, _P, ctypes.c_int]),
     ("nmhd_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
+    ("nmhd_set_kernel", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
 ]
 EXPORTS = [s[0] for s in _SIGS]
 

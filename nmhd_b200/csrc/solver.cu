@@ -32,6 +32,8 @@ struct nmhd_solver {
   StepCtl *ctl = nullptr;
   double *diag = nullptr;
   bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
+  int variant = 0;         // 0: tiled kernels, 1: per-cell flux + update kernels
+  nmhd::TileShape shape = {8, 16};
   std::map<int, cudaGraphExec_t> graphs;
   std::string err;
 };
@@ -130,6 +132,19 @@ nmhd_status write_ctl(nmhd_solver *s, const StepCtl &h) {
 
 float *current_buffer(nmhd_solver *s, const StepCtl &h) { return h.parity ? s->w1 : s->w0; }
 
+// One RK stage with the selected kernel variant.
+void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
+  const GridParams &g = s->g;
+  if (s->variant == 0) {
+    float *unew = s->flux, *bflux = s->flux + (size_t)5 * g.n;
+    nmhd::launch_tile_stage(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
+                            half, final_stage, s->shape, st);
+  } else {
+    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
+                       final_stage, st);
+  }
+}
+
 // One time step, enqueued on the solver's stream (mhd_solver.inlrb:865-985).
 void enqueue_step(nmhd_solver *s) {
   const GridParams &g = s->g;
@@ -139,10 +154,10 @@ void enqueue_step(nmhd_solver *s) {
     nmhd::launch_cfl_margin(g, s->ctl, s->w0, s->w1, st);
   }
   if (s->cfg.time_order == 1) {
-    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 1, 0, 1, st);
+    enqueue_stage(s, 0, 1, 0, 1, st);
   } else {
-    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 2, 1, 0, st);
-    nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 2, 1, 0, 1, st);
+    enqueue_stage(s, 0, 2, 1, 0, st);
+    enqueue_stage(s, 2, 1, 0, 1, st);
   }
 }
 
@@ -479,20 +494,36 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
     NMHD_CUDA(s, cudaEventRecord(ev[1], q));
     if (margins) nmhd::launch_cfl_margin(g, s->ctl, s->w0, s->w1, q);
     NMHD_CUDA(s, cudaEventRecord(ev[2], q));
+    float *unew = s->flux, *bflux = s->flux + (size_t)5 * g.n;
+    // each stage as its two kernels (flux, then update / CT), separately timed
+    auto flux_k = [&](int in_sel, int half) {
+      if (s->variant == 0)
+        nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
+      else
+        nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
+    };
+    auto upd_k = [&](int in_sel, int out_sel, int half, int fin) {
+      if (s->variant == 0)
+        nmhd::launch_tile_ct(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
+                             half, fin, s->shape, q);
+      else
+        nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
+                            fin, q);
+    };
     if (midpoint) {
-      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 0, 1, q);
+      flux_k(0, 1);
       NMHD_CUDA(s, cudaEventRecord(ev[3], q));
-      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 2, 1, 0, q);
+      upd_k(0, 2, 1, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[4], q));
-      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 2, 0, q);
+      flux_k(2, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[5], q));
-      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 2, 1, 0, 1, q);
+      upd_k(2, 1, 0, 1);
     } else {
       NMHD_CUDA(s, cudaEventRecord(ev[3], q));
       NMHD_CUDA(s, cudaEventRecord(ev[4], q));
-      nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, 0, 0, q);
+      flux_k(0, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[5], q));
-      nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, 0, 1, 0, 1, q);
+      upd_k(0, 1, 0, 1);
     }
     NMHD_CUDA(s, cudaEventRecord(ev[6], q));
     NMHD_CUDA(s, cudaEventSynchronize(ev[6]));
@@ -519,6 +550,19 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
     if (launches_out) launches_out[i] = cnt[i] / steps;
   }
   return k;
+}
+
+nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (variant != 0 && variant != 1) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0 or 1");
+  if (variant == 0 && tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
+    return fail(s, NMHD_ERR_INVALID_ARGUMENT, "tile_rows must be 4, 8 or 16");
+  if (z_chunk < 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "z_chunk must be >= 0");
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
+  drop_graphs(s);
+  s->variant = variant;
+  if (variant == 0) s->shape = nmhd::TileShape{tile_rows, z_chunk};
+  return NMHD_OK;
 }
 
 int nmhd_device(const nmhd_solver *s) { return s ? s->device : -1; }

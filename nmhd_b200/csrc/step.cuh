@@ -56,6 +56,23 @@ void launch_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float 
 void launch_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                    float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
                    cudaStream_t stream);
+// Tile shape of the tiled stage kernels: rows per CTA (4, 8 or 16; the CTA
+// is 32 x ty threads) and z planes per CTA (0: the whole box height).
+struct TileShape {
+  int ty;
+  int zc;
+};
+// One RK stage with the tiled kernels (k_tile_flux + k_tile_ct); unew holds
+// 5 and bflux 6 fields of Sx*Sy*Sz floats.
+void launch_tile_stage(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
+                       float *bflux, float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                       const TileShape &shape, cudaStream_t stream);
+// The two kernels of a tiled stage, separately (for per-kernel timing).
+void launch_tile_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
+                      float *bflux, int in_sel, int half, const TileShape &shape, cudaStream_t stream);
+void launch_tile_ct(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
+                    float *bflux, float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                    const TileShape &shape, cudaStream_t stream);
 void launch_diag(const GridParams &g, StepCtl *ctl, float *w0, float *w1, double *acc,
                  cudaStream_t stream);
 constexpr int kDiagFields = 14;

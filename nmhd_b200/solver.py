@@ -189,6 +189,11 @@ class MHDSolver:
         self.set_time(meta["current_time"], meta["generation"])
         return True
 
+    def set_kernel(self, variant=0, tile_rows=8, z_chunk=16):
+        """Select the kernel variant and tile shape (results are identical)."""
+        _check(self._L, self._h, self._L.nmhd_set_kernel(self._h, int(variant), int(tile_rows),
+                                                         int(z_chunk)))
+
     def profile(self, steps):
         """Mean device time (ms) and launches per step of every kernel class,
         from CUDA events around separately launched kernels."""

@@ -163,3 +163,28 @@ def test_goal_time_semantics(gpu):
         g = sol.generation()
         assert not sol.proceed(1.0, -1.0, 3)
         assert sol.generation() == g + 3
+
+
+@pytest.mark.parametrize("variant,rows,zc", [(1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5), (0, 8, 3)])
+@pytest.mark.parametrize("case", ["ot_ragged", "shear_ragged", "shear_mz"])
+def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
+    """Every kernel variant and tile shape, on boxes whose sizes are not
+    multiples of the tile (partial tiles in x, y and z)."""
+    if case == "ot_ragged":
+        cfg, s = orszag_tang_3d(40, ny=20, nz=13)
+        steps = 12
+    elif case == "shear_ragged":
+        cfg, s = shearing_box(n_radial=12, n_azimuthal=48, n_vertical=7, l_azimuthal=2.0, seed=5)
+        steps = 12
+    else:
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=6)
+        cfg.margin_z, cfg.size_z = 4, 16
+        s = np.concatenate([s[:, -4:], s, s[:, :4]], axis=1)
+        steps = 10
+    o = oracle.proceed(cfg, s, steps)
+    with MHDSolver(cfg) as sol:
+        sol.set_kernel(variant, rows, zc)
+        sol.set_state(s)
+        sol.step(steps)
+        assert sol.current_time() == o["time"]
+        assert_same(sol.get_state(), o["state"])
