@@ -1,0 +1,138 @@
+// Allocation-free entry point: nmhd_advance_noalloc (include/nmhd.h).
+//
+// Some callers cannot call cudaMalloc: code that runs while a CUDA graph is
+// being captured by someone else, a host framework whose allocator owns all
+// device memory, or a real-time loop where a device allocation (and the
+// implicit synchronisation it can bring) is not allowed.  For them this file
+// keeps all the scratch of the tiled time step in one static __device__ array
+// and advances a caller-owned state without allocating anything.
+//
+// The array below is part of this library's device image: every GPU that
+// loads the library holds it (kNoAllocScratchFloats floats, about 28 MB)
+// until the process exits.  All calls share it and it keeps the last call's
+// contents, so calls that overlap on the GPU race; the control block at its
+// start is rewritten by every call.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <string>
+
+#include "../../include/nmhd.h"
+#include "step.cuh"
+
+namespace {
+
+// Largest box (cells including margins) the allocation-free path accepts.
+constexpr long long kNoAllocMaxCells = NMHD_NOALLOC_MAX_CELLS;
+// Control block + dt history, then 27 fields of kNoAllocMaxCells floats:
+// second state buffer (8), predictor (8), conserved update (5), B fluxes (6).
+constexpr size_t kCtlFloats = 256;  // sizeof(StepCtl) rounded up, in floats
+constexpr size_t kNoAllocScratchFloats =
+    kCtlFloats + nmhd::kDtHistCap + 27 * (size_t)kNoAllocMaxCells;
+
+static __device__ __align__(256) float g_noalloc_scratch[kNoAllocScratchFloats];
+
+thread_local std::string g_noalloc_error;
+float *g_scratch_ptr[64] = {nullptr};  // device address of the array, per device
+
+nmhd_status noalloc_fail(nmhd_status st, const std::string &msg) {
+  g_noalloc_error = msg;
+  return st;
+}
+
+}  // namespace
+
+extern "C" const char *nmhd_noalloc_last_error(void) { return g_noalloc_error.c_str(); }
+
+extern "C" nmhd_status nmhd_advance_noalloc(const nmhd_config *cfg, const float *state_in,
+                                            float *state_out, double *time, int64_t *generation,
+                                            double goal_time, int64_t nsteps, int64_t *steps_done,
+                                            void *cuda_stream) {
+  static_assert(sizeof(nmhd::StepCtl) <= kCtlFloats * sizeof(float), "control block too large");
+  if (steps_done) *steps_done = 0;
+  if (!cfg || !state_in || !state_out || !time || !generation || nsteps < 0)
+    return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT, "NULL argument or negative nsteps");
+  if (state_in == state_out)
+    return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT, "state_in and state_out must not alias");
+  const long long cells = (long long)cfg->size_x * cfg->size_y * cfg->size_z;
+  if (cfg->size_x < 1 || cfg->size_y < 1 || cfg->size_z < 1)
+    return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT, "sizes must be >= 1");
+  if (cells > kNoAllocMaxCells)
+    return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT,
+                        "box has " + std::to_string(cells) + " cells; the allocation-free path holds at most " +
+                            std::to_string(kNoAllocMaxCells));
+  if (cfg->margin_y < 0 || cfg->margin_z < 0 || cfg->size_y - 2 * cfg->margin_y < cfg->margin_y ||
+      (cfg->margin_z > 0 && cfg->size_z - 2 * cfg->margin_z < cfg->margin_z) ||
+      !(cfg->gamma > 1.0f) || !(cfg->cfl > 0.0f) || (cfg->space_order != 1 && cfg->space_order != 2) ||
+      (cfg->time_order != 1 && cfg->time_order != 2) ||
+      (cfg->problem != NMHD_PROBLEM_NONE && cfg->problem != NMHD_PROBLEM_SHEARING_BOX))
+    return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT, "invalid configuration");
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return noalloc_fail(NMHD_ERR_CUDA, cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return noalloc_fail(NMHD_ERR_NOT_SUPPORTED, "device index >= 64");
+  // Set-up, once per device with that device current: the host-side name of a
+  // __device__ array is not a device address; ask the runtime for it.
+  if (!g_scratch_ptr[dev]) {
+    void *p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p)
+      return noalloc_fail(NMHD_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    g_scratch_ptr[dev] = static_cast<float *>(p);
+  }
+  float *base = g_scratch_ptr[dev];
+  cudaStream_t st = (cudaStream_t)cuda_stream;
+  const size_t n = (size_t)cells;
+  nmhd::StepCtl *ctl = reinterpret_cast<nmhd::StepCtl *>(base);
+  float *dt_hist = base + kCtlFloats;
+  float *w1 = dt_hist + nmhd::kDtHistCap;
+  float *wp = w1 + 8 * n;
+  float *unew = wp + 8 * n;
+  float *bflux = unew + 5 * n;
+  float *w0 = state_out;
+
+  nmhd::GridParams g = nmhd::derive_grid(*cfg);
+  // Control block: everything that must start at zero starts at zero.
+  nmhd::StepCtl h;
+  std::memset(&h, 0, sizeof(h));
+  h.time = *time;
+  h.generation = *generation;
+  h.cfl_cur = h.cfl_next = 0x7f800000u;
+  h.goal = (float)goal_time;
+  h.hist_cap = nmhd::kDtHistCap;
+  e = cudaMemcpyAsync(ctl, &h, sizeof(h), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(w0, state_in, sizeof(float) * 8 * n, cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return noalloc_fail(NMHD_ERR_CUDA, cudaGetErrorString(e));
+  const nmhd::TileShape shape = {8, 16};
+  nmhd::launch_fill(g, ctl, w0, w1, st);
+  nmhd::launch_cfl_all(g, ctl, w0, w1, st);
+  for (int64_t i = 0; i < nsteps; ++i) {
+    if (g.my > 0 || g.mz > 0) {
+      nmhd::launch_fill(g, ctl, w0, w1, st);
+      nmhd::launch_cfl_margin(g, ctl, w0, w1, st);
+    }
+    if (cfg->time_order == 1) {
+      nmhd::launch_tile_stage(g, ctl, w0, w1, wp, unew, bflux, dt_hist, 0, 1, 0, 1, shape, st);
+    } else {
+      nmhd::launch_tile_stage(g, ctl, w0, w1, wp, unew, bflux, dt_hist, 0, 2, 1, 0, shape, st);
+      nmhd::launch_tile_stage(g, ctl, w0, w1, wp, unew, bflux, dt_hist, 2, 1, 0, 1, shape, st);
+    }
+  }
+  e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(&h, ctl, sizeof(h), cudaMemcpyDeviceToHost, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+  if (e != cudaSuccess) return noalloc_fail(NMHD_ERR_CUDA, cudaGetErrorString(e));
+  // The result is in the current buffer; bring it to state_out if it ended in scratch.
+  if (h.parity == 1) {
+    e = cudaMemcpyAsync(state_out, w1, sizeof(float) * 8 * n, cudaMemcpyDeviceToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return noalloc_fail(NMHD_ERR_CUDA, cudaGetErrorString(e));
+  }
+  if (steps_done) *steps_done = h.generation - *generation;
+  *time = h.time;
+  *generation = h.generation;
+  if (h.status)
+    return noalloc_fail(NMHD_ERR_NUMERICAL, "non-finite state, density <= 0, pressure <= 0 or bad dt");
+  return h.done ? NMHD_GOAL_REACHED : NMHD_STEP_LIMIT;
+}

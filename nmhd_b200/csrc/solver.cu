@@ -60,10 +60,12 @@ nmhd_status cuda_fail(nmhd_solver *s, cudaError_t e, const char *what) {
     if (e_ != cudaSuccess) return cuda_fail(s, e_, #call); \
   } while (0)
 
+}  // namespace
+
 // Derived constants exactly as the reference's float chains produce them
 // (simulation_config_default.h:56-103; relative_velocity of
 // src/application/kepler_disk_demo/mhd_solver.curb:50-52).
-GridParams derive(const nmhd_config &c) {
+GridParams nmhd::derive_grid(const nmhd_config &c) {
   GridParams g;
   g.sx = c.size_x;
   g.sy = c.size_y;
@@ -97,6 +99,8 @@ GridParams derive(const nmhd_config &c) {
   g.order2 = c.space_order != 1;
   return g;
 }
+
+namespace {
 
 nmhd_status validate(const nmhd_config *c, std::string &why) {
   if (!c) { why = "config is NULL"; return NMHD_ERR_INVALID_ARGUMENT; }
@@ -214,7 +218,7 @@ nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
   if (st != NMHD_OK) return fail(nullptr, st, why);
   nmhd_solver *s = new nmhd_solver();
   s->cfg = *cfg;
-  s->g = derive(*cfg);
+  s->g = nmhd::derive_grid(*cfg);
   cudaError_t e = cudaGetDevice(&s->device);
   const size_t n = (size_t)s->g.n;
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking);

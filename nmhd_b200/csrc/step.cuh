@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "../../include/nmhd.h"
+
 namespace nmhd {
 
 // Runtime constants of one box (the reference's simulation_config.h values).
@@ -37,6 +39,9 @@ struct StepCtl {
 };
 
 enum : int { kStatusNumerical = 1, kStatusBadDt = 2 };
+
+// Box constants from a configuration, with the reference's float chains.
+GridParams derive_grid(const nmhd_config &c);
 constexpr int kDtHistCap = 4096;
 constexpr int kFluxFields = 21;  // 3 face directions x 7 flux components
 
