@@ -192,6 +192,15 @@ def run_gpu_arm(args):
     sol = MHDSolver(cfg)
     sol.set_stream(stream.cuda_stream)
     sol.set_state(state)
+    tuning = None
+    if args.kernel:
+        v, rows, zc = (int(t) for t in args.kernel.split(","))
+        sol.set_kernel(v, rows, zc)
+        choice = {"variant": v, "tile_rows": rows, "z_chunk": zc, "source": "--kernel"}
+    else:
+        tuning = sol.autotune(steps=5)
+        best = min(tuning, key=lambda t: t[3])
+        choice = {"variant": best[0], "tile_rows": best[1], "z_chunk": best[2], "source": "autotune"}
     sol.step(args.warmup)
     torch.cuda.synchronize(dev)
 
@@ -262,7 +271,8 @@ def run_gpu_arm(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing-box noise)",
             "config": {"workload": wl, "cells_interior": cells, "cells_with_margins": cfg.cells,
                        "parallelism": "replicas" if world > 1 else "single",
-                       "l2": "working set per step (state x3 + fluxes) > 126 MB L2"},
+                       "l2": "working set per step (state x3 + fluxes) > 126 MB L2",
+                       "kernel": choice},
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
@@ -272,6 +282,8 @@ def run_gpu_arm(args):
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks.summary(),
         }
+        if tuning:
+            line["autotune_ms_per_step"] = {f"v{a}_r{b}_z{c}": round(d, 4) for a, b, c, d in tuning}
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_sample(wl)
         print(json.dumps(line), flush=True)
@@ -288,6 +300,7 @@ def main():
     ap.add_argument("--impl", default="nmhd", choices=["nmhd", "reference"])
     ap.add_argument("--workload", default="mri_shearing_box_128x256x64", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

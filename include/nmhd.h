@@ -140,6 +140,16 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * {4, 8, 16}, z_chunk planes per CTA, 0 = whole height); variant 1: per-cell
  * flux and update kernels.  Every variant gives bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
+/* Autotuner (replaces the reference's Ruby GA/parallel-tempering tuner of
+ * launch dimensions, src/nushio_script/optimization.rb:33-140,
+ * optimization_manager.rb:63-256).  Times `steps` steps of every kernel
+ * variant and tile shape on this solver's box with CUDA events, starting each
+ * trial from the current state, then restores the state and clock and selects
+ * the fastest.  trials_out (may be NULL) receives up to max_trials rows of
+ * (variant, tile_rows, z_chunk, ms_per_step).  Returns the number of rows
+ * written or a negative nmhd_status.  Every candidate gives bitwise the same
+ * result, so tuning never changes the physics. */
+int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials);
 /* Name of kernel class i of nmhd_profile (NULL when out of range). */
 const char *nmhd_kernel_name(int i);
 

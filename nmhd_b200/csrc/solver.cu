@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -567,6 +568,104 @@ nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_ch
   s->variant = variant;
   if (variant == 0) s->shape = nmhd::TileShape{tile_rows, z_chunk};
   return NMHD_OK;
+}
+
+namespace {
+struct TuneKey {
+  int sx, sy, sz, my, mz, problem, so, to;
+  bool operator<(const TuneKey &o) const {
+    return std::tie(sx, sy, sz, my, mz, problem, so, to) <
+           std::tie(o.sx, o.sy, o.sz, o.my, o.mz, o.problem, o.so, o.to);
+  }
+};
+struct TuneChoice {
+  int variant, rows, zc;
+};
+std::map<TuneKey, TuneChoice> g_tune_cache;
+}  // namespace
+
+int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials) {
+  if (!s || steps <= 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  const GridParams &g = s->g;
+  const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order, s->cfg.time_order};
+  std::vector<TuneChoice> cands;
+  cands.push_back({1, 8, 0});
+  for (int rows : {4, 8, 16})
+    for (int zc : {0, 8, 16, 32})
+      if (zc == 0 || zc < g.sz) cands.push_back({0, rows, zc});
+  // save the state and the clock; every trial starts from them
+  StepCtl h0;
+  nmhd_status st = read_ctl(s, h0);
+  if (st != NMHD_OK) return st;
+  const size_t bytes = sizeof(float) * 8 * (size_t)g.n;
+  float *saved = nullptr;
+  NMHD_CUDA(s, cudaMalloc(&saved, bytes));
+  cudaError_t e = cudaMemcpyAsync(saved, current_buffer(s, h0), bytes, cudaMemcpyDeviceToDevice, s->stream);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (e == cudaSuccess) e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  const int saved_variant = s->variant;
+  const nmhd::TileShape saved_shape = s->shape;
+  double best = 1e30;
+  TuneChoice choice = {saved_variant, saved_shape.ty, saved_shape.zc};
+  int written = 0;
+  for (size_t c = 0; c < cands.size() && e == cudaSuccess; ++c) {
+    s->variant = cands[c].variant;
+    s->shape = nmhd::TileShape{cands[c].rows, cands[c].zc};
+    StepCtl h = h0;
+    h.goal = INFINITY;
+    h.done = 0;
+    h.status = 0;
+    h.blocks_done = 0;
+    h.cfl_cur = h.cfl_next = 0x7f800000u;
+    e = cudaMemcpyAsync(s->ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream);
+    if (e == cudaSuccess)
+      e = cudaMemcpyAsync(current_buffer(s, h0), saved, bytes, cudaMemcpyDeviceToDevice, s->stream);
+    if (e != cudaSuccess) break;
+    nmhd::launch_fill(g, s->ctl, s->w0, s->w1, s->stream);
+    nmhd::launch_cfl_all(g, s->ctl, s->w0, s->w1, s->stream);
+    enqueue_step(s);  // warm-up step
+    e = cudaEventRecord(e0, s->stream);
+    for (int i = 0; i < steps && e == cudaSuccess; ++i) enqueue_step(s);
+    if (e == cudaSuccess) e = cudaEventRecord(e1, s->stream);
+    if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+    float ms = 0.f;
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+    if (e != cudaSuccess) break;
+    StepCtl hr;
+    if (cudaMemcpy(&hr, s->ctl, sizeof(hr), cudaMemcpyDeviceToHost) != cudaSuccess || hr.status) continue;
+    const double per = ms / steps;
+    if (trials_out && written < max_trials) {
+      trials_out[4 * written + 0] = cands[c].variant;
+      trials_out[4 * written + 1] = cands[c].rows;
+      trials_out[4 * written + 2] = cands[c].zc;
+      trials_out[4 * written + 3] = per;
+      ++written;
+    }
+    if (per < best) {
+      best = per;
+      choice = cands[c];
+    }
+  }
+  // restore the state, the clock and the CFL of the saved state
+  if (e == cudaSuccess) e = cudaMemcpyAsync(s->ctl, &h0, sizeof(h0), cudaMemcpyHostToDevice, s->stream);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(current_buffer(s, h0), saved, bytes, cudaMemcpyDeviceToDevice, s->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(s->stream);
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  cudaFree(saved);
+  if (e != cudaSuccess) {
+    s->variant = saved_variant;
+    s->shape = saved_shape;
+    return cuda_fail(s, e, "nmhd_autotune");
+  }
+  s->cfl_ready = false;
+  drop_graphs(s);
+  s->variant = choice.variant;
+  s->shape = nmhd::TileShape{choice.rows, choice.zc};
+  g_tune_cache[key] = choice;
+  return written;
 }
 
 int nmhd_device(const nmhd_solver *s) { return s ? s->device : -1; }

@@ -194,6 +194,13 @@ class MHDSolver:
         _check(self._L, self._h, self._L.nmhd_set_kernel(self._h, int(variant), int(tile_rows),
                                                          int(z_chunk)))
 
+    def autotune(self, steps=5):
+        """Time every kernel variant / tile shape on this box and keep the
+        fastest; returns [(variant, tile_rows, z_chunk, ms_per_step), ...]."""
+        out = np.zeros((64, 4), np.float64)
+        k = _check(self._L, self._h, self._L.nmhd_autotune(self._h, int(steps), out.ctypes.data, 64))
+        return [(int(a), int(b), int(c), float(d)) for a, b, c, d in out[:k]]
+
     def profile(self, steps):
         """Mean device time (ms) and launches per step of every kernel class,
         from CUDA events around separately launched kernels."""

@@ -188,3 +188,20 @@ def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
         sol.step(steps)
         assert sol.current_time() == o["time"]
         assert_same(sol.get_state(), o["state"])
+
+
+def test_autotune_restores_state_and_keeps_results_bitwise(gpu):
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=64, n_vertical=16, l_azimuthal=4.0, seed=13)
+    o = oracle.proceed(cfg, s, 6)
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        sol.step(2)
+        mid = sol.get_state()
+        t_mid = sol.current_time()
+        trials = sol.autotune(steps=2)
+        assert len(trials) >= 5
+        assert sol.generation() == 2 and sol.current_time() == t_mid
+        assert_same(sol.get_state(), mid)
+        sol.step(4)
+        assert sol.current_time() == o["time"]
+        assert_same(sol.get_state(), o["state"])
