@@ -136,9 +136,11 @@ const char *nmhd_last_error(const nmhd_solver *s);
 int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max);
 /* Kernel selection (the reference picks launch shapes with its Ruby autotuner,
  * src/application/optimize_mhd, kernel_call() in src/library/mhd_solver.inlrb:24-33).
- * variant 0: tiled kernels (32 x tile_rows cells per CTA, tile_rows in
- * {4, 8, 16}, z_chunk planes per CTA, 0 = whole height); variant 1: per-cell
- * flux and update kernels.  Every variant gives bitwise identical results. */
+ * variant 0: z-marching tiled kernels (32 x tile_rows cells per CTA,
+ * tile_rows in {4, 8, 16}, z_chunk planes per CTA, 0 = whole height);
+ * variant 1: per-cell flux and update kernels on 1-D blocks; variant 2 (the
+ * default): per-cell kernels on 32x4x2 blocks.  tile_rows and z_chunk are
+ * used by variant 0 only.  Every variant gives bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
 /* Autotuner (replaces the reference's Ruby GA/parallel-tempering tuner of
  * launch dimensions, src/nushio_script/optimization.rb:33-140,

@@ -33,7 +33,7 @@ struct nmhd_solver {
   StepCtl *ctl = nullptr;
   double *diag = nullptr;
   bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
-  int variant = 0;         // 0: tiled kernels, 1: per-cell flux + update kernels
+  int variant = 2;         // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks
   nmhd::TileShape shape = {8, 16};
   std::map<int, cudaGraphExec_t> graphs;
   std::string err;
@@ -144,6 +144,10 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
     float *unew = s->flux, *bflux = s->flux + (size_t)5 * g.n;
     nmhd::launch_tile_stage(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
                             half, final_stage, s->shape, st);
+  } else if (s->variant == 2) {
+    nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
+    nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
+                             final_stage, st);
   } else {
     nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                        final_stage, st);
@@ -504,6 +508,8 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
     auto flux_k = [&](int in_sel, int half) {
       if (s->variant == 0)
         nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
+      else if (s->variant == 2)
+        nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
       else
         nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
     };
@@ -511,6 +517,9 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       if (s->variant == 0)
         nmhd::launch_tile_ct(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
                              half, fin, s->shape, q);
+      else if (s->variant == 2)
+        nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel,
+                                 half, fin, q);
       else
         nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                             fin, q);
@@ -559,7 +568,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
 
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk) {
   if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
-  if (variant != 0 && variant != 1) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0 or 1");
+  if (variant < 0 || variant > 2) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0, 1 or 2");
   if (variant == 0 && tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
     return fail(s, NMHD_ERR_INVALID_ARGUMENT, "tile_rows must be 4, 8 or 16");
   if (z_chunk < 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "z_chunk must be >= 0");
@@ -589,6 +598,7 @@ int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials)
   const GridParams &g = s->g;
   const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order, s->cfg.time_order};
   std::vector<TuneChoice> cands;
+  cands.push_back({2, 8, 0});
   cands.push_back({1, 8, 0});
   for (int rows : {4, 8, 16})
     for (int zc : {0, 8, 16, 32})

@@ -72,6 +72,12 @@ struct TileShape {
 void launch_tile_stage(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
                        float *bflux, float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
                        const TileShape &shape, cudaStream_t stream);
+// Per-cell stage kernels with 32x4x2 CTAs (flux: 21 fields of scratch).
+void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                      int in_sel, int half, cudaStream_t stream);
+void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                        float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                        cudaStream_t stream);
 // The two kernels of a tiled stage, separately (for per-kernel timing).
 void launch_tile_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
                       float *bflux, int in_sel, int half, const TileShape &shape, cudaStream_t stream);

@@ -165,7 +165,8 @@ def test_goal_time_semantics(gpu):
         assert sol.generation() == g + 3
 
 
-@pytest.mark.parametrize("variant,rows,zc", [(1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5), (0, 8, 3)])
+@pytest.mark.parametrize("variant,rows,zc", [(2, 8, 0), (1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5),
+                                             (0, 8, 3)])
 @pytest.mark.parametrize("case", ["ot_ragged", "shear_ragged", "shear_mz"])
 def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
     """Every kernel variant and tile shape, on boxes whose sizes are not
