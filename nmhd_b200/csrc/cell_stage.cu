@@ -71,18 +71,19 @@ __device__ __forceinline__ const float *cell_pick(const StepCtl *c, int sel, con
   return (sel == 0) == (c->parity == 0) ? w0 : w1;
 }
 
-// Flux through the lower AX-face of cell o.  s[t] are the offsets of the four
-// stencil cells along AX (-2, -1, 0, +1); t1, t2 the +1 offsets along the two
-// transverse axes (t1 = AX+1, t2 = AX+2 mod 3).  Output: mass, momentum x/y/z
-// (absolute), energy, F(B_t1), F(B_t2).
-template <int AX>
-__device__ __forceinline__ void cell_face(const GridParams &g, const float *__restrict__ w, size_t N,
-                                          int o, const int s[4], int t1, int t2, int yidx, float dt,
-                                          float out[7]) {
-  constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
+// Flux through the lower face of cell o along runtime axis `ax` (one HLLD
+// instance serves all three axes, keeping the kernel's code small).
+// sm/sp: offsets of the stencil cells -2, -1, +1 along ax; t1/t2: +1 offsets
+// along the transverse axes ax+1 and ax+2 (mod 3).  The 7 results go to
+// flux + (7*ax + k)*N + o with momentum in absolute components.
+__device__ __forceinline__ void cell_face_rt(const GridParams &g, const float *__restrict__ w, size_t N,
+                                             int o, int ax, int m2, int m1, int p1, int t1, int t2,
+                                             int yidx, float dt, float *__restrict__ flux) {
+  const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
   const float *rho = w, *p = w + 4 * N;
-  const float *vn = w + (1 + AX) * N, *v1 = w + (1 + E1) * N, *v2 = w + (1 + E2) * N;
-  const float *bn = w + (5 + AX) * N, *b1 = w + (5 + E1) * N, *b2 = w + (5 + E2) * N;
+  const float *vn = w + (1 + ax) * N, *v1 = w + (1 + e1) * N, *v2 = w + (1 + e2) * N;
+  const float *bn = w + (5 + ax) * N, *b1 = w + (5 + e1) * N, *b2 = w + (5 + e2) * N;
+  const int s[4] = {m2, m1, 0, p1};
   float bc1[4], bc2[4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
@@ -92,29 +93,29 @@ __device__ __forceinline__ void cell_face(const GridParams &g, const float *__re
   }
   HlldIn in;
   if (g.order2) {
-    reconstruct4(__ldg(rho + o + s[0]), __ldg(rho + o + s[1]), __ldg(rho + o + s[2]), __ldg(rho + o + s[3]), in.dl, in.dr);
-    reconstruct4(__ldg(vn + o + s[0]), __ldg(vn + o + s[1]), __ldg(vn + o + s[2]), __ldg(vn + o + s[3]), in.ul, in.ur);
-    reconstruct4(__ldg(v1 + o + s[0]), __ldg(v1 + o + s[1]), __ldg(v1 + o + s[2]), __ldg(v1 + o + s[3]), in.vl, in.vr);
-    reconstruct4(__ldg(v2 + o + s[0]), __ldg(v2 + o + s[1]), __ldg(v2 + o + s[2]), __ldg(v2 + o + s[3]), in.wl, in.wr);
-    reconstruct4(__ldg(p + o + s[0]), __ldg(p + o + s[1]), __ldg(p + o + s[2]), __ldg(p + o + s[3]), in.pl, in.pr);
+    reconstruct4(__ldg(rho + o + m2), __ldg(rho + o + m1), __ldg(rho + o), __ldg(rho + o + p1), in.dl, in.dr);
+    reconstruct4(__ldg(vn + o + m2), __ldg(vn + o + m1), __ldg(vn + o), __ldg(vn + o + p1), in.ul, in.ur);
+    reconstruct4(__ldg(v1 + o + m2), __ldg(v1 + o + m1), __ldg(v1 + o), __ldg(v1 + o + p1), in.vl, in.vr);
+    reconstruct4(__ldg(v2 + o + m2), __ldg(v2 + o + m1), __ldg(v2 + o), __ldg(v2 + o + p1), in.wl, in.wr);
+    reconstruct4(__ldg(p + o + m2), __ldg(p + o + m1), __ldg(p + o), __ldg(p + o + p1), in.pl, in.pr);
     reconstruct4(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
     reconstruct4(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
   } else {
-    in.dl = __ldg(rho + o + s[1]); in.dr = __ldg(rho + o);
-    in.ul = __ldg(vn + o + s[1]); in.ur = __ldg(vn + o);
-    in.vl = __ldg(v1 + o + s[1]); in.vr = __ldg(v1 + o);
-    in.wl = __ldg(v2 + o + s[1]); in.wr = __ldg(v2 + o);
-    in.pl = __ldg(p + o + s[1]); in.pr = __ldg(p + o);
+    in.dl = __ldg(rho + o + m1); in.dr = __ldg(rho + o);
+    in.ul = __ldg(vn + o + m1); in.ur = __ldg(vn + o);
+    in.vl = __ldg(v1 + o + m1); in.vr = __ldg(v1 + o);
+    in.wl = __ldg(v2 + o + m1); in.wr = __ldg(v2 + o);
+    in.pl = __ldg(p + o + m1); in.pr = __ldg(p + o);
     in.byl = bc1[1]; in.byr = bc1[2];
     in.bzl = bc2[1]; in.bzr = bc2[2];
   }
   if (g.shear) {
     float acc;
-    if (AX == 0) {
-      const float vY = 0.5f * (__ldg(w + 2 * N + o + s[1]) + __ldg(w + 2 * N + o));
+    if (ax == 0) {
+      const float vY = 0.5f * (__ldg(w + 2 * N + o + m1) + __ldg(w + 2 * N + o));
       acc = -2.0f * g.omega * vY;
-    } else if (AX == 1) {
-      const float vX = 0.5f * (__ldg(w + N + o + s[1]) + __ldg(w + N + o));
+    } else if (ax == 1) {
+      const float vX = 0.5f * (__ldg(w + N + o + m1) + __ldg(w + N + o));
       acc = 2.0f * g.omega * vX + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)yidx + 0.5f));
     } else {
       acc = 0.0f;
@@ -125,18 +126,19 @@ __device__ __forceinline__ void cell_face(const GridParams &g, const float *__re
   }
   float f[7];
   hlld_flux(g.gamma, __ldg(bn + o), in, f);
+  float *out = flux + (size_t)(7 * ax) * N + o;
   out[0] = f[0];
-  out[1 + AX] = f[1];
-  out[1 + E1] = f[2];
-  out[1 + E2] = f[3];
-  out[4] = f[4];
-  out[5] = f[5];
-  out[6] = f[6];
+  out[(1 + ax) * N] = f[1];
+  out[(1 + e1) * N] = f[2];
+  out[(1 + e2) * N] = f[3];
+  out[4 * N] = f[4];
+  out[5 * N] = f[5];
+  out[6 * N] = f[6];
 }
 
 __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const StepCtl *ctl, const float *w0,
-                                                        const float *w1, const float *wp,
-                                                        float *__restrict__ flux, int in_sel, int half) {
+                                                           const float *w1, const float *wp,
+                                                           float *__restrict__ flux, int in_sel, int half) {
   if (ctl->done) return;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
@@ -148,34 +150,31 @@ __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const S
   const size_t N = (size_t)g.n;
   const int o = (z * g.sy + y) * g.sx + x;
   const Offsets f = offsets(g, x, y, z);
-  float out[7];
-  {
-    const int s[4] = {f.xm2, f.xm1, 0, f.xp1};
-    cell_face<0>(g, w, N, o, s, f.yp1, f.zp1, y, dt, out);
-#pragma unroll
-    for (int v = 0; v < 7; ++v) flux[v * N + o] = out[v];
-  }
-  {
-    const int s[4] = {f.ym2, f.ym1, 0, f.yp1};
-    cell_face<1>(g, w, N, o, s, f.zp1, f.xp1, y, dt, out);
-#pragma unroll
-    for (int v = 0; v < 7; ++v) flux[(7 + v) * N + o] = out[v];
-  }
-  {
-    const int s[4] = {f.zm2, f.zm1, 0, f.zp1};
-    cell_face<2>(g, w, N, o, s, f.xp1, f.yp1, y, dt, out);
-#pragma unroll
-    for (int v = 0; v < 7; ++v) flux[(14 + v) * N + o] = out[v];
+#pragma unroll 1
+  for (int ax = 0; ax < 3; ++ax) {
+    const int m2 = ax == 0 ? f.xm2 : ax == 1 ? f.ym2 : f.zm2;
+    const int m1 = ax == 0 ? f.xm1 : ax == 1 ? f.ym1 : f.zm1;
+    const int p1 = ax == 0 ? f.xp1 : ax == 1 ? f.yp1 : f.zp1;
+    const int t1 = ax == 0 ? f.yp1 : ax == 1 ? f.zp1 : f.xp1;
+    const int t2 = ax == 0 ? f.zp1 : ax == 1 ? f.xp1 : f.yp1;
+    cell_face_rt(g, w, N, o, ax, m2, m1, p1, t1, t2, y, dt, flux);
   }
 }
 
-// corner_magnet_flux (mhd_solver.inlrb:641-653) at edge address e; mb, ma are
-// the offsets of -1 along the flux's B component (b) and the flux direction (a).
-__device__ __forceinline__ float cell_corner(const float *__restrict__ vb, const float *__restrict__ fb,
-                                             int e, int mb, int ma) {
-  const float w = __ldg(vb + e) + __ldg(vb + e + mb) + __ldg(vb + e + ma) + __ldg(vb + e + ma + mb);
-  const float f0 = __ldg(fb + e + mb);
-  const float f1 = __ldg(fb + e);
+// Shared-memory staging of the constrained-transport inputs: 6 face-B flux
+// fields and the 3 flux-input velocities on the CTA's cells plus a 1-cell
+// halo: (32+2) x (4+2) x (2+2) cells.
+constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2, HPLANE = HX * HY * HZ;
+enum { S_FXBY = 0, S_FXBZ, S_FYBZ, S_FYBX, S_FZBX, S_FZBY, S_VX, S_VY, S_VZ, S_NF };
+
+// corner_magnet_flux (mhd_solver.inlrb:641-653) from the staged fields: the
+// a-flux of B_b on the edge at staged cell index e (lower a- and b-face
+// index of the edge); mb, ma: index offsets of -1 along b and a.
+__device__ __forceinline__ float corner_s(const float *sm, int fw, int ff, int e, int mb, int ma) {
+  const float *vw = sm + fw * HPLANE, *vf = sm + ff * HPLANE;
+  const float w = vw[e] + vw[e + mb] + vw[e + ma] + vw[e + ma + mb];
+  const float f0 = vf[e + mb];
+  const float f1 = vf[e];
   return w > 0.0f ? f0 : (w < 0.0f ? f1 : 0.5f * (f0 + f1));
 }
 
@@ -197,10 +196,11 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
                                                           float *wp, const float *__restrict__ flux,
                                                           float *dt_hist, int in_sel, int out_sel, int half,
                                                           int final_stage) {
+  __shared__ float sm[S_NF * HPLANE];
   if (ctl->done) return;
-  const int x = blockIdx.x * BX + threadIdx.x;
-  const int y = blockIdx.y * BY + threadIdx.y;
-  const int z = blockIdx.z * BZ + threadIdx.z;
+  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * BZ;
+  const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
   const bool inside = x < g.sx && y < g.sy && z < g.sz;
   const size_t N = (size_t)g.n;
   const float *win = cell_pick(ctl, in_sel, w0, w1, wp);
@@ -208,13 +208,32 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
   float *wo = const_cast<float *>(cell_pick(ctl, out_sel, w0, w1, wp));
   float dt = cell_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
+  const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+  {
+    // stage rows of 34 cells: warp w takes rows w, w+8, ...; lanes cover x
+    const int warp = (tz * BY + ty), lane = tx;
+    const int xa = wrap_any(x0 - 1 + lane, g.sx);
+    const int xb = lane < 2 ? wrap_any(x0 + 31 + lane, g.sx) : 0;
+    for (int row = warp; row < S_NF * HZ * HY; row += kThreads / 32) {
+      const int f = row / (HZ * HY);
+      const int rem = row - f * (HZ * HY);
+      const int kz = rem / HY, jy = rem - kz * HY;
+      const size_t base = ((size_t)wrap_any(z0 - 1 + kz, g.sz) * g.sy + wrap_any(y0 - 1 + jy, g.sy)) * g.sx;
+      // staged field f: B fluxes 5, 6 of face direction f/2, then velocities
+      const float *sp = (f < 6 ? flux + (size_t)(7 * (f >> 1) + 5 + (f & 1)) * N : win + (size_t)(f - 5) * N) + base;
+      float *dp = sm + f * HPLANE + (kz * HY + jy) * HX;
+      dp[lane] = __ldg(sp + xa);
+      if (lane < 2) dp[32 + lane] = __ldg(sp + xb);
+    }
+  }
+  __syncthreads();
   float tcfl = __uint_as_float(0x7f800000u);
   int bad = 0;
   if (inside) {
     const int o = (z * g.sy + y) * g.sx + x;
     const Offsets f = offsets(g, x, y, z);
-    const int xm = f.xm1, xp = f.xp1, ym = f.ym1, yp = f.yp1, zm = f.zm1, zp = f.zp1;
-    const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+    const int xp = f.xp1, yp = f.yp1, zp = f.zp1;
+    // flux divergence of rho, m, E (add_flux_kernel :689-693), x then y then z
     float pace[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -224,32 +243,26 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
       pc = pc + (__ldg(Fz + v * N + o) - __ldg(Fz + v * N + o + zp)) / g.dz;
       pace[v] = pc;
     }
-    const float *vx = win + N, *vy = win + 2 * N, *vz = win + 3 * N;
-    const float *FxBy = Fx + 5 * N, *FxBz = Fx + 6 * N;
-    const float *FyBz = Fy + 5 * N, *FyBx = Fy + 6 * N;
-    const float *FzBx = Fz + 5 * N, *FzBy = Fz + 6 * N;
-    // corner fluxes on the 4 edges of each plane touching the cell's faces
+    // corner EMFs on the 4 edges of each plane touching the cell's faces
+    const int c = ((tz + 1) * HY + (ty + 1)) * HX + (tx + 1);
+    const int DX = 1, DY = HX, DZ = HX * HY;
     float XY[2][2], YX[2][2], XZ[2][2], ZX[2][2], YZ[2][2], ZY[2][2];
 #pragma unroll
     for (int i = 0; i < 2; ++i) {
 #pragma unroll
       for (int j = 0; j < 2; ++j) {
-        const int ex = i ? xp : 0, exm = i ? 0 : xm;    // edge x offset and its -1
-        const int ey = j ? yp : 0, eym = j ? 0 : ym;
-        const int ez = j ? zp : 0, ezm = j ? 0 : zm;
-        const int fy = i ? yp : 0, fym = i ? 0 : ym;
-        // XY (a = x, b = y): mb = -y, ma = -x
-        XY[i][j] = cell_corner(vy, FxBy, o + ex + ey, eym - ey, exm - ex);
-        // YX (a = y, b = x): mb = -x, ma = -y
-        YX[i][j] = cell_corner(vx, FyBx, o + ex + ey, exm - ex, eym - ey);
-        // XZ (a = x, b = z), plane index (x: i, z: j)
-        XZ[i][j] = cell_corner(vz, FxBz, o + ex + ez, ezm - ez, exm - ex);
-        // ZX (a = z, b = x)
-        ZX[i][j] = cell_corner(vx, FzBx, o + ex + ez, exm - ex, ezm - ez);
-        // YZ (a = y, b = z), plane index (y: i, z: j)
-        YZ[i][j] = cell_corner(vz, FyBz, o + fy + ez, ezm - ez, fym - fy);
-        // ZY (a = z, b = y)
-        ZY[i][j] = cell_corner(vy, FzBy, o + fy + ez, fym - fy, ezm - ez);
+        // XY: F_x(B_y), wind v_y, edge (x+i, y+j); mb = -y, ma = -x
+        XY[i][j] = corner_s(sm, S_VY, S_FXBY, c + i * DX + j * DY, -DY, -DX);
+        // YX: F_y(B_x), wind v_x; mb = -x, ma = -y
+        YX[i][j] = corner_s(sm, S_VX, S_FYBX, c + i * DX + j * DY, -DX, -DY);
+        // XZ: F_x(B_z), wind v_z, edge (x+i, z+j); mb = -z, ma = -x
+        XZ[i][j] = corner_s(sm, S_VZ, S_FXBZ, c + i * DX + j * DZ, -DZ, -DX);
+        // ZX: F_z(B_x), wind v_x; mb = -x, ma = -z
+        ZX[i][j] = corner_s(sm, S_VX, S_FZBX, c + i * DX + j * DZ, -DX, -DZ);
+        // YZ: F_y(B_z), wind v_z, edge (y+i, z+j); mb = -z, ma = -y
+        YZ[i][j] = corner_s(sm, S_VZ, S_FYBZ, c + i * DY + j * DZ, -DZ, -DY);
+        // ZY: F_z(B_y), wind v_y; mb = -y, ma = -z
+        ZY[i][j] = corner_s(sm, S_VY, S_FZBY, c + i * DY + j * DZ, -DY, -DZ);
       }
     }
     float pbx[2], pby[2], pbz[2];
@@ -271,6 +284,8 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
       pb = pb + 0.5f * ((ZX[1][k] - ZX[0][k]) / g.dx + (ZY[1][k] - ZY[0][k]) / g.dy);
       pbz[k] = pb;
     }
+    // conserved state before the stage (to_conserved_kernel :762-777), update
+    // (add_pace/update :797-835), primitive recovery (:779-795)
     const float gm1 = g.gamma - 1.0f;
     const float rho0 = wb[o];
     const float vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o], p0 = wb[4 * N + o];
@@ -298,6 +313,7 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
                                 bz[0] * bz[0] + bz[1] * bz[1]);
     const float po = eint * gm1;
     if (g.shear) {
+      // external_acceleration_kernel (:837-848) with the Kepler hook
       const float ax = -2.0f * g.omega * vyo;
       const float ay = 2.0f * g.omega * vxo + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)y + 0.5f));
       vxo = vxo + dt * ax;
@@ -320,22 +336,23 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
       if (!margin_cell) {
         const float b2 = fmaxf(bx[0] * bx[0], bx[1] * bx[1]) + fmaxf(by[0] * by[0], by[1] * by[1]) +
                          fmaxf(bz[0] * bz[0], bz[1] * bz[1]);
-        const float c = sqrtf((g.gamma * po + b2) / rho);
-        tcfl = fminf(fminf(g.cfl * g.dx / fabsf(vxo + c), g.cfl * g.dy / fabsf(vyo + c)),
-                     g.cfl * g.dz / fabsf(vzo + c));
+        const float cs = sqrtf((g.gamma * po + b2) / rho);
+        tcfl = fminf(fminf(g.cfl * g.dx / fabsf(vxo + cs), g.cfl * g.dy / fabsf(vyo + cs)),
+                     g.cfl * g.dz / fabsf(vzo + cs));
       }
     }
   }
   if (!final_stage) return;
   tcfl = cell_block_min(tcfl);
   bad = __syncthreads_or(bad);
-  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
+  if (tx == 0 && ty == 0 && tz == 0) {
     atomicMin(&ctl->cfl_next, __float_as_uint(tcfl));
     if (bad) atomicOr(&ctl->status, kStatusNumerical);
     __threadfence();
     const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
     const unsigned prev = atomicAdd(&ctl->blocks_done, 1u);
     if (prev == nblocks - 1) {
+      // last block: advance the clock (GlobalSetup::proceed, :981) and rotate
       __threadfence();
       bool last;
       const float dts = cell_dt(ctl, &last);
