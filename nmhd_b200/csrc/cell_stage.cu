@@ -10,11 +10,12 @@
 //                 (calc_flux_kernel<X,Y,Z>, src/library/mhd_solver.inlrb:562-636);
 //                 21 flux values per cell (mass, momentum x/y/z, energy, two
 //                 transverse B) go to scratch.
-//  k_cell_update  flux divergence (add_flux_kernel :689-693), corner EMFs and
-//                 face-B update (:641-714), conserved update (:762-835),
-//                 primitive recovery (:779-795), the Kepler kick (:837-848),
-//                 and in the final stage the CFL reduction and clock update
-//                 (:496-521, 870-901, 981).
+//  k_cell_ct      corner EMFs and the face-B update (:641-714), written into
+//                 the output state.
+//  k_cell_prim    flux divergence (add_flux_kernel :689-693), conserved update
+//                 (:762-835), primitive recovery (:779-795), the Kepler kick
+//                 (:837-848), and in the final stage the CFL reduction and
+//                 clock update (:496-521, 870-901, 981).
 //
 // Same arithmetic as the other variants (mhd_math.cuh, -fmad=false): results
 // are bitwise identical.
@@ -161,20 +162,13 @@ __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const S
   }
 }
 
-// Shared-memory staging of the constrained-transport inputs: 6 face-B flux
-// fields and the 3 flux-input velocities on the CTA's cells plus a 1-cell
-// halo: (32+2) x (4+2) x (2+2) cells.
-constexpr int HX = BX + 2, HY = BY + 2, HZ = BZ + 2, HPLANE = HX * HY * HZ;
-enum { S_FXBY = 0, S_FXBZ, S_FYBZ, S_FYBX, S_FZBX, S_FZBY, S_VX, S_VY, S_VZ, S_NF };
-
-// corner_magnet_flux (mhd_solver.inlrb:641-653) from the staged fields: the
-// a-flux of B_b on the edge at staged cell index e (lower a- and b-face
-// index of the edge); mb, ma: index offsets of -1 along b and a.
-__device__ __forceinline__ float corner_s(const float *sm, int fw, int ff, int e, int mb, int ma) {
-  const float *vw = sm + fw * HPLANE, *vf = sm + ff * HPLANE;
-  const float w = vw[e] + vw[e + mb] + vw[e + ma] + vw[e + ma + mb];
-  const float f0 = vf[e + mb];
-  const float f1 = vf[e];
+// corner_magnet_flux (mhd_solver.inlrb:641-653) at edge address e: the
+// a-flux of B_b; mb, ma are the offsets of -1 along b and along a.
+__device__ __forceinline__ float cell_corner(const float *__restrict__ vb, const float *__restrict__ fb,
+                                             int e, int mb, int ma) {
+  const float w = __ldg(vb + e) + __ldg(vb + e + mb) + __ldg(vb + e + ma) + __ldg(vb + e + ma + mb);
+  const float f0 = __ldg(fb + e + mb);
+  const float f1 = __ldg(fb + e);
   return w > 0.0f ? f0 : (w < 0.0f ? f1 : 0.5f * (f0 + f1));
 }
 
@@ -192,48 +186,101 @@ __device__ __forceinline__ float cell_block_min(float v) {
   return v;
 }
 
-__global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl *ctl, float *w0, float *w1,
-                                                          float *wp, const float *__restrict__ flux,
-                                                          float *dt_hist, int in_sel, int out_sel, int half,
-                                                          int final_stage) {
-  __shared__ float sm[S_NF * HPLANE];
+// Constrained transport of one stage (add_flux_kernel's B part,
+// mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
+// new face B on the cell's lower x-, y- and z-face, written into the output
+// state.  18 corner EMFs per cell.
+__global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
+                                                         float *w1, float *wp,
+                                                         const float *__restrict__ flux, int in_sel,
+                                                         int out_sel, int half) {
   if (ctl->done) return;
-  const int tx = threadIdx.x, ty = threadIdx.y, tz = threadIdx.z;
-  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * BZ;
-  const int x = x0 + tx, y = y0 + ty, z = z0 + tz;
-  const bool inside = x < g.sx && y < g.sy && z < g.sz;
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int y = blockIdx.y * BY + threadIdx.y;
+  const int z = blockIdx.z * BZ + threadIdx.z;
+  if (x >= g.sx || y >= g.sy || z >= g.sz) return;
   const size_t N = (size_t)g.n;
   const float *win = cell_pick(ctl, in_sel, w0, w1, wp);
   const float *wb = cell_pick(ctl, 0, w0, w1, wp);
   float *wo = const_cast<float *>(cell_pick(ctl, out_sel, w0, w1, wp));
   float dt = cell_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
-  const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
-  {
-    // stage rows of 34 cells: warp w takes rows w, w+8, ...; lanes cover x
-    const int warp = (tz * BY + ty), lane = tx;
-    const int xa = wrap_any(x0 - 1 + lane, g.sx);
-    const int xb = lane < 2 ? wrap_any(x0 + 31 + lane, g.sx) : 0;
-    for (int row = warp; row < S_NF * HZ * HY; row += kThreads / 32) {
-      const int f = row / (HZ * HY);
-      const int rem = row - f * (HZ * HY);
-      const int kz = rem / HY, jy = rem - kz * HY;
-      const size_t base = ((size_t)wrap_any(z0 - 1 + kz, g.sz) * g.sy + wrap_any(y0 - 1 + jy, g.sy)) * g.sx;
-      // staged field f: B fluxes 5, 6 of face direction f/2, then velocities
-      const float *sp = (f < 6 ? flux + (size_t)(7 * (f >> 1) + 5 + (f & 1)) * N : win + (size_t)(f - 5) * N) + base;
-      float *dp = sm + f * HPLANE + (kz * HY + jy) * HX;
-      dp[lane] = __ldg(sp + xa);
-      if (lane < 2) dp[32 + lane] = __ldg(sp + xb);
-    }
-  }
-  __syncthreads();
+  const int o = (z * g.sy + y) * g.sx + x;
+  const Offsets f = offsets(g, x, y, z);
+  const int xm = f.xm1, xp = f.xp1, ym = f.ym1, yp = f.yp1, zm = f.zm1, zp = f.zp1;
+  const float *vx = win + N, *vy = win + 2 * N, *vz = win + 3 * N;
+  const float *FxBy = flux + 5 * N, *FxBz = flux + 6 * N;
+  const float *FyBz = flux + 12 * N, *FyBx = flux + 13 * N;
+  const float *FzBx = flux + 19 * N, *FzBy = flux + 20 * N;
+  // corners at the cell's edge (00) and the edges one step up each in-plane axis
+  // XY: F_x(B_y) with wind v_y, edges (x, y), (x, y+1), (x+1, y)
+  const float XY00 = cell_corner(vy, FxBy, o, ym, xm);
+  const float XY01 = cell_corner(vy, FxBy, o + yp, -yp, xm);
+  const float XY10 = cell_corner(vy, FxBy, o + xp, ym, -xp);
+  // YX: F_y(B_x) with wind v_x
+  const float YX00 = cell_corner(vx, FyBx, o, xm, ym);
+  const float YX01 = cell_corner(vx, FyBx, o + yp, xm, -yp);
+  const float YX10 = cell_corner(vx, FyBx, o + xp, -xp, ym);
+  // XZ: F_x(B_z) with wind v_z, edges (x, z), (x, z+1), (x+1, z)
+  const float XZ00 = cell_corner(vz, FxBz, o, zm, xm);
+  const float XZ01 = cell_corner(vz, FxBz, o + zp, -zp, xm);
+  const float XZ10 = cell_corner(vz, FxBz, o + xp, zm, -xp);
+  // ZX: F_z(B_x) with wind v_x
+  const float ZX00 = cell_corner(vx, FzBx, o, xm, zm);
+  const float ZX01 = cell_corner(vx, FzBx, o + zp, xm, -zp);
+  const float ZX10 = cell_corner(vx, FzBx, o + xp, -xp, zm);
+  // YZ: F_y(B_z) with wind v_z, edges (y, z), (y, z+1), (y+1, z)
+  const float YZ00 = cell_corner(vz, FyBz, o, zm, ym);
+  const float YZ01 = cell_corner(vz, FyBz, o + zp, -zp, ym);
+  const float YZ10 = cell_corner(vz, FyBz, o + yp, zm, -yp);
+  // ZY: F_z(B_y) with wind v_y
+  const float ZY00 = cell_corner(vy, FzBy, o, ym, zm);
+  const float ZY01 = cell_corner(vy, FzBy, o + zp, ym, -zp);
+  const float ZY10 = cell_corner(vy, FzBy, o + yp, -yp, zm);
+  float pb = 0.0f;
+  pb = pb + 0.5f * ((XY01 - XY00) / g.dy + (XZ01 - XZ00) / g.dz);
+  pb = pb - 0.5f * (YX01 - YX00) / g.dy;
+  pb = pb - 0.5f * (ZX01 - ZX00) / g.dz;
+  wo[5 * N + o] = wb[5 * N + o] + dt * pb;
+  pb = 0.0f;
+  pb = pb - 0.5f * (XY10 - XY00) / g.dx;
+  pb = pb + 0.5f * ((YZ01 - YZ00) / g.dz + (YX10 - YX00) / g.dx);
+  pb = pb - 0.5f * (ZY01 - ZY00) / g.dz;
+  wo[6 * N + o] = wb[6 * N + o] + dt * pb;
+  pb = 0.0f;
+  pb = pb - 0.5f * (XZ10 - XZ00) / g.dx;
+  pb = pb - 0.5f * (YZ10 - YZ00) / g.dy;
+  pb = pb + 0.5f * ((ZX10 - ZX00) / g.dx + (ZY10 - ZY00) / g.dy);
+  wo[7 * N + o] = wb[7 * N + o] + dt * pb;
+}
+
+// Rest of the stage: flux divergence of rho, m, E (mhd_solver.inlrb:689-693),
+// conserved state before the stage (to_conserved :762-777), update
+// (add_pace/update :797-835), primitive recovery with the new face B
+// (:779-795), the Kepler kick (:837-848) and, in the final stage, the CFL
+// reduction and clock update (:496-521, 870-901, 981).
+__global__ void __launch_bounds__(kThreads, 4) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
+                                                           float *w1, float *wp,
+                                                           const float *__restrict__ flux, float *dt_hist,
+                                                           int out_sel, int half, int final_stage) {
+  if (ctl->done) return;
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int y = blockIdx.y * BY + threadIdx.y;
+  const int z = blockIdx.z * BZ + threadIdx.z;
+  const bool inside = x < g.sx && y < g.sy && z < g.sz;
+  const size_t N = (size_t)g.n;
+  const float *wb = cell_pick(ctl, 0, w0, w1, wp);
+  float *wo = const_cast<float *>(cell_pick(ctl, out_sel, w0, w1, wp));
+  float dt = cell_dt(ctl, nullptr);
+  if (half) dt = dt / 2.0f;
   float tcfl = __uint_as_float(0x7f800000u);
   int bad = 0;
   if (inside) {
     const int o = (z * g.sy + y) * g.sx + x;
-    const Offsets f = offsets(g, x, y, z);
-    const int xp = f.xp1, yp = f.yp1, zp = f.zp1;
-    // flux divergence of rho, m, E (add_flux_kernel :689-693), x then y then z
+    const int xp = x + 1 < g.sx ? 1 : 1 - g.sx;
+    const int yp = (y + 1 < g.sy ? 1 : 1 - g.sy) * g.sx;
+    const int zp = (z + 1 < g.sz ? 1 : 1 - g.sz) * g.sx * g.sy;
+    const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
     float pace[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
@@ -243,77 +290,29 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
       pc = pc + (__ldg(Fz + v * N + o) - __ldg(Fz + v * N + o + zp)) / g.dz;
       pace[v] = pc;
     }
-    // corner EMFs on the 4 edges of each plane touching the cell's faces
-    const int c = ((tz + 1) * HY + (ty + 1)) * HX + (tx + 1);
-    const int DX = 1, DY = HX, DZ = HX * HY;
-    float XY[2][2], YX[2][2], XZ[2][2], ZX[2][2], YZ[2][2], ZY[2][2];
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-#pragma unroll
-      for (int j = 0; j < 2; ++j) {
-        // XY: F_x(B_y), wind v_y, edge (x+i, y+j); mb = -y, ma = -x
-        XY[i][j] = corner_s(sm, S_VY, S_FXBY, c + i * DX + j * DY, -DY, -DX);
-        // YX: F_y(B_x), wind v_x; mb = -x, ma = -y
-        YX[i][j] = corner_s(sm, S_VX, S_FYBX, c + i * DX + j * DY, -DX, -DY);
-        // XZ: F_x(B_z), wind v_z, edge (x+i, z+j); mb = -z, ma = -x
-        XZ[i][j] = corner_s(sm, S_VZ, S_FXBZ, c + i * DX + j * DZ, -DZ, -DX);
-        // ZX: F_z(B_x), wind v_x; mb = -x, ma = -z
-        ZX[i][j] = corner_s(sm, S_VX, S_FZBX, c + i * DX + j * DZ, -DX, -DZ);
-        // YZ: F_y(B_z), wind v_z, edge (y+i, z+j); mb = -z, ma = -y
-        YZ[i][j] = corner_s(sm, S_VZ, S_FYBZ, c + i * DY + j * DZ, -DZ, -DY);
-        // ZY: F_z(B_y), wind v_y; mb = -y, ma = -z
-        ZY[i][j] = corner_s(sm, S_VY, S_FZBY, c + i * DY + j * DZ, -DY, -DZ);
-      }
-    }
-    float pbx[2], pby[2], pbz[2];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      float pb = 0.0f;
-      pb = pb + 0.5f * ((XY[k][1] - XY[k][0]) / g.dy + (XZ[k][1] - XZ[k][0]) / g.dz);
-      pb = pb - 0.5f * (YX[k][1] - YX[k][0]) / g.dy;
-      pb = pb - 0.5f * (ZX[k][1] - ZX[k][0]) / g.dz;
-      pbx[k] = pb;
-      pb = 0.0f;
-      pb = pb - 0.5f * (XY[1][k] - XY[0][k]) / g.dx;
-      pb = pb + 0.5f * ((YZ[k][1] - YZ[k][0]) / g.dz + (YX[1][k] - YX[0][k]) / g.dx);
-      pb = pb - 0.5f * (ZY[k][1] - ZY[k][0]) / g.dz;
-      pby[k] = pb;
-      pb = 0.0f;
-      pb = pb - 0.5f * (XZ[1][k] - XZ[0][k]) / g.dx;
-      pb = pb - 0.5f * (YZ[1][k] - YZ[0][k]) / g.dy;
-      pb = pb + 0.5f * ((ZX[1][k] - ZX[0][k]) / g.dx + (ZY[1][k] - ZY[0][k]) / g.dy);
-      pbz[k] = pb;
-    }
-    // conserved state before the stage (to_conserved_kernel :762-777), update
-    // (add_pace/update :797-835), primitive recovery (:779-795)
     const float gm1 = g.gamma - 1.0f;
     const float rho0 = wb[o];
     const float vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o], p0 = wb[4 * N + o];
-    float bx[2] = {wb[5 * N + o], wb[5 * N + o + xp]};
-    float by[2] = {wb[6 * N + o], wb[6 * N + o + yp]};
-    float bz[2] = {wb[7 * N + o], wb[7 * N + o + zp]};
+    const float bxl = wb[5 * N + o], bxh = wb[5 * N + o + xp];
+    const float byl = wb[6 * N + o], byh = wb[6 * N + o + yp];
+    const float bzl = wb[7 * N + o], bzh = wb[7 * N + o + zp];
     const float mx0 = rho0 * vx0, my0 = rho0 * vy0, mz0 = rho0 * vz0;
     const float e0 = p0 / gm1 + 0.5f * rho0 * (vx0 * vx0 + vy0 * vy0 + vz0 * vz0) +
-                     0.25f * (bx[0] * bx[0] + bx[1] * bx[1] + by[0] * by[0] + by[1] * by[1] +
-                              bz[0] * bz[0] + bz[1] * bz[1]);
+                     0.25f * (bxl * bxl + bxh * bxh + byl * byl + byh * byh + bzl * bzl + bzh * bzh);
     const float rho = rho0 + dt * pace[0];
     const float mx = mx0 + dt * pace[1];
     const float my = my0 + dt * pace[2];
     const float mz = mz0 + dt * pace[3];
     const float ene = e0 + dt * pace[4];
-#pragma unroll
-    for (int k = 0; k < 2; ++k) {
-      bx[k] = bx[k] + dt * pbx[k];
-      by[k] = by[k] + dt * pby[k];
-      bz[k] = bz[k] + dt * pbz[k];
-    }
+    // new face B from k_cell_ct (this cell's lower faces and its neighbours')
+    const float bx0 = wo[5 * N + o], bx1 = wo[5 * N + o + xp];
+    const float by0 = wo[6 * N + o], by1 = wo[6 * N + o + yp];
+    const float bz0 = wo[7 * N + o], bz1 = wo[7 * N + o + zp];
     float vxo = mx / rho, vyo = my / rho, vzo = mz / rho;
     const float eint = ene - 0.5f * (mx * mx + my * my + mz * mz) / rho -
-                       0.25f * (bx[0] * bx[0] + bx[1] * bx[1] + by[0] * by[0] + by[1] * by[1] +
-                                bz[0] * bz[0] + bz[1] * bz[1]);
+                       0.25f * (bx0 * bx0 + bx1 * bx1 + by0 * by0 + by1 * by1 + bz0 * bz0 + bz1 * bz1);
     const float po = eint * gm1;
     if (g.shear) {
-      // external_acceleration_kernel (:837-848) with the Kepler hook
       const float ax = -2.0f * g.omega * vyo;
       const float ay = 2.0f * g.omega * vxo + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)y + 0.5f));
       vxo = vxo + dt * ax;
@@ -325,17 +324,13 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
     wo[2 * N + o] = vyo;
     wo[3 * N + o] = vzo;
     wo[4 * N + o] = po;
-    wo[5 * N + o] = bx[0];
-    wo[6 * N + o] = by[0];
-    wo[7 * N + o] = bz[0];
     if (final_stage) {
       bad = !(rho > 0.0f) || !(po > 0.0f) || !isfinite(vxo) || !isfinite(vyo) || !isfinite(vzo) ||
-            !isfinite(bx[0]) || !isfinite(by[0]) || !isfinite(bz[0]);
+            !isfinite(bx0) || !isfinite(by0) || !isfinite(bz0);
       const bool margin_cell = (y < g.my) || (y >= g.sy - g.my) ||
                                (g.mz > 0 && (z < g.mz || z >= g.sz - g.mz - 1));
       if (!margin_cell) {
-        const float b2 = fmaxf(bx[0] * bx[0], bx[1] * bx[1]) + fmaxf(by[0] * by[0], by[1] * by[1]) +
-                         fmaxf(bz[0] * bz[0], bz[1] * bz[1]);
+        const float b2 = fmaxf(bx0 * bx0, bx1 * bx1) + fmaxf(by0 * by0, by1 * by1) + fmaxf(bz0 * bz0, bz1 * bz1);
         const float cs = sqrtf((g.gamma * po + b2) / rho);
         tcfl = fminf(fminf(g.cfl * g.dx / fabsf(vxo + cs), g.cfl * g.dy / fabsf(vyo + cs)),
                      g.cfl * g.dz / fabsf(vzo + cs));
@@ -345,7 +340,7 @@ __global__ void __launch_bounds__(kThreads) k_cell_update(GridParams g, StepCtl 
   if (!final_stage) return;
   tcfl = cell_block_min(tcfl);
   bad = __syncthreads_or(bad);
-  if (tx == 0 && ty == 0 && tz == 0) {
+  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
     atomicMin(&ctl->cfl_next, __float_as_uint(tcfl));
     if (bad) atomicOr(&ctl->status, kStatusNumerical);
     __threadfence();
@@ -384,8 +379,9 @@ void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, f
 
 void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                         float *dt_hist, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
-  k_cell_update<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel,
-                                                           out_sel, half, final_stage);
+  k_cell_ct<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
+  k_cell_prim<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel, half,
+                                                         final_stage);
 }
 
 }  // namespace nmhd
