@@ -56,6 +56,13 @@ __device__ __forceinline__ Offsets offsets(const GridParams &g, int x, int y, in
   return f;
 }
 
+// x / d for a grid spacing d; with power-of-two spacings the product with the
+// exact reciprocal is the same float.
+template <bool kPow2>
+__device__ __forceinline__ float divs(float x, float d, float inv) {
+  return kPow2 ? x * inv : x / d;
+}
+
 __device__ __forceinline__ float cell_dt(const StepCtl *c, bool *last) {
   const float cmin = __uint_as_float(c->cfl_cur);
   float dt = fminf(c->goal, cmin);
@@ -190,6 +197,7 @@ __device__ __forceinline__ float cell_block_min(float v) {
 // mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
 // new face B on the cell's lower x-, y- and z-face, written into the output
 // state.  18 corner EMFs per cell.
+template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
                                                          float *w1, float *wp,
                                                          const float *__restrict__ flux, int in_sel,
@@ -237,20 +245,21 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const Ste
   const float ZY00 = cell_corner(vy, FzBy, o, ym, zm);
   const float ZY01 = cell_corner(vy, FzBy, o + zp, ym, -zp);
   const float ZY10 = cell_corner(vy, FzBy, o + yp, -yp, zm);
+  const float dx = g.dx, dy = g.dy, dz = g.dz, ix = g.inv_dx, iy = g.inv_dy, iz = g.inv_dz;
   float pb = 0.0f;
-  pb = pb + 0.5f * ((XY01 - XY00) / g.dy + (XZ01 - XZ00) / g.dz);
-  pb = pb - 0.5f * (YX01 - YX00) / g.dy;
-  pb = pb - 0.5f * (ZX01 - ZX00) / g.dz;
+  pb = pb + 0.5f * (divs<kPow2>(XY01 - XY00, dy, iy) + divs<kPow2>(XZ01 - XZ00, dz, iz));
+  pb = pb - divs<kPow2>(0.5f * (YX01 - YX00), dy, iy);
+  pb = pb - divs<kPow2>(0.5f * (ZX01 - ZX00), dz, iz);
   wo[5 * N + o] = wb[5 * N + o] + dt * pb;
   pb = 0.0f;
-  pb = pb - 0.5f * (XY10 - XY00) / g.dx;
-  pb = pb + 0.5f * ((YZ01 - YZ00) / g.dz + (YX10 - YX00) / g.dx);
-  pb = pb - 0.5f * (ZY01 - ZY00) / g.dz;
+  pb = pb - divs<kPow2>(0.5f * (XY10 - XY00), dx, ix);
+  pb = pb + 0.5f * (divs<kPow2>(YZ01 - YZ00, dz, iz) + divs<kPow2>(YX10 - YX00, dx, ix));
+  pb = pb - divs<kPow2>(0.5f * (ZY01 - ZY00), dz, iz);
   wo[6 * N + o] = wb[6 * N + o] + dt * pb;
   pb = 0.0f;
-  pb = pb - 0.5f * (XZ10 - XZ00) / g.dx;
-  pb = pb - 0.5f * (YZ10 - YZ00) / g.dy;
-  pb = pb + 0.5f * ((ZX10 - ZX00) / g.dx + (ZY10 - ZY00) / g.dy);
+  pb = pb - divs<kPow2>(0.5f * (XZ10 - XZ00), dx, ix);
+  pb = pb - divs<kPow2>(0.5f * (YZ10 - YZ00), dy, iy);
+  pb = pb + 0.5f * (divs<kPow2>(ZX10 - ZX00, dx, ix) + divs<kPow2>(ZY10 - ZY00, dy, iy));
   wo[7 * N + o] = wb[7 * N + o] + dt * pb;
 }
 
@@ -259,7 +268,8 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const Ste
 // (add_pace/update :797-835), primitive recovery with the new face B
 // (:779-795), the Kepler kick (:837-848) and, in the final stage, the CFL
 // reduction and clock update (:496-521, 870-901, 981).
-__global__ void __launch_bounds__(kThreads, 4) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
+template <bool kPow2>
+__global__ void __launch_bounds__(kThreads, 3) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
                                                            float *w1, float *wp,
                                                            const float *__restrict__ flux, float *dt_hist,
                                                            int out_sel, int half, int final_stage) {
@@ -281,13 +291,24 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_prim(GridParams g, StepCtl
     const int yp = (y + 1 < g.sy ? 1 : 1 - g.sy) * g.sx;
     const int zp = (z + 1 < g.sz ? 1 : 1 - g.sz) * g.sx * g.sy;
     const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+    // all loads first: 30 face fluxes, the state before the stage, new face B
+    float fl[5][6];
+#pragma unroll
+    for (int v = 0; v < 5; ++v) {
+      fl[v][0] = __ldg(Fx + v * N + o);
+      fl[v][1] = __ldg(Fx + v * N + o + xp);
+      fl[v][2] = __ldg(Fy + v * N + o);
+      fl[v][3] = __ldg(Fy + v * N + o + yp);
+      fl[v][4] = __ldg(Fz + v * N + o);
+      fl[v][5] = __ldg(Fz + v * N + o + zp);
+    }
     float pace[5];
 #pragma unroll
     for (int v = 0; v < 5; ++v) {
       float pc = 0.0f;
-      pc = pc + (__ldg(Fx + v * N + o) - __ldg(Fx + v * N + o + xp)) / g.dx;
-      pc = pc + (__ldg(Fy + v * N + o) - __ldg(Fy + v * N + o + yp)) / g.dy;
-      pc = pc + (__ldg(Fz + v * N + o) - __ldg(Fz + v * N + o + zp)) / g.dz;
+      pc = pc + divs<kPow2>(fl[v][0] - fl[v][1], g.dx, g.inv_dx);
+      pc = pc + divs<kPow2>(fl[v][2] - fl[v][3], g.dy, g.inv_dy);
+      pc = pc + divs<kPow2>(fl[v][4] - fl[v][5], g.dz, g.inv_dz);
       pace[v] = pc;
     }
     const float gm1 = g.gamma - 1.0f;
@@ -379,9 +400,15 @@ void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, f
 
 void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                         float *dt_hist, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
-  k_cell_ct<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
-  k_cell_prim<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel, half,
-                                                         final_stage);
+  if (g.pow2_spacing) {
+    k_cell_ct<true><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
+    k_cell_prim<true><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel,
+                                                               half, final_stage);
+  } else {
+    k_cell_ct<false><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
+    k_cell_prim<false><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel,
+                                                                half, final_stage);
+  }
 }
 
 }  // namespace nmhd

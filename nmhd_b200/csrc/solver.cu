@@ -98,6 +98,14 @@ GridParams nmhd::derive_grid(const nmhd_config &c) {
   g.rel_vel = (double)rv;
   g.shear = c.problem == NMHD_PROBLEM_SHEARING_BOX;
   g.order2 = c.space_order != 1;
+  auto pow2 = [](float v) {
+    int e;
+    return v > 0.0f && std::isfinite(v) && std::frexp(v, &e) == 0.5f && e > -125 && e < 126;
+  };
+  g.pow2_spacing = pow2(g.dx) && pow2(g.dy) && pow2(g.dz);
+  g.inv_dx = 1.0f / g.dx;
+  g.inv_dy = 1.0f / g.dy;
+  g.inv_dz = 1.0f / g.dz;
   return g;
 }
 

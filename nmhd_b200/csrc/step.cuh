@@ -20,6 +20,10 @@ struct GridParams {
   double rel_vel;  // relative_velocity(): -q*Omega*kLocalExtentY
   int shear;       // shearing box: Kepler acceleration + shearing-periodic Y margins
   int order2;      // minbee (2) vs piecewise-constant (1) reconstruction
+  // 1/dx, 1/dy, 1/dz; when all three spacings are powers of two (pow2_spacing),
+  // x / d == x * (1/d) exactly and kernels may multiply instead of divide.
+  float inv_dx, inv_dy, inv_dz;
+  int pow2_spacing;
 };
 
 // Device-resident step control.  The time step is a pure function of
