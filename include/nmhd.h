@@ -182,6 +182,29 @@ nmhd_status nmhd_advance_noalloc(const nmhd_config *cfg, const float *state_in, 
                                  int64_t *steps_done, void *cuda_stream);
 const char *nmhd_noalloc_last_error(void);
 
+/* ---- Batched ensemble -------------------------------------------------------
+ * Many independent boxes of uneven sizes (e.g. an ensemble over beta, shear
+ * and seed) advanced together.  No counterpart in the reference, which runs
+ * one compile-time box per process.  Every box has its own configuration,
+ * state, clock and CFL time step (reduced per box), and is advanced bitwise as
+ * nmhd_proceed would advance it alone.  Each kernel of a step is one
+ * persistent launch over all boxes; batches of steps are one CUDA graph.
+ * Batched boxes use time_order 2 and no Z margins. */
+typedef struct nmhd_batch nmhd_batch;
+nmhd_status nmhd_batch_create(const nmhd_config *boxes, int n, nmhd_batch **out);
+void nmhd_batch_destroy(nmhd_batch *b);
+int nmhd_batch_size(const nmhd_batch *b);
+/* State of box `box`, as nmhd_set_state/nmhd_get_state. */
+nmhd_status nmhd_batch_set_state(nmhd_batch *b, int box, const float *const fields[8], int on_device);
+nmhd_status nmhd_batch_get_state(nmhd_batch *b, int box, float *const fields[8], int on_device);
+/* Clock of box `box` (current_time, generation). */
+nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *generation);
+/* Advances every box until all reach goal_time or max_steps steps are done
+ * (semantics of nmhd_proceed, per box; a box that reached the goal waits).
+ * *steps_done: steps taken by the box that took most. */
+nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
+const char *nmhd_batch_last_error(const nmhd_batch *b);
+
 /* Library version string. */
 const char *nmhd_version(void);
 

@@ -50,6 +50,16 @@ _SIGS = [
                                             ctypes.POINTER(ctypes.c_int64), ctypes.c_double,
                                             ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), _P]),
     ("nmhd_noalloc_last_error", ctypes.c_char_p, []),
+    ("nmhd_batch_create", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
+    ("nmhd_batch_destroy", None, [_P]),
+    ("nmhd_batch_size", ctypes.c_int, [_P]),
+    ("nmhd_batch_set_state", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_batch_get_state", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_batch_clock", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
+                                        ctypes.POINTER(ctypes.c_int64)]),
+    ("nmhd_batch_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64,
+                                          ctypes.POINTER(ctypes.c_int64)]),
+    ("nmhd_batch_last_error", ctypes.c_char_p, [_P]),
 ]
 EXPORTS = [s[0] for s in _SIGS]
 

@@ -1,0 +1,95 @@
+"""Batched ensemble of independent boxes (nmhd_batch_* in include/nmhd.h).
+
+Every box keeps its own configuration, state, clock and CFL time step; all
+boxes advance together, one persistent launch per kernel per stage.  A box
+advanced in a batch is bitwise the box advanced alone by
+:class:`~nmhd_b200.solver.MHDSolver`.
+"""
+from __future__ import annotations
+
+import ctypes
+import math
+
+import numpy as np
+
+from . import _lib
+
+
+class BatchSolver:
+    def __init__(self, configs):
+        self.configs = list(configs)
+        self._L = _lib.lib()
+        arr = (type(self.configs[0].to_ctypes()) * len(self.configs))(
+            *[c.to_ctypes() for c in self.configs])
+        self._arr = arr
+        h = ctypes.c_void_p()
+        code = self._L.nmhd_batch_create(arr, len(self.configs), ctypes.byref(h))
+        if code != 0:
+            raise _lib.NmhdError(code, self._L.nmhd_batch_last_error(None).decode())
+        self._h = h
+
+    def _check(self, code):
+        if code < 0:
+            raise _lib.NmhdError(code, self._L.nmhd_batch_last_error(self._h).decode())
+        return code
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.nmhd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return len(self.configs)
+
+    def _ptrs(self, i, arr):
+        n = self.configs[i].cells
+        base = arr.ctypes.data
+        return (ctypes.c_void_p * 8)(*[base + 4 * n * v for v in range(8)])
+
+    def set_state(self, i, state):
+        st = np.ascontiguousarray(state, dtype=np.float32)
+        if st.shape != (8,) + self.configs[i].shape:
+            raise ValueError(f"box {i}: state shape {st.shape} != {(8,) + self.configs[i].shape}")
+        self._check(self._L.nmhd_batch_set_state(self._h, i, self._ptrs(i, st), 0))
+
+    def get_state(self, i):
+        out = np.empty((8,) + self.configs[i].shape, dtype=np.float32)
+        self._check(self._L.nmhd_batch_get_state(self._h, i, self._ptrs(i, out), 0))
+        return out
+
+    def clock(self, i):
+        t = ctypes.c_double()
+        g = ctypes.c_int64()
+        self._check(self._L.nmhd_batch_clock(self._h, i, ctypes.byref(t), ctypes.byref(g)))
+        return t.value, g.value
+
+    def proceed(self, goal_time=math.inf, max_steps=0):
+        done = ctypes.c_int64()
+        code = self._check(self._L.nmhd_batch_proceed(self._h, float(goal_time), int(max_steps),
+                                                      ctypes.byref(done)))
+        self.last_steps = done.value
+        return code == _lib.GOAL_REACHED
+
+    def step(self, nsteps):
+        self.proceed(math.inf, nsteps)
+        return self.last_steps
+
+    @property
+    def cells(self):
+        return sum(c.cells for c in self.configs)
+
+    @property
+    def interior_cells(self):
+        return sum(c.interior_cells for c in self.configs)

@@ -1,0 +1,457 @@
+// Batched ensemble: many independent boxes of uneven sizes advanced together.
+//
+// No counterpart in the reference (one box per process, sizes fixed at compile
+// time).  Every box keeps its own configuration, state buffers, control block
+// (clock, CFL minimum, status) and therefore its own time step from its own CFL
+// reduction.  Each kernel of a step is ONE persistent launch over all boxes: a
+// CTA walks a flattened list of 32 x 4 x 2-cell tiles, finds the tile's box in
+// a descriptor table and runs the same per-cell code as the single-box path
+// (cell_ops.cuh, margin_ops.cuh), so every box is bitwise the box advanced
+// alone.  A step is 8 launches whatever the number of boxes, and batches of
+// steps are one CUDA graph.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <map>
+#include <string>
+#include <vector>
+
+#include "../../include/nmhd.h"
+#include "cell_ops.cuh"
+#include "margin_ops.cuh"
+
+namespace nmhd {
+
+struct BoxDesc {
+  GridParams g;
+  float *w0, *w1, *wp, *flux, *dt_hist;
+  StepCtl *ctl;
+  int tile_begin;                 // first tile of this box in the flattened list
+  int tiles_x, tiles_y, tiles_z;  // 32 x 4 x 2-cell tiles per axis
+  long long fill_begin;           // first Y-margin fill item
+  long long mcfl_begin;           // first margin-CFL cell
+  long long cell_begin;           // first cell
+};
+
+namespace {
+
+using namespace cell;
+
+// Box owning flattened item `i`, where box b owns [begin(b), begin(b+1)).
+template <class F>
+__device__ __forceinline__ int find_box(int nb, long long i, F begin) {
+  int lo = 0, hi = nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (begin(mid) <= i) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+// One stage kernel over all boxes.  KIND 0: face fluxes, 1: constrained
+// transport, 2: conserved update + primitive recovery (+ CFL and clock in the
+// final stage).
+template <int KIND>
+__global__ void __launch_bounds__(kThreads, 3)
+    k_batch_stage(const BoxDesc *__restrict__ boxes, int nb, int total_tiles, int in_sel, int out_sel, int half,
+                  int final_stage) {
+  __shared__ BoxDesc sb;
+  __shared__ float red[kThreads / 32];
+  const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
+  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
+    __syncthreads();  // the previous tile is done with sb
+    if (tid == 0) sb = boxes[find_box(nb, t, [&](int b) { return (long long)boxes[b].tile_begin; })];
+    __syncthreads();
+    const GridParams &g = sb.g;
+    StepCtl *ctl = sb.ctl;
+    if (ctl->done) continue;
+    const int lt = t - sb.tile_begin;
+    const int bx = lt % sb.tiles_x, by = (lt / sb.tiles_x) % sb.tiles_y, bz = lt / (sb.tiles_x * sb.tiles_y);
+    const int x = bx * BX + threadIdx.x, y = by * BY + threadIdx.y, z = bz * BZ + threadIdx.z;
+    const bool inside = x < g.sx && y < g.sy && z < g.sz;
+    float dt = step_dt(ctl, nullptr);
+    if (half) dt = dt / 2.0f;
+    if (KIND == 0) {
+      if (inside) flux_cell(g, pick(ctl, in_sel, sb.w0, sb.w1, sb.wp), sb.flux, x, y, z, dt);
+    } else if (KIND == 1) {
+      if (inside) {
+        const float *win = pick(ctl, in_sel, sb.w0, sb.w1, sb.wp), *wb = pick(ctl, 0, sb.w0, sb.w1, sb.wp);
+        float *wo = const_cast<float *>(pick(ctl, out_sel, sb.w0, sb.w1, sb.wp));
+        if (g.pow2_spacing) ct_cell<true>(g, win, wb, wo, sb.flux, x, y, z, dt);
+        else ct_cell<false>(g, win, wb, wo, sb.flux, x, y, z, dt);
+      }
+    } else {
+      float tcfl = __uint_as_float(0x7f800000u);
+      int bad = 0;
+      if (inside) {
+        const float *wb = pick(ctl, 0, sb.w0, sb.w1, sb.wp);
+        float *wo = const_cast<float *>(pick(ctl, out_sel, sb.w0, sb.w1, sb.wp));
+        tcfl = g.pow2_spacing ? prim_cell<true>(g, wb, wo, sb.flux, x, y, z, dt, final_stage != 0, &bad)
+                              : prim_cell<false>(g, wb, wo, sb.flux, x, y, z, dt, final_stage != 0, &bad);
+      }
+      if (final_stage)
+        finish_tile(ctl, (unsigned)(sb.tiles_x * sb.tiles_y * sb.tiles_z), tcfl, bad, sb.dt_hist, red);
+    }
+  }
+}
+
+// Shearing-periodic Y-margin fill of every box (margin_ops.cuh).
+__global__ void __launch_bounds__(256) k_batch_fill(const BoxDesc *__restrict__ boxes, int nb, long long total) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
+    const int b = find_box(nb, i, [&](int k) { return boxes[k].fill_begin; });
+    const BoxDesc &d = boxes[b];
+    const StepCtl *ctl = d.ctl;
+    if (ctl->done) continue;
+    float *w = ctl->parity ? d.w1 : d.w0;
+    margin::fill_y_item(d.g, ctl->time, w, (int)(i - d.fill_begin));
+  }
+}
+
+// CFL time of every cell (all = 1) or of the margin cells (all = 0) of every
+// box, folded into each box's cfl_cur; lanes of a warp that belong to the same
+// box combine before one atomic.
+__global__ void __launch_bounds__(256) k_batch_cfl(const BoxDesc *__restrict__ boxes, int nb, long long total,
+                                                   int all) {
+  for (long long base = (long long)blockIdx.x * blockDim.x; base < total; base += (long long)gridDim.x * blockDim.x) {
+    const long long i = base + threadIdx.x;
+    int b = -1;
+    unsigned bits = 0x7f800000u;
+    if (i < total) {
+      b = all ? find_box(nb, i, [&](int k) { return boxes[k].cell_begin; })
+              : find_box(nb, i, [&](int k) { return boxes[k].mcfl_begin; });
+      const BoxDesc &d = boxes[b];
+      if (!d.ctl->done) {
+        const float *w = d.ctl->parity ? d.w1 : d.w0;
+        int x, y, z;
+        if (all) {
+          const int c = (int)(i - d.cell_begin);
+          x = c % d.g.sx;
+          y = (c / d.g.sx) % d.g.sy;
+          z = c / (d.g.sx * d.g.sy);
+        } else {
+          margin::margin_cfl_cell(d.g, (int)(i - d.mcfl_begin), &x, &y, &z);
+        }
+        bits = __float_as_uint(margin::cfl_of_cell(d.g, w, x, y, z));
+      }
+    }
+    const unsigned same = __match_any_sync(0xffffffffu, b);
+    const unsigned m = __reduce_min_sync(same, bits);
+    const int lane = threadIdx.x & 31;
+    if (b >= 0 && lane == __ffs(same) - 1) atomicMin(&boxes[b].ctl->cfl_cur, m);
+  }
+}
+
+}  // namespace
+}  // namespace nmhd
+
+using nmhd::BoxDesc;
+using nmhd::GridParams;
+using nmhd::StepCtl;
+
+struct nmhd_batch {
+  int n = 0;
+  std::vector<nmhd_config> cfg;
+  std::vector<BoxDesc> boxes;
+  BoxDesc *d_boxes = nullptr;
+  float *pool = nullptr;  // per box: w0, w1, wp (8 fields each), flux (21 fields)
+  float *hist = nullptr;
+  StepCtl *ctls = nullptr;
+  int total_tiles = 0;
+  long long total_fill = 0, total_mcfl = 0, total_cells = 0;
+  int ctas[3] = {0, 0, 0};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool cfl_ready = false;
+  std::map<int, cudaGraphExec_t> graphs;
+  std::string err;
+};
+
+namespace {
+
+thread_local std::string g_batch_error;
+
+nmhd_status bfail(nmhd_batch *b, nmhd_status st, const std::string &msg) {
+  if (b) b->err = msg;
+  else g_batch_error = msg;
+  return st;
+}
+
+#define BATCH_CUDA(b, call)                                                                       \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess)                                                                        \
+      return bfail(b, e_ == cudaErrorMemoryAllocation ? NMHD_ERR_OUT_OF_MEMORY : NMHD_ERR_CUDA,   \
+                   std::string(#call) + ": " + cudaGetErrorString(e_));                          \
+  } while (0)
+
+int grid_for(long long work, int cap) {
+  long long blocks = (work + 255) / 256;
+  return (int)std::max(1LL, std::min<long long>(blocks, cap));
+}
+
+void enqueue_batch_step(nmhd_batch *b) {
+  using namespace nmhd;
+  cudaStream_t st = b->stream;
+  const int cap = 148 * 16;
+  if (b->total_fill > 0)
+    k_batch_fill<<<grid_for(b->total_fill, cap), 256, 0, st>>>(b->d_boxes, b->n, b->total_fill);
+  if (b->total_mcfl > 0)
+    k_batch_cfl<<<grid_for(b->total_mcfl, cap), 256, 0, st>>>(b->d_boxes, b->n, b->total_mcfl, 0);
+  const dim3 blk(cell::BX, cell::BY, cell::BZ);
+  auto stage = [&](int in_sel, int out_sel, int half, int fin) {
+    k_batch_stage<0><<<std::min(b->ctas[0], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
+                                                                           in_sel, out_sel, half, fin);
+    k_batch_stage<1><<<std::min(b->ctas[1], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
+                                                                           in_sel, out_sel, half, fin);
+    k_batch_stage<2><<<std::min(b->ctas[2], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
+                                                                           in_sel, out_sel, half, fin);
+  };
+  stage(0, 2, 1, 0);
+  stage(2, 1, 0, 1);
+}
+
+nmhd_status read_ctls(nmhd_batch *b, std::vector<StepCtl> &h) {
+  h.resize(b->n);
+  BATCH_CUDA(b, cudaMemcpyAsync(h.data(), b->ctls, sizeof(StepCtl) * b->n, cudaMemcpyDeviceToHost, b->stream));
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  return NMHD_OK;
+}
+
+nmhd_status write_ctls(nmhd_batch *b, const std::vector<StepCtl> &h) {
+  BATCH_CUDA(b, cudaMemcpyAsync(b->ctls, h.data(), sizeof(StepCtl) * b->n, cudaMemcpyHostToDevice, b->stream));
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  return NMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) {
+  if (!out || !cfgs || n < 1) return bfail(nullptr, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  *out = nullptr;
+  nmhd_batch *b = new nmhd_batch();
+  b->n = n;
+  b->cfg.assign(cfgs, cfgs + n);
+  // layout: box regions rounded to 64 floats (256 bytes)
+  std::vector<size_t> off(n);
+  size_t pool_floats = 0;
+  for (int i = 0; i < n; ++i) {
+    const nmhd_config &c = cfgs[i];
+    const long long cells = (long long)c.size_x * c.size_y * c.size_z;
+    if (c.size_x < 1 || c.size_y < 1 || c.size_z < 1 || cells * 21 >= (1LL << 31) || c.margin_z != 0 ||
+        c.margin_y < 0 || c.size_y - 2 * c.margin_y < c.margin_y || !(c.gamma > 1.0f) || !(c.cfl > 0.0f) ||
+        (c.space_order != 1 && c.space_order != 2) || c.time_order != 2 ||
+        (c.problem != NMHD_PROBLEM_NONE && c.problem != NMHD_PROBLEM_SHEARING_BOX)) {
+      delete b;
+      return bfail(nullptr, NMHD_ERR_INVALID_ARGUMENT,
+                   "box " + std::to_string(i) + ": invalid configuration (batched boxes use time_order 2, "
+                   "no Z margins, at most 2^31/21 cells)");
+    }
+    off[i] = pool_floats;
+    pool_floats += (size_t)((cells + 63) / 64 * 64) * (3 * 8 + nmhd::kFluxFields);
+  }
+  cudaError_t e = cudaGetDevice(&b->device);
+  if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking);
+  if (e == cudaSuccess) e = cudaMalloc(&b->pool, sizeof(float) * pool_floats);
+  if (e == cudaSuccess) e = cudaMalloc(&b->hist, sizeof(float) * nmhd::kDtHistCap * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b->ctls, sizeof(StepCtl) * n);
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_boxes, sizeof(BoxDesc) * n);
+  if (e == cudaSuccess) e = cudaMemsetAsync(b->pool, 0, sizeof(float) * pool_floats, b->stream);
+  if (e != cudaSuccess) {
+    nmhd_batch_destroy(b);
+    return bfail(nullptr, e == cudaErrorMemoryAllocation ? NMHD_ERR_OUT_OF_MEMORY : NMHD_ERR_CUDA,
+                 std::string("nmhd_batch_create: ") + cudaGetErrorString(e));
+  }
+  b->boxes.resize(n);
+  std::vector<StepCtl> h(n);
+  for (int i = 0; i < n; ++i) {
+    BoxDesc &d = b->boxes[i];
+    d.g = nmhd::derive_grid(cfgs[i]);
+    const size_t cells = (size_t)d.g.n;
+    const size_t stride = (cells + 63) / 64 * 64;
+    float *base = b->pool + off[i];
+    d.w0 = base;
+    d.w1 = base + 8 * stride;
+    d.wp = base + 16 * stride;
+    d.flux = base + 24 * stride;
+    d.dt_hist = b->hist + (size_t)nmhd::kDtHistCap * i;
+    d.ctl = b->ctls + i;
+    d.tiles_x = (d.g.sx + nmhd::cell::BX - 1) / nmhd::cell::BX;
+    d.tiles_y = (d.g.sy + nmhd::cell::BY - 1) / nmhd::cell::BY;
+    d.tiles_z = (d.g.sz + nmhd::cell::BZ - 1) / nmhd::cell::BZ;
+    d.tile_begin = b->total_tiles;
+    d.fill_begin = b->total_fill;
+    d.mcfl_begin = b->total_mcfl;
+    d.cell_begin = b->total_cells;
+    b->total_tiles += d.tiles_x * d.tiles_y * d.tiles_z;
+    b->total_fill += (long long)d.g.sx * d.g.my * d.g.sz;
+    b->total_mcfl += nmhd::margin::margin_cfl_cells(d.g);
+    b->total_cells += (long long)cells;
+    std::memset(&h[i], 0, sizeof(StepCtl));
+    h[i].cfl_cur = h[i].cfl_next = 0x7f800000u;
+    h[i].goal = INFINITY;
+    h[i].hist_cap = nmhd::kDtHistCap;
+  }
+  // persistent launch: as many CTAs as fit on the GPU at once
+  int sms = 148;
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+  int occ[3] = {1, 1, 1};
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2>, nmhd::cell::kThreads, 0);
+  for (int k = 0; k < 3; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
+  e = cudaMemcpyAsync(b->d_boxes, b->boxes.data(), sizeof(BoxDesc) * n, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaMemcpyAsync(b->ctls, h.data(), sizeof(StepCtl) * n, cudaMemcpyHostToDevice, b->stream);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
+  if (e != cudaSuccess) {
+    nmhd_batch_destroy(b);
+    return bfail(nullptr, NMHD_ERR_CUDA, std::string("nmhd_batch_create: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return NMHD_OK;
+}
+
+void nmhd_batch_destroy(nmhd_batch *b) {
+  if (!b) return;
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  cudaFree(b->pool);
+  cudaFree(b->hist);
+  cudaFree(b->ctls);
+  cudaFree(b->d_boxes);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  delete b;
+}
+
+int nmhd_batch_size(const nmhd_batch *b) { return b ? b->n : 0; }
+
+nmhd_status nmhd_batch_set_state(nmhd_batch *b, int box, const float *const fields[8], int on_device) {
+  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  std::vector<StepCtl> h;
+  nmhd_status st = read_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  const BoxDesc &d = b->boxes[box];
+  float *cur = h[box].parity ? d.w1 : d.w0;
+  const size_t bytes = sizeof(float) * (size_t)d.g.n;
+  for (int v = 0; v < 8; ++v) {
+    if (!fields[v]) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+    BATCH_CUDA(b, cudaMemcpyAsync(cur + (size_t)v * d.g.n, fields[v], bytes,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+  }
+  h[box].status = 0;
+  h[box].done = 0;
+  h[box].cfl_cur = h[box].cfl_next = 0x7f800000u;
+  b->cfl_ready = false;
+  return write_ctls(b, h);
+}
+
+nmhd_status nmhd_batch_get_state(nmhd_batch *b, int box, float *const fields[8], int on_device) {
+  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  std::vector<StepCtl> h;
+  nmhd_status st = read_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  const BoxDesc &d = b->boxes[box];
+  const float *cur = h[box].parity ? d.w1 : d.w0;
+  const size_t bytes = sizeof(float) * (size_t)d.g.n;
+  for (int v = 0; v < 8; ++v) {
+    if (!fields[v]) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
+    BATCH_CUDA(b, cudaMemcpyAsync(fields[v], cur + (size_t)v * d.g.n, bytes,
+                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
+  }
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *generation) {
+  if (!b || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  std::vector<StepCtl> h;
+  nmhd_status st = read_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  if (time) *time = h[box].time;
+  if (generation) *generation = h[box].generation;
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done) {
+  if (steps_done) *steps_done = 0;
+  if (!b) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "NULL batch");
+  std::vector<StepCtl> h;
+  nmhd_status st = read_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  for (int i = 0; i < b->n; ++i)
+    if (h[i].status) return bfail(b, NMHD_ERR_NUMERICAL, "box " + std::to_string(i) + " holds an invalid state");
+  long long gen0 = 0;
+  for (int i = 0; i < b->n; ++i) {
+    gen0 = std::max(gen0, h[i].generation);
+    h[i].goal = (float)goal_time;
+    h[i].done = 0;
+    if (!b->cfl_ready) {
+      h[i].cfl_cur = h[i].cfl_next = 0x7f800000u;
+      h[i].blocks_done = 0;
+    }
+  }
+  st = write_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  if (!b->cfl_ready) {
+    const int cap = 148 * 16;
+    if (b->total_fill > 0)
+      nmhd::k_batch_fill<<<grid_for(b->total_fill, cap), 256, 0, b->stream>>>(b->d_boxes, b->n, b->total_fill);
+    nmhd::k_batch_cfl<<<grid_for(b->total_cells, cap), 256, 0, b->stream>>>(b->d_boxes, b->n, b->total_cells, 1);
+    BATCH_CUDA(b, cudaGetLastError());
+    b->cfl_ready = true;
+  }
+  const int kBatch = 16;
+  long long left = max_steps > 0 ? max_steps : -1;
+  long long launched = 0;
+  nmhd_status result = NMHD_OK;
+  for (;;) {
+    int k = kBatch;
+    if (left >= 0 && left < k) k = (int)left;
+    if (k == 0) { result = NMHD_STEP_LIMIT; break; }
+    cudaGraphExec_t ge;
+    auto it = b->graphs.find(k);
+    if (it == b->graphs.end()) {
+      cudaGraph_t graph;
+      BATCH_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+      for (int i = 0; i < k; ++i) enqueue_batch_step(b);
+      BATCH_CUDA(b, cudaStreamEndCapture(b->stream, &graph));
+      cudaError_t e = cudaGraphInstantiate(&ge, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return bfail(b, NMHD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      b->graphs[k] = ge;
+    } else {
+      ge = it->second;
+    }
+    BATCH_CUDA(b, cudaGraphLaunch(ge, b->stream));
+    st = read_ctls(b, h);
+    if (st != NMHD_OK) return st;
+    launched += k;
+    if (left > 0) left -= k;
+    int bad = -1, done = 0;
+    for (int i = 0; i < b->n; ++i) {
+      if (h[i].status && bad < 0) bad = i;
+      done += h[i].done;
+    }
+    if (bad >= 0) {
+      result = bfail(b, NMHD_ERR_NUMERICAL, "box " + std::to_string(bad) + ": non-finite state, density <= 0, "
+                                            "pressure <= 0 or bad dt");
+      break;
+    }
+    if (done == b->n) { result = NMHD_GOAL_REACHED; break; }
+  }
+  if (steps_done) {
+    long long gen1 = 0;
+    for (int i = 0; i < b->n; ++i) gen1 = std::max(gen1, h[i].generation);
+    *steps_done = gen1 - gen0;
+  }
+  return result;
+}
+
+const char *nmhd_batch_last_error(const nmhd_batch *b) { return b ? b->err.c_str() : g_batch_error.c_str(); }
+
+}  // extern "C"

@@ -1,148 +1,23 @@
-// Per-cell stage kernels (v3) of the B200 ideal-MHD time step, sm_100a.
+// Per-cell stage kernels (variant 2, the default) of the B200 ideal-MHD time
+// step, sm_100a: one thread per cell on 32 x 4 x 2 CTAs.
 //
-// One thread per cell, 32 x 4 x 2 cells per CTA so that the stencil
-// neighbours in x, y and z of a CTA mostly hit the SM's L1.  Every periodic
-// neighbour address is the cell address plus one of nine offsets computed once
-// per thread (wrap along x, y, z at -2, -1, +1), so the stencil gathers cost
-// one add each.
-//
-//  k_cell_flux    reconstruction + HLLD on the cell's lower x-, y- and z-face
-//                 (calc_flux_kernel<X,Y,Z>, src/library/mhd_solver.inlrb:562-636);
-//                 21 flux values per cell (mass, momentum x/y/z, energy, two
-//                 transverse B) go to scratch.
-//  k_cell_ct      corner EMFs and the face-B update (:641-714), written into
-//                 the output state.
-//  k_cell_prim    flux divergence (add_flux_kernel :689-693), conserved update
-//                 (:762-835), primitive recovery (:779-795), the Kepler kick
-//                 (:837-848), and in the final stage the CFL reduction and
-//                 clock update (:496-521, 870-901, 981).
-//
-// Same arithmetic as the other variants (mhd_math.cuh, -fmad=false): results
-// are bitwise identical.
-#include "mhd_math.cuh"
-#include "step.cuh"
+//  k_cell_flux  reconstruction + HLLD on the cell's lower x-, y- and z-face
+//               (calc_flux_kernel<X,Y,Z>, src/library/mhd_solver.inlrb:562-636);
+//               21 flux values per cell go to scratch.
+//  k_cell_ct    corner EMFs and the face-B update (:641-714), written into the
+//               output state.
+//  k_cell_prim  flux divergence (add_flux_kernel :689-693), conserved update
+//               (:762-835), primitive recovery (:779-795), the Kepler kick
+//               (:837-848), and in the final stage the CFL reduction and clock
+//               update (:496-521, 870-901, 981).
+// The per-cell work lives in cell_ops.cuh, shared with the batch kernels.
+#include "cell_ops.cuh"
 
 namespace nmhd {
 
 namespace {
 
-constexpr int BX = 32, BY = 4, BZ = 2, kThreads = BX * BY * BZ;
-
-__device__ __forceinline__ int wrap_any(int v, int s) {
-  while (v < 0) v += s;
-  while (v >= s) v -= s;
-  return v;
-}
-
-// Offset (in elements of stride) from coordinate c to the periodic c + d.
-__device__ __forceinline__ int woff(int c, int d, int s) { return wrap_any(c + d, s) - c; }
-
-struct Offsets {
-  int xm2, xm1, xp1, ym2, ym1, yp1, zm2, zm1, zp1;
-};
-
-__device__ __forceinline__ Offsets offsets(const GridParams &g, int x, int y, int z) {
-  const int sxy = g.sx * g.sy;
-  Offsets f;
-  f.xm2 = woff(x, -2, g.sx);
-  f.xm1 = woff(x, -1, g.sx);
-  f.xp1 = woff(x, 1, g.sx);
-  f.ym2 = woff(y, -2, g.sy) * g.sx;
-  f.ym1 = woff(y, -1, g.sy) * g.sx;
-  f.yp1 = woff(y, 1, g.sy) * g.sx;
-  f.zm2 = woff(z, -2, g.sz) * sxy;
-  f.zm1 = woff(z, -1, g.sz) * sxy;
-  f.zp1 = woff(z, 1, g.sz) * sxy;
-  return f;
-}
-
-// x / d for a grid spacing d; with power-of-two spacings the product with the
-// exact reciprocal is the same float.
-template <bool kPow2>
-__device__ __forceinline__ float divs(float x, float d, float inv) {
-  return kPow2 ? x * inv : x / d;
-}
-
-__device__ __forceinline__ float cell_dt(const StepCtl *c, bool *last) {
-  const float cmin = __uint_as_float(c->cfl_cur);
-  float dt = fminf(c->goal, cmin);
-  const double next_time = c->time + (double)dt;
-  const bool l = next_time > (double)c->goal;
-  if (l) dt = (float)((double)c->goal - c->time);
-  if (last) *last = l;
-  return dt;
-}
-
-__device__ __forceinline__ const float *cell_pick(const StepCtl *c, int sel, const float *w0,
-                                                  const float *w1, const float *wp) {
-  if (sel == 2) return wp;
-  return (sel == 0) == (c->parity == 0) ? w0 : w1;
-}
-
-// Flux through the lower face of cell o along runtime axis `ax` (one HLLD
-// instance serves all three axes, keeping the kernel's code small).
-// sm/sp: offsets of the stencil cells -2, -1, +1 along ax; t1/t2: +1 offsets
-// along the transverse axes ax+1 and ax+2 (mod 3).  The 7 results go to
-// flux + (7*ax + k)*N + o with momentum in absolute components.
-__device__ __forceinline__ void cell_face_rt(const GridParams &g, const float *__restrict__ w, size_t N,
-                                             int o, int ax, int m2, int m1, int p1, int t1, int t2,
-                                             int yidx, float dt, float *__restrict__ flux) {
-  const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
-  const float *rho = w, *p = w + 4 * N;
-  const float *vn = w + (1 + ax) * N, *v1 = w + (1 + e1) * N, *v2 = w + (1 + e2) * N;
-  const float *bn = w + (5 + ax) * N, *b1 = w + (5 + e1) * N, *b2 = w + (5 + e2) * N;
-  const int s[4] = {m2, m1, 0, p1};
-  float bc1[4], bc2[4];
-#pragma unroll
-  for (int t = 0; t < 4; ++t) {
-    const int c = o + s[t];
-    bc1[t] = 0.5f * (__ldg(b1 + c) + __ldg(b1 + c + t1));
-    bc2[t] = 0.5f * (__ldg(b2 + c) + __ldg(b2 + c + t2));
-  }
-  HlldIn in;
-  if (g.order2) {
-    reconstruct4(__ldg(rho + o + m2), __ldg(rho + o + m1), __ldg(rho + o), __ldg(rho + o + p1), in.dl, in.dr);
-    reconstruct4(__ldg(vn + o + m2), __ldg(vn + o + m1), __ldg(vn + o), __ldg(vn + o + p1), in.ul, in.ur);
-    reconstruct4(__ldg(v1 + o + m2), __ldg(v1 + o + m1), __ldg(v1 + o), __ldg(v1 + o + p1), in.vl, in.vr);
-    reconstruct4(__ldg(v2 + o + m2), __ldg(v2 + o + m1), __ldg(v2 + o), __ldg(v2 + o + p1), in.wl, in.wr);
-    reconstruct4(__ldg(p + o + m2), __ldg(p + o + m1), __ldg(p + o), __ldg(p + o + p1), in.pl, in.pr);
-    reconstruct4(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
-    reconstruct4(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
-  } else {
-    in.dl = __ldg(rho + o + m1); in.dr = __ldg(rho + o);
-    in.ul = __ldg(vn + o + m1); in.ur = __ldg(vn + o);
-    in.vl = __ldg(v1 + o + m1); in.vr = __ldg(v1 + o);
-    in.wl = __ldg(v2 + o + m1); in.wr = __ldg(v2 + o);
-    in.pl = __ldg(p + o + m1); in.pr = __ldg(p + o);
-    in.byl = bc1[1]; in.byr = bc1[2];
-    in.bzl = bc2[1]; in.bzr = bc2[2];
-  }
-  if (g.shear) {
-    float acc;
-    if (ax == 0) {
-      const float vY = 0.5f * (__ldg(w + 2 * N + o + m1) + __ldg(w + 2 * N + o));
-      acc = -2.0f * g.omega * vY;
-    } else if (ax == 1) {
-      const float vX = 0.5f * (__ldg(w + N + o + m1) + __ldg(w + N + o));
-      acc = 2.0f * g.omega * vX + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)yidx + 0.5f));
-    } else {
-      acc = 0.0f;
-    }
-    const float mbv = 0.5f * dt * acc;
-    in.ul += mbv;
-    in.ur += mbv;
-  }
-  float f[7];
-  hlld_flux(g.gamma, __ldg(bn + o), in, f);
-  float *out = flux + (size_t)(7 * ax) * N + o;
-  out[0] = f[0];
-  out[(1 + ax) * N] = f[1];
-  out[(1 + e1) * N] = f[2];
-  out[(1 + e2) * N] = f[3];
-  out[4 * N] = f[4];
-  out[5 * N] = f[5];
-  out[6 * N] = f[6];
-}
+using namespace cell;
 
 __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const StepCtl *ctl, const float *w0,
                                                            const float *w1, const float *wp,
@@ -152,51 +27,11 @@ __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const S
   const int y = blockIdx.y * BY + threadIdx.y;
   const int z = blockIdx.z * BZ + threadIdx.z;
   if (x >= g.sx || y >= g.sy || z >= g.sz) return;
-  const float *w = cell_pick(ctl, in_sel, w0, w1, wp);
-  float dt = cell_dt(ctl, nullptr);
+  float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
-  const size_t N = (size_t)g.n;
-  const int o = (z * g.sy + y) * g.sx + x;
-  const Offsets f = offsets(g, x, y, z);
-#pragma unroll 1
-  for (int ax = 0; ax < 3; ++ax) {
-    const int m2 = ax == 0 ? f.xm2 : ax == 1 ? f.ym2 : f.zm2;
-    const int m1 = ax == 0 ? f.xm1 : ax == 1 ? f.ym1 : f.zm1;
-    const int p1 = ax == 0 ? f.xp1 : ax == 1 ? f.yp1 : f.zp1;
-    const int t1 = ax == 0 ? f.yp1 : ax == 1 ? f.zp1 : f.xp1;
-    const int t2 = ax == 0 ? f.zp1 : ax == 1 ? f.xp1 : f.yp1;
-    cell_face_rt(g, w, N, o, ax, m2, m1, p1, t1, t2, y, dt, flux);
-  }
+  flux_cell(g, pick(ctl, in_sel, w0, w1, wp), flux, x, y, z, dt);
 }
 
-// corner_magnet_flux (mhd_solver.inlrb:641-653) at edge address e: the
-// a-flux of B_b; mb, ma are the offsets of -1 along b and along a.
-__device__ __forceinline__ float cell_corner(const float *__restrict__ vb, const float *__restrict__ fb,
-                                             int e, int mb, int ma) {
-  const float w = __ldg(vb + e) + __ldg(vb + e + mb) + __ldg(vb + e + ma) + __ldg(vb + e + ma + mb);
-  const float f0 = __ldg(fb + e + mb);
-  const float f1 = __ldg(fb + e);
-  return w > 0.0f ? f0 : (w < 0.0f ? f1 : 0.5f * (f0 + f1));
-}
-
-__device__ __forceinline__ float cell_block_min(float v) {
-  __shared__ float red[kThreads / 32];
-  for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
-  const int lane = tid & 31, warp = tid >> 5;
-  if (lane == 0) red[warp] = v;
-  __syncthreads();
-  if (warp == 0) {
-    v = lane < kThreads / 32 ? red[lane] : __uint_as_float(0x7f800000u);
-    for (int o = 16; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(0xffffffffu, v, o));
-  }
-  return v;
-}
-
-// Constrained transport of one stage (add_flux_kernel's B part,
-// mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
-// new face B on the cell's lower x-, y- and z-face, written into the output
-// state.  18 corner EMFs per cell.
 template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
                                                          float *w1, float *wp,
@@ -207,184 +42,30 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const Ste
   const int y = blockIdx.y * BY + threadIdx.y;
   const int z = blockIdx.z * BZ + threadIdx.z;
   if (x >= g.sx || y >= g.sy || z >= g.sz) return;
-  const size_t N = (size_t)g.n;
-  const float *win = cell_pick(ctl, in_sel, w0, w1, wp);
-  const float *wb = cell_pick(ctl, 0, w0, w1, wp);
-  float *wo = const_cast<float *>(cell_pick(ctl, out_sel, w0, w1, wp));
-  float dt = cell_dt(ctl, nullptr);
+  float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
-  const int o = (z * g.sy + y) * g.sx + x;
-  const Offsets f = offsets(g, x, y, z);
-  const int xm = f.xm1, xp = f.xp1, ym = f.ym1, yp = f.yp1, zm = f.zm1, zp = f.zp1;
-  const float *vx = win + N, *vy = win + 2 * N, *vz = win + 3 * N;
-  const float *FxBy = flux + 5 * N, *FxBz = flux + 6 * N;
-  const float *FyBz = flux + 12 * N, *FyBx = flux + 13 * N;
-  const float *FzBx = flux + 19 * N, *FzBy = flux + 20 * N;
-  // corners at the cell's edge (00) and the edges one step up each in-plane axis
-  // XY: F_x(B_y) with wind v_y, edges (x, y), (x, y+1), (x+1, y)
-  const float XY00 = cell_corner(vy, FxBy, o, ym, xm);
-  const float XY01 = cell_corner(vy, FxBy, o + yp, -yp, xm);
-  const float XY10 = cell_corner(vy, FxBy, o + xp, ym, -xp);
-  // YX: F_y(B_x) with wind v_x
-  const float YX00 = cell_corner(vx, FyBx, o, xm, ym);
-  const float YX01 = cell_corner(vx, FyBx, o + yp, xm, -yp);
-  const float YX10 = cell_corner(vx, FyBx, o + xp, -xp, ym);
-  // XZ: F_x(B_z) with wind v_z, edges (x, z), (x, z+1), (x+1, z)
-  const float XZ00 = cell_corner(vz, FxBz, o, zm, xm);
-  const float XZ01 = cell_corner(vz, FxBz, o + zp, -zp, xm);
-  const float XZ10 = cell_corner(vz, FxBz, o + xp, zm, -xp);
-  // ZX: F_z(B_x) with wind v_x
-  const float ZX00 = cell_corner(vx, FzBx, o, xm, zm);
-  const float ZX01 = cell_corner(vx, FzBx, o + zp, xm, -zp);
-  const float ZX10 = cell_corner(vx, FzBx, o + xp, -xp, zm);
-  // YZ: F_y(B_z) with wind v_z, edges (y, z), (y, z+1), (y+1, z)
-  const float YZ00 = cell_corner(vz, FyBz, o, zm, ym);
-  const float YZ01 = cell_corner(vz, FyBz, o + zp, -zp, ym);
-  const float YZ10 = cell_corner(vz, FyBz, o + yp, zm, -yp);
-  // ZY: F_z(B_y) with wind v_y
-  const float ZY00 = cell_corner(vy, FzBy, o, ym, zm);
-  const float ZY01 = cell_corner(vy, FzBy, o + zp, ym, -zp);
-  const float ZY10 = cell_corner(vy, FzBy, o + yp, -yp, zm);
-  const float dx = g.dx, dy = g.dy, dz = g.dz, ix = g.inv_dx, iy = g.inv_dy, iz = g.inv_dz;
-  float pb = 0.0f;
-  pb = pb + 0.5f * (divs<kPow2>(XY01 - XY00, dy, iy) + divs<kPow2>(XZ01 - XZ00, dz, iz));
-  pb = pb - divs<kPow2>(0.5f * (YX01 - YX00), dy, iy);
-  pb = pb - divs<kPow2>(0.5f * (ZX01 - ZX00), dz, iz);
-  wo[5 * N + o] = wb[5 * N + o] + dt * pb;
-  pb = 0.0f;
-  pb = pb - divs<kPow2>(0.5f * (XY10 - XY00), dx, ix);
-  pb = pb + 0.5f * (divs<kPow2>(YZ01 - YZ00, dz, iz) + divs<kPow2>(YX10 - YX00, dx, ix));
-  pb = pb - divs<kPow2>(0.5f * (ZY01 - ZY00), dz, iz);
-  wo[6 * N + o] = wb[6 * N + o] + dt * pb;
-  pb = 0.0f;
-  pb = pb - divs<kPow2>(0.5f * (XZ10 - XZ00), dx, ix);
-  pb = pb - divs<kPow2>(0.5f * (YZ10 - YZ00), dy, iy);
-  pb = pb + 0.5f * (divs<kPow2>(ZX10 - ZX00, dx, ix) + divs<kPow2>(ZY10 - ZY00, dy, iy));
-  wo[7 * N + o] = wb[7 * N + o] + dt * pb;
+  ct_cell<kPow2>(g, pick(ctl, in_sel, w0, w1, wp), pick(ctl, 0, w0, w1, wp),
+                 const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)), flux, x, y, z, dt);
 }
 
-// Rest of the stage: flux divergence of rho, m, E (mhd_solver.inlrb:689-693),
-// conserved state before the stage (to_conserved :762-777), update
-// (add_pace/update :797-835), primitive recovery with the new face B
-// (:779-795), the Kepler kick (:837-848) and, in the final stage, the CFL
-// reduction and clock update (:496-521, 870-901, 981).
 template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, 3) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
                                                            float *w1, float *wp,
                                                            const float *__restrict__ flux, float *dt_hist,
                                                            int out_sel, int half, int final_stage) {
+  __shared__ float red[kThreads / 32];
   if (ctl->done) return;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
   const int z = blockIdx.z * BZ + threadIdx.z;
-  const bool inside = x < g.sx && y < g.sy && z < g.sz;
-  const size_t N = (size_t)g.n;
-  const float *wb = cell_pick(ctl, 0, w0, w1, wp);
-  float *wo = const_cast<float *>(cell_pick(ctl, out_sel, w0, w1, wp));
-  float dt = cell_dt(ctl, nullptr);
+  float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
   float tcfl = __uint_as_float(0x7f800000u);
   int bad = 0;
-  if (inside) {
-    const int o = (z * g.sy + y) * g.sx + x;
-    const int xp = x + 1 < g.sx ? 1 : 1 - g.sx;
-    const int yp = (y + 1 < g.sy ? 1 : 1 - g.sy) * g.sx;
-    const int zp = (z + 1 < g.sz ? 1 : 1 - g.sz) * g.sx * g.sy;
-    const float *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
-    // all loads first: 30 face fluxes, the state before the stage, new face B
-    float fl[5][6];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      fl[v][0] = __ldg(Fx + v * N + o);
-      fl[v][1] = __ldg(Fx + v * N + o + xp);
-      fl[v][2] = __ldg(Fy + v * N + o);
-      fl[v][3] = __ldg(Fy + v * N + o + yp);
-      fl[v][4] = __ldg(Fz + v * N + o);
-      fl[v][5] = __ldg(Fz + v * N + o + zp);
-    }
-    float pace[5];
-#pragma unroll
-    for (int v = 0; v < 5; ++v) {
-      float pc = 0.0f;
-      pc = pc + divs<kPow2>(fl[v][0] - fl[v][1], g.dx, g.inv_dx);
-      pc = pc + divs<kPow2>(fl[v][2] - fl[v][3], g.dy, g.inv_dy);
-      pc = pc + divs<kPow2>(fl[v][4] - fl[v][5], g.dz, g.inv_dz);
-      pace[v] = pc;
-    }
-    const float gm1 = g.gamma - 1.0f;
-    const float rho0 = wb[o];
-    const float vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o], p0 = wb[4 * N + o];
-    const float bxl = wb[5 * N + o], bxh = wb[5 * N + o + xp];
-    const float byl = wb[6 * N + o], byh = wb[6 * N + o + yp];
-    const float bzl = wb[7 * N + o], bzh = wb[7 * N + o + zp];
-    const float mx0 = rho0 * vx0, my0 = rho0 * vy0, mz0 = rho0 * vz0;
-    const float e0 = p0 / gm1 + 0.5f * rho0 * (vx0 * vx0 + vy0 * vy0 + vz0 * vz0) +
-                     0.25f * (bxl * bxl + bxh * bxh + byl * byl + byh * byh + bzl * bzl + bzh * bzh);
-    const float rho = rho0 + dt * pace[0];
-    const float mx = mx0 + dt * pace[1];
-    const float my = my0 + dt * pace[2];
-    const float mz = mz0 + dt * pace[3];
-    const float ene = e0 + dt * pace[4];
-    // new face B from k_cell_ct (this cell's lower faces and its neighbours')
-    const float bx0 = wo[5 * N + o], bx1 = wo[5 * N + o + xp];
-    const float by0 = wo[6 * N + o], by1 = wo[6 * N + o + yp];
-    const float bz0 = wo[7 * N + o], bz1 = wo[7 * N + o + zp];
-    float vxo = mx / rho, vyo = my / rho, vzo = mz / rho;
-    const float eint = ene - 0.5f * (mx * mx + my * my + mz * mz) / rho -
-                       0.25f * (bx0 * bx0 + bx1 * bx1 + by0 * by0 + by1 * by1 + bz0 * bz0 + bz1 * bz1);
-    const float po = eint * gm1;
-    if (g.shear) {
-      const float ax = -2.0f * g.omega * vyo;
-      const float ay = 2.0f * g.omega * vxo + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)y + 0.5f));
-      vxo = vxo + dt * ax;
-      vyo = vyo + dt * ay;
-      vzo = vzo + dt * 0.0f;
-    }
-    wo[o] = rho;
-    wo[N + o] = vxo;
-    wo[2 * N + o] = vyo;
-    wo[3 * N + o] = vzo;
-    wo[4 * N + o] = po;
-    if (final_stage) {
-      bad = !(rho > 0.0f) || !(po > 0.0f) || !isfinite(vxo) || !isfinite(vyo) || !isfinite(vzo) ||
-            !isfinite(bx0) || !isfinite(by0) || !isfinite(bz0);
-      const bool margin_cell = (y < g.my) || (y >= g.sy - g.my) ||
-                               (g.mz > 0 && (z < g.mz || z >= g.sz - g.mz - 1));
-      if (!margin_cell) {
-        const float b2 = fmaxf(bx0 * bx0, bx1 * bx1) + fmaxf(by0 * by0, by1 * by1) + fmaxf(bz0 * bz0, bz1 * bz1);
-        const float cs = sqrtf((g.gamma * po + b2) / rho);
-        tcfl = fminf(fminf(g.cfl * g.dx / fabsf(vxo + cs), g.cfl * g.dy / fabsf(vyo + cs)),
-                     g.cfl * g.dz / fabsf(vzo + cs));
-      }
-    }
-  }
-  if (!final_stage) return;
-  tcfl = cell_block_min(tcfl);
-  bad = __syncthreads_or(bad);
-  if (threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0) {
-    atomicMin(&ctl->cfl_next, __float_as_uint(tcfl));
-    if (bad) atomicOr(&ctl->status, kStatusNumerical);
-    __threadfence();
-    const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
-    const unsigned prev = atomicAdd(&ctl->blocks_done, 1u);
-    if (prev == nblocks - 1) {
-      // last block: advance the clock (GlobalSetup::proceed, :981) and rotate
-      __threadfence();
-      bool last;
-      const float dts = cell_dt(ctl, &last);
-      volatile StepCtl *vc = ctl;
-      const long long gen = vc->generation;
-      dt_hist[gen % kDtHistCap] = dts;
-      vc->time = vc->time + (double)dts;
-      vc->generation = gen + 1;
-      vc->parity = vc->parity ^ 1;
-      vc->cfl_cur = atomicAdd(&ctl->cfl_next, 0u);
-      vc->cfl_next = 0x7f800000u;
-      if (!(dts >= 0.0f)) atomicOr(&ctl->status, kStatusBadDt);
-      if (last || vc->status) vc->done = 1;
-      vc->blocks_done = 0;
-    }
-  }
+  if (x < g.sx && y < g.sy && z < g.sz)
+    tcfl = prim_cell<kPow2>(g, pick(ctl, 0, w0, w1, wp), const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)),
+                            flux, x, y, z, dt, final_stage != 0, &bad);
+  if (final_stage) finish_tile(ctl, gridDim.x * gridDim.y * gridDim.z, tcfl, bad, dt_hist, red);
 }
 
 dim3 cell_grid(const GridParams &g) {

@@ -16,6 +16,7 @@
 //
 // All arithmetic follows the reference operation by operation (mhd_math.cuh);
 // this file is compiled with -fmad=false.
+#include "margin_ops.cuh"
 #include "mhd_math.cuh"
 #include "step.cuh"
 
@@ -98,13 +99,7 @@ __device__ __forceinline__ float block_min(float v) {
 }
 
 __device__ __forceinline__ float cell_cfl(const GridParams &g, const float *w, int x, int y, int z) {
-  const int n = g.n;
-  const int o = (z * g.sy + y) * g.sx + x;
-  const float bxl = w[5 * n + o], bxh = w[5 * n + at(g, x + 1, y, z)];
-  const float byl = w[6 * n + o], byh = w[6 * n + at(g, x, y + 1, z)];
-  const float bzl = w[7 * n + o], bzh = w[7 * n + at(g, x, y, z + 1)];
-  const float b2 = fmaxf(bxl * bxl, bxh * bxh) + fmaxf(byl * byl, byh * byh) + fmaxf(bzl * bzl, bzh * bzh);
-  return cfl_time(g, w[o], w[n + o], w[2 * n + o], w[3 * n + o], w[4 * n + o], b2);
+  return margin::cfl_of_cell(g, w, x, y, z);
 }
 
 // ---------------------------------------------------------------------------
@@ -123,21 +118,9 @@ __global__ void __launch_bounds__(kBlock) k_cfl(GridParams g, StepCtl *ctl, cons
       t = cell_cfl(g, w, c.x, c.y, c.z);
     }
   } else {
-    const int part_a = 2 * g.my * g.sx * g.sz;
-    const int zplanes = g.mz > 0 ? 2 * g.mz + 1 : 0;
-    const int part_b = zplanes * g.sx * g.sy;
-    if (idx < part_a) {
-      const int x = idx % g.sx;
-      const int r = (idx / g.sx) % (2 * g.my);
-      const int z = idx / (g.sx * 2 * g.my);
-      const int y = r < g.my ? r : g.sy - 2 * g.my + r;
-      t = cell_cfl(g, w, x, y, z);
-    } else if (idx < part_a + part_b) {
-      const int j = idx - part_a;
-      const int x = j % g.sx;
-      const int y = (j / g.sx) % g.sy;
-      const int p = j / (g.sx * g.sy);
-      const int z = p < g.mz ? p : g.sz - g.mz - 1 + (p - g.mz);
+    if (idx < margin::margin_cfl_cells(g)) {
+      int x, y, z;
+      margin::margin_cfl_cell(g, idx, &x, &y, &z);
       t = cell_cfl(g, w, x, y, z);
     }
   }
@@ -160,37 +143,7 @@ __global__ void __launch_bounds__(kBlock) k_fill_y(GridParams g, StepCtl *ctl, f
   const int total = g.sx * M * g.sz;
   const int idx = blockIdx.x * blockDim.x + threadIdx.x;
   if (idx >= total) return;
-  const int sx = idx % g.sx;
-  const int sy = (idx / g.sx) % M;
-  const int sz = idx / (g.sx * M);
-  // relative_displacement(t): all double except the float product fold*kExtentX
-  const double d0 = 0.0 + ctl->time * g.rel_vel;
-  const int fold = (int)floor(d0 / (double)g.extent_x);
-  const double d1 = d0 - (double)((float)fold * g.extent_x);
-  const int dint = (int)floor(d1 / (double)g.dx);
-  const float f = (float)(d1 / (double)g.dx - dint);
-  const float rv = (float)g.rel_vel;
-  const int inc_x = wrapc((sx + dint) % g.sx, g.sx);
-  const int dec_x = wrapc((sx - dint - 1) % g.sx, g.sx);
-  const int n = g.n;
-  const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + inc_x;
-  const int src_dec = (sz * g.sy + (M + sy)) * g.sx + dec_x;
-  const int dst_lo = (sz * g.sy + sy) * g.sx + sx;
-  const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx;
-  const float omf = 1.0f - f;
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    const float vi = w[v * n + src_inc];
-    const float vd = w[v * n + src_dec];
-    float bi = omf * vi + f * vi;
-    float bd = f * vd + omf * vd;
-    if (v == 1) {
-      bi = bi - rv;
-      bd = bd + rv;
-    }
-    w[v * n + dst_lo] = bi;
-    if (!(v == 6 && sy == 0)) w[v * n + dst_hi] = bd;
-  }
+  margin::fill_y_item(g, ctl->time, w, idx);
 }
 
 // Plain periodic Z-margin copy (the Z part of communicate(), mhd_solver.inlrb:384-402, 463-480).
@@ -567,7 +520,7 @@ void launch_cfl_all(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cud
 }
 
 void launch_cfl_margin(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t st) {
-  const long long work = 2LL * g.my * g.sx * g.sz + (g.mz > 0 ? (2LL * g.mz + 1) * g.sx * g.sy : 0);
+  const long long work = margin::margin_cfl_cells(g);
   if (work > 0) k_cfl<<<blocks_for(work), kBlock, 0, st>>>(g, ctl, w0, w1, 1);
 }
 

@@ -99,3 +99,30 @@ def shearing_box(n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0, l_a
     pert = rng.uniform(-noise, noise, size=(3, sz, n_radial, sx)) * cs
     state[1:4, :, margin:margin + n_radial, :] += pert
     return cfg, state.astype(np.float32)
+
+
+def mri_ensemble(n_boxes=64, seed=0, sides=(32, 48, 64, 96), ratios=(2, 3, 4), beta_range=(1e2, 1e4),
+                 q_range=(1.2, 1.8), noise=0.01, margin=4):
+    """Ensemble of independent MRI shearing boxes of uneven sizes.
+
+    Per box: radial and vertical cell counts drawn from ``sides``, azimuthal =
+    k * radial with k from ``ratios``; extents radial 1, azimuthal k, vertical 1
+    (cubic cells); beta log-uniform in ``beta_range``; q uniform in ``q_range``;
+    noise seed 1000 + box.  The draws use numpy PCG64(seed).
+    Returns (list of (config, state), list of per-box parameter dicts).
+    """
+    rng = np.random.Generator(np.random.PCG64(seed))
+    boxes, params = [], []
+    for b in range(n_boxes):
+        nr = int(rng.choice(sides))
+        nz = int(rng.choice(sides))
+        k = int(rng.choice(ratios))
+        beta = float(10.0 ** rng.uniform(math.log10(beta_range[0]), math.log10(beta_range[1])))
+        q = float(rng.uniform(*q_range))
+        cfg, state = shearing_box(n_radial=nr, n_azimuthal=k * nr, n_vertical=nz, l_radial=1.0,
+                                  l_azimuthal=float(k), l_vertical=1.0, q=q, beta=beta, noise=noise,
+                                  seed=1000 + b, margin=margin)
+        boxes.append((cfg, state))
+        params.append({"n_radial": nr, "n_azimuthal": k * nr, "n_vertical": nz, "beta": beta, "q": q,
+                       "seed": 1000 + b})
+    return boxes, params

@@ -1,0 +1,80 @@
+"""Batched ensemble (nmhd_batch_*): every box of a batch is bitwise the box
+advanced alone by the single-box solver (which is pinned to the oracle), with
+its own CFL time step and clock."""
+import ctypes
+import math
+
+import numpy as np
+import pytest
+
+from nmhd_b200 import _lib
+from nmhd_b200.config import SolverConfig
+from nmhd_b200.problems import mri_ensemble, orszag_tang_3d, shearing_box
+
+
+def small_ensemble(n=7, seed=3):
+    return mri_ensemble(n_boxes=n, seed=seed, sides=(8, 12, 16), ratios=(2, 3, 4))
+
+
+def test_ensemble_draws_follow_the_spec():
+    boxes, params = mri_ensemble(n_boxes=64, seed=0)
+    assert len(boxes) == 64
+    for (cfg, state), p in zip(boxes, params):
+        assert p["n_radial"] in (32, 48, 64, 96) and p["n_vertical"] in (32, 48, 64, 96)
+        assert p["n_azimuthal"] // p["n_radial"] in (2, 3, 4)
+        assert 1e2 <= p["beta"] <= 1e4 and 1.2 <= p["q"] <= 1.8
+        assert state.shape == (8,) + cfg.shape
+        assert cfg.size_x == p["n_azimuthal"] and cfg.size_y == p["n_radial"] + 8
+    total = sum(c.interior_cells for (c, _) in boxes)
+    assert 20e6 < total < 120e6
+
+
+def test_batch_rejects_unsupported_configs_on_cpu():
+    L = _lib.lib()
+    cfg, _ = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8)
+    bad = SolverConfig(**{**cfg.__dict__, "time_order": 1})
+    arr = (type(cfg.to_ctypes()) * 2)(cfg.to_ctypes(), bad.to_ctypes())
+    h = ctypes.c_void_p()
+    assert L.nmhd_batch_create(arr, 2, ctypes.byref(h)) == -1
+    assert b"box 1" in L.nmhd_batch_last_error(None)
+
+
+@pytest.mark.gpu
+def test_batch_boxes_equal_single_box_runs(gpu):
+    from nmhd_b200.batch import BatchSolver
+    from nmhd_b200.solver import MHDSolver
+    boxes, _ = small_ensemble()
+    # add two non-shearing boxes of other shapes (power-of-two and not)
+    boxes.append(orszag_tang_3d(16))
+    boxes.append(orszag_tang_3d(24, ny=20, nz=12))
+    steps = 9
+    with BatchSolver([c for c, _ in boxes]) as batch:
+        for i, (c, s) in enumerate(boxes):
+            batch.set_state(i, s)
+        batch.step(4)
+        batch.step(steps - 4)
+        for i, (c, s) in enumerate(boxes):
+            with MHDSolver(c) as one:
+                one.set_state(s)
+                one.step(steps)
+                t, g = batch.clock(i)
+                assert g == steps and t == one.current_time(), f"box {i} clock"
+                assert np.array_equal(batch.get_state(i), one.get_state()), f"box {i} state"
+
+
+@pytest.mark.gpu
+def test_batch_goal_time_per_box(gpu):
+    from nmhd_b200.batch import BatchSolver
+    from nmhd_b200.solver import MHDSolver
+    boxes, _ = small_ensemble(n=4, seed=8)
+    with BatchSolver([c for c, _ in boxes]) as batch:
+        for i, (c, s) in enumerate(boxes):
+            batch.set_state(i, s)
+        assert batch.proceed(0.05)
+        for i, (c, s) in enumerate(boxes):
+            with MHDSolver(c) as one:
+                one.set_state(s)
+                assert one.proceed(0.05)
+                t, g = batch.clock(i)
+                assert t == float(np.float32(0.05)) and g == one.generation()
+                assert np.array_equal(batch.get_state(i), one.get_state())
