@@ -41,6 +41,7 @@ WORKLOADS = {
                                           l_radial=1.0, l_azimuthal=4.0, l_vertical=1.0, seed=3),
 }
 REF_BINARY = {"mri_shearing_box_128x256x64": "shear256x128x64"}
+ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0)}
 BYTES_PER_CELL_UPDATE = 160  # 8 FP32 state words: stage 1 read+write, stage 2 2x read + write
 
 
@@ -292,19 +293,94 @@ def run_gpu_arm(args):
         dist.destroy_process_group()
 
 
+def run_ensemble_arm(args):
+    """Batched ensemble (64 uneven shearing boxes): aggregate interior
+    cell-updates/s of the batch, and of the same boxes stepped one by one
+    through the single-box path (plain per-box launches)."""
+    import torch
+    from nmhd_b200.batch import BatchSolver
+    from nmhd_b200.problems import mri_ensemble
+    from nmhd_b200.solver import MHDSolver
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    boxes, params = mri_ensemble(**ENSEMBLES[args.workload])
+    cfgs = [c for c, _ in boxes]
+    interior = sum(c.interior_cells for c in cfgs)
+    stream = torch.cuda.Stream(device=dev)
+    batch = BatchSolver(cfgs)
+    for i, (_, s) in enumerate(boxes):
+        batch.set_state(i, s)
+    batch.step(args.warmup)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    with ClockSampler(dev.index) as clocks:
+        t0 = time.perf_counter()
+        batch.step(args.steps)
+        torch.cuda.synchronize(dev)
+        wall = time.perf_counter() - t0
+    ms = wall * 1e3
+    if dist:
+        t = torch.tensor([ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * interior * args.steps / (ms * 1e-3) / 1e6
+    # plain: each box through its own single-box solver, one after another
+    plain_steps = max(3, args.steps // 4)
+    solvers = []
+    for c, s in boxes:
+        sol = MHDSolver(c)
+        sol.set_stream(stream.cuda_stream)
+        sol.set_state(s)
+        sol.step(args.warmup)
+        solvers.append(sol)
+    torch.cuda.synchronize(dev)
+    t0 = time.perf_counter()
+    for sol in solvers:
+        sol.step(plain_steps)
+    torch.cuda.synchronize(dev)
+    plain_wall = time.perf_counter() - t0
+    plain = interior * plain_steps / plain_wall / 1e6
+    for sol in solvers:
+        sol.close()
+    if rank == 0:
+        line = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded ensemble of shearing boxes)",
+            "config": {"workload": args.workload, "boxes": len(cfgs), "cells_interior": interior,
+                       "parallelism": "replicas" if world > 1 else "single",
+                       "timing": "host wallclock around proceed() (one sync per 16-step graph)"},
+            "plain_per_box": {"value": plain, "unit": "Mcell-updates/s", "steps": plain_steps,
+                              "note": "same boxes, one single-box solver each, stepped one after another"},
+            "batch_speedup": value / plain,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    if dist:
+        dist.destroy_process_group()
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=400)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="nmhd", choices=["nmhd", "reference"])
-    ap.add_argument("--workload", default="mri_shearing_box_128x256x64", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="mri_shearing_box_128x256x64",
+                    choices=sorted(WORKLOADS) + sorted(ENSEMBLES))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference_arm(args)
+    elif args.workload in ENSEMBLES:
+        run_ensemble_arm(args)
     else:
         run_gpu_arm(args)
 
