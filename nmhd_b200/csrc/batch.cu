@@ -25,7 +25,7 @@
 
 namespace nmhd {
 
-struct BoxDesc {
+struct __align__(8) BoxDesc {
   GridParams g;
   float *w0, *w1, *wp, *flux, *dt_hist;
   StepCtl *ctl;
@@ -62,10 +62,21 @@ __global__ void __launch_bounds__(kThreads, 3)
   __shared__ BoxDesc sb;
   __shared__ float red[kThreads / 32];
   const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
-  for (int t = blockIdx.x; t < total_tiles; t += gridDim.x) {
-    __syncthreads();  // the previous tile is done with sb
-    if (tid == 0) sb = boxes[find_box(nb, t, [&](int b) { return (long long)boxes[b].tile_begin; })];
-    __syncthreads();
+  // a contiguous range of tiles per CTA: consecutive tiles mostly share a box
+  const int t0 = (int)((long long)total_tiles * blockIdx.x / gridDim.x);
+  const int t1 = (int)((long long)total_tiles * (blockIdx.x + 1) / gridDim.x);
+  if (t0 >= t1) return;
+  int b = find_box(nb, t0, [&](int k) { return (long long)boxes[k].tile_begin; });
+  int b_end = -1;  // first tile past the box held in sb
+  for (int t = t0; t < t1; ++t) {
+    if (t >= b_end) {
+      if (b_end >= 0) ++b;  // boxes are laid out in tile order
+      __syncthreads();      // everyone is done with the previous box
+      constexpr int kWords = sizeof(BoxDesc) / sizeof(int);
+      if (tid < kWords) reinterpret_cast<int *>(&sb)[tid] = reinterpret_cast<const int *>(boxes + b)[tid];
+      __syncthreads();
+      b_end = sb.tile_begin + sb.tiles_x * sb.tiles_y * sb.tiles_z;
+    }
     const GridParams &g = sb.g;
     StepCtl *ctl = sb.ctl;
     if (ctl->done) continue;
