@@ -205,6 +205,60 @@ nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *gene
 nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
 const char *nmhd_batch_last_error(const nmhd_batch *b);
 
+/* ---- Differentiation ---------------------------------------------------------
+ * Gradients of a time-averaged diagnostic with respect to the initial state.
+ * No counterpart in the reference.  The differentiated step is the solver's
+ * own step with its time steps frozen (no derivative through the CFL dt) and
+ * its non-smooth choices frozen at the branch taken: minbee limiter slopes,
+ * the HLLD fan region, min/max of the wave speeds, sign(Bx) and the CT
+ * upwind corner selection.  All runs start from the solver's current state
+ * and clock and leave the solver's state, clock and time-step history
+ * unchanged.  `dt_seq` (host, nsteps floats) freezes the time steps; NULL
+ * means "the steps the CFL condition gives", i.e. exactly what nmhd_proceed
+ * would take from this state.  `dt_out` (host, nsteps floats, may be NULL)
+ * receives the time steps used.  At most NMHD_ADJOINT_MAX_STEPS steps. */
+#define NMHD_ADJOINT_MAX_STEPS 4096
+typedef enum nmhd_loss_kind {
+  /* J = (1/nw) sum_{n = first_step}^{last_step} <-Bx By>_n: the Maxwell stress
+   * of the state after n steps (n = 0: the initial state), averaged over the
+   * interior cells with B at cell centres (nmhd_diag.maxwell_stress), and over
+   * the nw = last_step - first_step + 1 states of the window. */
+  NMHD_LOSS_MAXWELL_STRESS = 1
+} nmhd_loss_kind;
+typedef struct nmhd_loss_spec {
+  int32_t kind;       /* nmhd_loss_kind */
+  int32_t first_step; /* 0 <= first_step <= last_step <= nsteps */
+  int32_t last_step;
+  int32_t reserved;   /* 0 */
+} nmhd_loss_spec;
+/* FP32 forward run of nsteps steps with the production kernels; *loss_out
+ * receives J. */
+nmhd_status nmhd_loss_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
+                          double *loss_out, float *dt_out);
+/* FP32 adjoint: J and dJ/d(initial state) in grad[8] (8 fields of Sx*Sy*Sz
+ * floats, host or device per on_device; margin entries that the first margin
+ * fill overwrites get 0).  The forward run stores a checkpoint every
+ * ckpt_every steps; the reverse sweep recomputes each segment from its
+ * checkpoint, keeping that segment's stage inputs and fluxes, then runs the
+ * hand-written adjoint kernels of every stage backwards. */
+nmhd_status nmhd_adjoint_run(nmhd_solver *s, int32_t nsteps, int32_t ckpt_every, const nmhd_loss_spec *loss,
+                             const float *dt_seq, double *loss_out, float *dt_out, float *const grad[8],
+                             int on_device);
+/* The same in FP64 (forward and adjoint in double from the float initial
+ * state); dt_seq is required; grad on the host. */
+nmhd_status nmhd_adjoint_run_f64(nmhd_solver *s, int32_t nsteps, int32_t ckpt_every,
+                                 const nmhd_loss_spec *loss, const float *dt_seq, double *loss_out,
+                                 double *const grad[8]);
+/* FP64 tangent-linear run: J and its directional derivative dJ[dir] along
+ * dir[8] (host, 8 fields of Sx*Sy*Sz doubles; NULL: J only), forward mode in
+ * double from the float initial state.  dt_seq is required. */
+nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
+                         const double *const dir[8], double *loss_out, double *dloss_out);
+/* Device time of the last nmhd_adjoint_run / nmhd_adjoint_run_f64 in ms:
+ * [0] forward run with checkpoints, [1] segment recomputation, [2] adjoint
+ * kernels, [3] the whole run. */
+nmhd_status nmhd_adjoint_timing(const nmhd_solver *s, double ms_out[4]);
+
 /* Library version string. */
 const char *nmhd_version(void);
 

@@ -22,6 +22,18 @@ ERRORS = {
     -5: "numerical error", -6: "out of device memory", -7: "not supported",
 }
 
+
+
+class LossSpec(ctypes.Structure):
+    """nmhd_loss_spec: J = mean over states first_step..last_step of the
+    volume-averaged Maxwell stress -<Bx By>."""
+    _fields_ = [("kind", ctypes.c_int32), ("first_step", ctypes.c_int32),
+                ("last_step", ctypes.c_int32), ("reserved", ctypes.c_int32)]
+
+
+LOSS_MAXWELL_STRESS = 1
+ADJOINT_MAX_STEPS = 4096
+
 # Every entry point declared in include/nmhd.h: (name, restype, argtypes)
 _P = ctypes.c_void_p
 _SIGS = [
@@ -50,6 +62,14 @@ _SIGS = [
                                             ctypes.POINTER(ctypes.c_int64), ctypes.c_double,
                                             ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), _P]),
     ("nmhd_noalloc_last_error", ctypes.c_char_p, []),
+    ("nmhd_loss_run", ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.POINTER(ctypes.c_double), _P]),
+    ("nmhd_adjoint_run", ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                        ctypes.POINTER(ctypes.c_double), _P, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_adjoint_run_f64", ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, _P,
+                                            ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_P)]),
+    ("nmhd_tlm_run", ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.POINTER(_P),
+                                    ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
+    ("nmhd_adjoint_timing", ctypes.c_int, [_P, _P]),
     ("nmhd_batch_create", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
     ("nmhd_batch_destroy", None, [_P]),
     ("nmhd_batch_size", ctypes.c_int, [_P]),

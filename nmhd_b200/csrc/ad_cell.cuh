@@ -1,0 +1,660 @@
+// Per-cell operations of the differentiated time step.
+//
+// Forward (generic scalar T, see ad_scalar.cuh): the margin fill and the three
+// parts of an RK stage exactly as the production kernels (cell_ops.cuh,
+// margin_ops.cuh) evaluate them, operation for operation, with plain
+// divisions by the spacing.  With T = float they reproduce the FP32 step,
+// with T = double the reference's Real = double build, with T = Dual<double>
+// the FP64 tangent-linear step.
+//
+// Adjoint (real R = float or double): the transpose of the linearised stage
+// with dt, the limiter choices, the Riemann fan region and the CT upwind
+// choices frozen at the values the forward took.  Every adjoint part is a
+// gather (each cell writes only its own entries), so no atomics are needed
+// and results are deterministic:
+//   a_prim_cell    to_primitive + kick + conserved update (per cell)
+//   a_bface_cell   face-B adjoint: output B, energy terms of old and new B
+//   a_flux_cell    CT transpose and flux divergence transpose -> adjoint of the
+//                  21 face fluxes of the cell -> HLLD adjoint per face
+//   a_recon_cell   minbee reconstruction, face kick and normal-B transposes
+//   a_bc_cell      transverse cell-centred B average transpose
+//   a_fill_*       transpose of the shearing-periodic and Z margin fills
+// References: src/library/mhd_solver.inlrb:140-155 (reconstruction), 184-259
+// (shear fill), 562-714 (flux, CT), 762-848 (conversions, update, kick).
+#pragma once
+#include "ad_hlld.cuh"
+
+namespace nmhd {
+namespace ad {
+
+// Grid constants in precision R (the reference's derived constants,
+// simulation_config_default.h:56-103, evaluated in R).
+template <class R>
+struct GGrid {
+  int sx, sy, sz, n, my, mz, shear, order2;
+  R dx, dy, dz, gamma, cfl, q, omega, corner_y, extent_x;
+  double rel_vel;
+};
+
+NMHD_HD int wrapc(int v, int s) {
+  while (v < 0) v += s;
+  while (v >= s) v -= s;
+  return v;
+}
+
+template <class R>
+NMHD_HD int cell_at(const GGrid<R> &g, int x, int y, int z) {
+  return (wrapc(z, g.sz) * g.sy + wrapc(y, g.sy)) * g.sx + wrapc(x, g.sx);
+}
+
+// (x, y, z) + k along axis a
+template <class R>
+NMHD_HD int shifted(const GGrid<R> &g, int x, int y, int z, int a, int k) {
+  return cell_at(g, x + (a == 0 ? k : 0), y + (a == 1 ? k : 0), z + (a == 2 ? k : 0));
+}
+
+template <class R>
+NMHD_HD R spacing(const GGrid<R> &g, int a) {
+  return a == 0 ? g.dx : (a == 1 ? g.dy : g.dz);
+}
+
+// ---------------------------------------------------------------------------
+// Forward
+template <class T>
+NMHD_HD T absolute_smaller_g(const T &a, const T &b) {
+  typedef typename Traits<T>::real R;
+  return val(a) * val(b) <= R(0) ? to<T>(R(0)) : (gabs(a) < gabs(b) ? a : b);
+}
+
+template <class T>
+NMHD_HD void reconstruct4_g(const T &x0, const T &x1, const T &x2, const T &x3, T &left, T &right) {
+  const T d01 = x1 - x0;
+  const T d12 = x2 - x1;
+  const T d23 = x3 - x2;
+  const T d1 = absolute_smaller_g(d01, d12);
+  const T d2 = absolute_smaller_g(d12, d23);
+  left = x1 + d1 / to<T>(2.0f);
+  right = x2 - d2 / to<T>(2.0f);
+}
+
+// Riemann input of the lower ax-face of cell (x, y, z): reconstruction,
+// transverse B averages and the face half-kick (calc_flux_kernel).
+template <class T, class R>
+NMHD_HD void face_input(const GGrid<R> &g, const T *w, int x, int y, int z, int ax, const T &h, HState<T> &in,
+                        T &bn) {
+  const size_t N = (size_t)g.n;
+  const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
+  int c[4];
+  for (int t = 0; t < 4; ++t) c[t] = shifted(g, x, y, z, ax, t - 2);
+  const T *rho = w, *p = w + 4 * N;
+  const T *vn = w + (1 + ax) * N, *v1 = w + (1 + e1) * N, *v2 = w + (1 + e2) * N;
+  const T *b1 = w + (5 + e1) * N, *b2 = w + (5 + e2) * N;
+  T bc1[4], bc2[4];
+  for (int t = 0; t < 4; ++t) {
+    const int cx = x + (ax == 0 ? t - 2 : 0), cy = y + (ax == 1 ? t - 2 : 0), cz = z + (ax == 2 ? t - 2 : 0);
+    bc1[t] = to<T>(0.5f) * (b1[c[t]] + b1[shifted(g, cx, cy, cz, e1, 1)]);
+    bc2[t] = to<T>(0.5f) * (b2[c[t]] + b2[shifted(g, cx, cy, cz, e2, 1)]);
+  }
+  if (g.order2) {
+    reconstruct4_g(rho[c[0]], rho[c[1]], rho[c[2]], rho[c[3]], in.dl, in.dr);
+    reconstruct4_g(vn[c[0]], vn[c[1]], vn[c[2]], vn[c[3]], in.ul, in.ur);
+    reconstruct4_g(v1[c[0]], v1[c[1]], v1[c[2]], v1[c[3]], in.vl, in.vr);
+    reconstruct4_g(v2[c[0]], v2[c[1]], v2[c[2]], v2[c[3]], in.wl, in.wr);
+    reconstruct4_g(p[c[0]], p[c[1]], p[c[2]], p[c[3]], in.pl, in.pr);
+    reconstruct4_g(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
+    reconstruct4_g(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
+  } else {
+    in.dl = rho[c[1]]; in.dr = rho[c[2]];
+    in.ul = vn[c[1]]; in.ur = vn[c[2]];
+    in.vl = v1[c[1]]; in.vr = v1[c[2]];
+    in.wl = v2[c[1]]; in.wr = v2[c[2]];
+    in.pl = p[c[1]]; in.pr = p[c[2]];
+    in.byl = bc1[1]; in.byr = bc1[2];
+    in.bzl = bc2[1]; in.bzr = bc2[2];
+  }
+  if (g.shear) {
+    T acc;
+    if (ax == 0) {
+      const T vY = to<T>(0.5f) * (w[2 * N + c[1]] + w[2 * N + c[2]]);
+      acc = to<T>(-2.0f) * to<T>(g.omega) * vY;
+    } else if (ax == 1) {
+      const T vX = to<T>(0.5f) * (w[N + c[1]] + w[N + c[2]]);
+      acc = to<T>(2.0f) * to<T>(g.omega) * vX +
+            to<T>(R(2.0f) * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((R)y + R(0.5f))));
+    } else {
+      acc = to<T>(R(0));
+    }
+    const T mbv = to<T>(0.5f) * h * acc;
+    in.ul = in.ul + mbv;
+    in.ur = in.ur + mbv;
+  }
+  bn = w[(5 + ax) * N + c[2]];
+}
+
+// The three lower-face fluxes of a cell (7 per face; momentum in absolute
+// components, then F(B_e1), F(B_e2)) into flux + (7*ax + k)*N.
+template <class T, class R>
+NMHD_HD void g_flux_cell(const GGrid<R> &g, const T *w, T *flux, int x, int y, int z, const T &h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  for (int ax = 0; ax < 3; ++ax) {
+    const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
+    HState<T> in;
+    T bn;
+    face_input(g, w, x, y, z, ax, h, in, bn);
+    T f[7];
+    hlld_g(to<T>(g.gamma), bn, in, f);
+    T *out = flux + (size_t)(7 * ax) * N + o;
+    out[0] = f[0];
+    out[(1 + ax) * N] = f[1];
+    out[(1 + e1) * N] = f[2];
+    out[(1 + e2) * N] = f[3];
+    out[4 * N] = f[4];
+    out[5 * N] = f[5];
+    out[6 * N] = f[6];
+  }
+}
+
+// Upwind edge flux (corner_magnet_flux): the a-flux of B_b at edge e,
+// F[e - b] if the 4-cell wind sum is positive, F[e] if negative, else the mean.
+template <class T, class R>
+NMHD_HD T g_corner(const GGrid<R> &g, const T *vb, const T *fb, int x, int y, int z, int a, int b) {
+  const int e = cell_at(g, x, y, z);
+  const int eb = shifted(g, x, y, z, b, -1);
+  const int ea = shifted(g, x, y, z, a, -1);
+  const int eab = cell_at(g, x - (a == 0 || b == 0), y - (a == 1 || b == 1), z - (a == 2 || b == 2));
+  const T w = vb[e] + vb[eb] + vb[ea] + vb[eab];
+  typedef typename Traits<T>::real RR;
+  const T f0 = fb[eb], f1 = fb[e];
+  return val(w) > RR(0) ? f0 : (val(w) < RR(0) ? f1 : to<T>(0.5f) * (f0 + f1));
+}
+
+// Face-B update of the cell's three lower faces (constrained transport).
+template <class T, class R>
+NMHD_HD void g_ct_cell(const GGrid<R> &g, const T *win, const T *wb, T *wo, const T *flux, int x, int y, int z,
+                       const T &h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  const T *vx = win + N, *vy = win + 2 * N, *vz = win + 3 * N;
+  const T *FxBy = flux + 5 * N, *FxBz = flux + 6 * N;
+  const T *FyBz = flux + 12 * N, *FyBx = flux + 13 * N;
+  const T *FzBx = flux + 19 * N, *FzBy = flux + 20 * N;
+  const T XY00 = g_corner(g, vy, FxBy, x, y, z, 0, 1), XY01 = g_corner(g, vy, FxBy, x, y + 1, z, 0, 1);
+  const T XY10 = g_corner(g, vy, FxBy, x + 1, y, z, 0, 1);
+  const T YX00 = g_corner(g, vx, FyBx, x, y, z, 1, 0), YX01 = g_corner(g, vx, FyBx, x, y + 1, z, 1, 0);
+  const T YX10 = g_corner(g, vx, FyBx, x + 1, y, z, 1, 0);
+  const T XZ00 = g_corner(g, vz, FxBz, x, y, z, 0, 2), XZ01 = g_corner(g, vz, FxBz, x, y, z + 1, 0, 2);
+  const T XZ10 = g_corner(g, vz, FxBz, x + 1, y, z, 0, 2);
+  const T ZX00 = g_corner(g, vx, FzBx, x, y, z, 2, 0), ZX01 = g_corner(g, vx, FzBx, x, y, z + 1, 2, 0);
+  const T ZX10 = g_corner(g, vx, FzBx, x + 1, y, z, 2, 0);
+  const T YZ00 = g_corner(g, vz, FyBz, x, y, z, 1, 2), YZ01 = g_corner(g, vz, FyBz, x, y, z + 1, 1, 2);
+  const T YZ10 = g_corner(g, vz, FyBz, x, y + 1, z, 1, 2);
+  const T ZY00 = g_corner(g, vy, FzBy, x, y, z, 2, 1), ZY01 = g_corner(g, vy, FzBy, x, y, z + 1, 2, 1);
+  const T ZY10 = g_corner(g, vy, FzBy, x, y + 1, z, 2, 1);
+  const T dx = to<T>(g.dx), dy = to<T>(g.dy), dz = to<T>(g.dz), half = to<T>(0.5f);
+  T pb = to<T>(0.0f);
+  pb = pb + half * ((XY01 - XY00) / dy + (XZ01 - XZ00) / dz);
+  pb = pb - half * (YX01 - YX00) / dy;
+  pb = pb - half * (ZX01 - ZX00) / dz;
+  wo[5 * N + o] = wb[5 * N + o] + h * pb;
+  pb = to<T>(0.0f);
+  pb = pb - half * (XY10 - XY00) / dx;
+  pb = pb + half * ((YZ01 - YZ00) / dz + (YX10 - YX00) / dx);
+  pb = pb - half * (ZY01 - ZY00) / dz;
+  wo[6 * N + o] = wb[6 * N + o] + h * pb;
+  pb = to<T>(0.0f);
+  pb = pb - half * (XZ10 - XZ00) / dx;
+  pb = pb - half * (YZ10 - YZ00) / dy;
+  pb = pb + half * ((ZX10 - ZX00) / dx + (ZY10 - ZY00) / dy);
+  wo[7 * N + o] = wb[7 * N + o] + h * pb;
+}
+
+// Flux divergence, conserved update, primitive recovery with the new face B
+// and the Kepler kick (cell fields of wo; its face B come from g_ct_cell).
+template <class T, class R>
+NMHD_HD void g_prim_cell(const GGrid<R> &g, const T *wb, T *wo, const T *flux, int x, int y, int z, const T &h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  const int oxp = cell_at(g, x + 1, y, z), oyp = cell_at(g, x, y + 1, z), ozp = cell_at(g, x, y, z + 1);
+  const T *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+  const T dx = to<T>(g.dx), dy = to<T>(g.dy), dz = to<T>(g.dz);
+  T pace[5];
+  for (int v = 0; v < 5; ++v) {
+    T pc = to<T>(0.0f);
+    pc = pc + (Fx[v * N + o] - Fx[v * N + oxp]) / dx;
+    pc = pc + (Fy[v * N + o] - Fy[v * N + oyp]) / dy;
+    pc = pc + (Fz[v * N + o] - Fz[v * N + ozp]) / dz;
+    pace[v] = pc;
+  }
+  const T gm1 = to<T>(g.gamma) - to<T>(1.0f);
+  const T rho0 = wb[o], vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o], p0 = wb[4 * N + o];
+  const T bxl = wb[5 * N + o], bxh = wb[5 * N + oxp];
+  const T byl = wb[6 * N + o], byh = wb[6 * N + oyp];
+  const T bzl = wb[7 * N + o], bzh = wb[7 * N + ozp];
+  const T mx0 = rho0 * vx0, my0 = rho0 * vy0, mz0 = rho0 * vz0;
+  const T e0 = p0 / gm1 + to<T>(0.5f) * rho0 * (vx0 * vx0 + vy0 * vy0 + vz0 * vz0) +
+               to<T>(0.25f) * (bxl * bxl + bxh * bxh + byl * byl + byh * byh + bzl * bzl + bzh * bzh);
+  const T rho = rho0 + h * pace[0];
+  const T mx = mx0 + h * pace[1];
+  const T my = my0 + h * pace[2];
+  const T mz = mz0 + h * pace[3];
+  const T ene = e0 + h * pace[4];
+  const T bx0 = wo[5 * N + o], bx1 = wo[5 * N + oxp];
+  const T by0 = wo[6 * N + o], by1 = wo[6 * N + oyp];
+  const T bz0 = wo[7 * N + o], bz1 = wo[7 * N + ozp];
+  T vxo = mx / rho, vyo = my / rho, vzo = mz / rho;
+  const T eint = ene - to<T>(0.5f) * (mx * mx + my * my + mz * mz) / rho -
+                 to<T>(0.25f) * (bx0 * bx0 + bx1 * bx1 + by0 * by0 + by1 * by1 + bz0 * bz0 + bz1 * bz1);
+  const T po = eint * gm1;
+  if (g.shear) {
+    const T ax = to<T>(-2.0f) * to<T>(g.omega) * vyo;
+    const T ay = to<T>(2.0f) * to<T>(g.omega) * vxo +
+                 to<T>(R(2.0f) * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((R)y + R(0.5f))));
+    vxo = vxo + h * ax;
+    vyo = vyo + h * ay;
+    vzo = vzo + h * to<T>(0.0f);
+  }
+  wo[o] = rho;
+  wo[N + o] = vxo;
+  wo[2 * N + o] = vyo;
+  wo[3 * N + o] = vzo;
+  wo[4 * N + o] = po;
+}
+
+// Shearing-periodic Y-margin fill, one item (sx, sy, sz) with sy < margin_y
+// (communicate_gather/scatter_kernel_y with relative_displacement).
+template <class R>
+NMHD_HD void shear_shift(const GGrid<R> &g, double time, int &dint, R &f) {
+  const double d0 = 0.0 + time * g.rel_vel;
+  const int fold = (int)floor(d0 / (double)g.extent_x);
+  const double d1 = d0 - (double)((R)fold * g.extent_x);
+  dint = (int)floor(d1 / (double)g.dx);
+  f = (R)(d1 / (double)g.dx - dint);
+}
+
+template <class T, class R>
+NMHD_HD void g_fill_y_item(const GGrid<R> &g, double time, T *w, int idx) {
+  const int M = g.my;
+  const int sx = idx % g.sx;
+  const int sy = (idx / g.sx) % M;
+  const int sz = idx / (g.sx * M);
+  int dint;
+  R f;
+  shear_shift(g, time, dint, f);
+  const R rv = (R)g.rel_vel;
+  const int inc_x = wrapc((sx + dint) % g.sx, g.sx);
+  const int dec_x = wrapc((sx - dint - 1) % g.sx, g.sx);
+  const size_t N = (size_t)g.n;
+  const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + inc_x;
+  const int src_dec = (sz * g.sy + (M + sy)) * g.sx + dec_x;
+  const int dst_lo = (sz * g.sy + sy) * g.sx + sx;
+  const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx;
+  const T omf = to<T>(R(1.0f) - f), ff = to<T>(f);
+  for (int v = 0; v < 8; ++v) {
+    const T vi = w[v * N + src_inc];
+    const T vd = w[v * N + src_dec];
+    T bi = omf * vi + ff * vi;
+    T bd = ff * vd + omf * vd;
+    if (v == 1) {
+      bi = bi - to<T>(rv);
+      bd = bd + to<T>(rv);
+    }
+    w[v * N + dst_lo] = bi;
+    if (!(v == 6 && sy == 0)) w[v * N + dst_hi] = bd;
+  }
+}
+
+// Plain periodic Z-margin copy, one item of the sx*sy*mz plane block.
+template <class T, class R>
+NMHD_HD void g_fill_z_item(const GGrid<R> &g, T *w, int idx) {
+  const size_t n = (size_t)g.n, unit = (size_t)g.sx * g.sy * g.mz;
+  for (int v = 0; v < 8; ++v) {
+    T *var = w + v * n;
+    const T lo = var[n - 2 * unit + idx];
+    const T hi = var[unit + idx];
+    var[idx] = lo;
+    var[n - unit + idx] = hi;
+  }
+}
+
+// -<Bx By> of one interior cell at the cell centre (the diagnostics' Maxwell
+// stress), in FP64 (or its dual).
+template <class T>
+struct Wide64 { typedef double type; };
+template <class R>
+struct Wide64<Dual<R>> { typedef Dual<double> type; };
+
+template <class T, class R>
+NMHD_HD typename Wide64<T>::type g_stress_cell(const GGrid<R> &g, const T *w, int x, int y, int z) {
+  typedef typename Wide64<T>::type D;
+  const size_t N = (size_t)g.n;
+  if (y < g.my || y >= g.sy - g.my || z < g.mz || z >= g.sz - g.mz) return to<D>(0.0);
+  const int o = cell_at(g, x, y, z);
+  const D bxl = to<D>(w[5 * N + o]), bxh = to<D>(w[5 * N + cell_at(g, x + 1, y, z)]);
+  const D byl = to<D>(w[6 * N + o]), byh = to<D>(w[6 * N + cell_at(g, x, y + 1, z)]);
+  return -(to<D>(0.25) * (bxl + bxh) * (byl + byh));
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint.  Scratch layout (N values per field):
+//   lamU  5 fields: adjoint of the updated conserved state (rho, m_x, m_y,
+//         m_z, E) of the stage, which is also that of the conserved state
+//         before it;
+//   lamE  1 field: adjoint of the internal energy;
+//   lamBn 3 fields: adjoint of the new face B (x, y, z);
+//   face  45 fields: per axis ax, 15 values at face + (15*ax + k)*N: the
+//         adjoints of the Riemann input (dl, dr, ul, ur, vl, vr, wl, wr, pl,
+//         pr, byl, byr, bzl, bzr) and of the normal face B;
+//   lamBc 3 fields: adjoint of the cell-centred transverse B averages.
+
+template <class R>
+NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R *lout, R *lamU, R *lamE, R *lb,
+                         int x, int y, int z, R h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  const int oxp = cell_at(g, x + 1, y, z), oyp = cell_at(g, x, y + 1, z), ozp = cell_at(g, x, y, z + 1);
+  const R *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+  R pace[4];
+  for (int v = 0; v < 4; ++v) {
+    R pc = R(0);
+    pc = pc + (Fx[v * N + o] - Fx[v * N + oxp]) / g.dx;
+    pc = pc + (Fy[v * N + o] - Fy[v * N + oyp]) / g.dy;
+    pc = pc + (Fz[v * N + o] - Fz[v * N + ozp]) / g.dz;
+    pace[v] = pc;
+  }
+  const R gm1 = g.gamma - R(1.0f);
+  const R rho0 = wb[o], vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o];
+  const R rho = rho0 + h * pace[0];
+  const R mx = rho0 * vx0 + h * pace[1];
+  const R my = rho0 * vy0 + h * pace[2];
+  const R mz = rho0 * vz0 + h * pace[3];
+  R l_vx = lout[N + o], l_vy = lout[2 * N + o];
+  const R l_vz = lout[3 * N + o];
+  if (g.shear) {
+    // vx' = vx - 2 omega h vy,  vy' = vy + 2 omega h vx + const
+    const R c = R(2.0f) * g.omega * h;
+    const R lx = l_vx + c * l_vy;
+    const R ly = l_vy - c * l_vx;
+    l_vx = lx;
+    l_vy = ly;
+  }
+  const R l_eint = gm1 * lout[4 * N + o];
+  const R r2 = rho * rho;
+  const R l_mx = l_vx / rho - l_eint * mx / rho;
+  const R l_my = l_vy / rho - l_eint * my / rho;
+  const R l_mz = l_vz / rho - l_eint * mz / rho;
+  const R l_rho = lout[o] - (l_vx * mx + l_vy * my + l_vz * mz) / r2 +
+                  l_eint * R(0.5f) * (mx * mx + my * my + mz * mz) / r2;
+  const R l_ene = l_eint;
+  lamU[o] = l_rho;
+  lamU[N + o] = l_mx;
+  lamU[2 * N + o] = l_my;
+  lamU[3 * N + o] = l_mz;
+  lamU[4 * N + o] = l_ene;
+  lamE[o] = l_eint;
+  // conserved state before the stage from the base primitives
+  lb[o] += l_rho + l_mx * vx0 + l_my * vy0 + l_mz * vz0 + l_ene * R(0.5f) * (vx0 * vx0 + vy0 * vy0 + vz0 * vz0);
+  lb[N + o] += (l_mx + l_ene * vx0) * rho0;
+  lb[2 * N + o] += (l_my + l_ene * vy0) * rho0;
+  lb[3 * N + o] += (l_mz + l_ene * vz0) * rho0;
+  lb[4 * N + o] += l_ene / gm1;
+}
+
+template <class R>
+NMHD_HD void a_bface_cell(const GGrid<R> &g, const R *wb, const R *wo, const R *lout, const R *lamU, const R *lamE,
+                          R *lamBn, R *lb, int x, int y, int z) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  for (int a = 0; a < 3; ++a) {
+    const int om = shifted(g, x, y, z, a, -1);
+    const size_t fb = (size_t)(5 + a) * N;
+    const R l = lout[fb + o] - R(0.5f) * wo[fb + o] * (lamE[o] + lamE[om]);
+    lamBn[a * N + o] = l;
+    lb[fb + o] += l + R(0.5f) * wb[fb + o] * (lamU[4 * N + o] + lamU[4 * N + om]);
+  }
+}
+
+// Upwind weights of the corner at edge (x, y, z): c0 on F[e - b], c1 on F[e].
+template <class R>
+NMHD_HD void corner_weights(const GGrid<R> &g, const R *vb, int x, int y, int z, int a, int b, R &c0, R &c1) {
+  const int e = cell_at(g, x, y, z);
+  const int eb = shifted(g, x, y, z, b, -1);
+  const int ea = shifted(g, x, y, z, a, -1);
+  const int eab = cell_at(g, x - (a == 0 || b == 0), y - (a == 1 || b == 1), z - (a == 2 || b == 2));
+  const R w = vb[e] + vb[eb] + vb[ea] + vb[eab];
+  c0 = w > R(0) ? R(1) : (w < R(0) ? R(0) : R(0.5f));
+  c1 = w > R(0) ? R(0) : (w < R(0) ? R(1) : R(0.5f));
+}
+
+// Adjoint of the corner value C = F_a(B_b) at edge (x, y, z).  In every
+// family (XY, YX, XZ, ZX, YZ, ZY) the corner enters the face-B updates as
+//   dB_a[o] = +h/2 (C[o+b] - C[o]) / d_b,   dB_b[o] = -h/2 (C[o+a] - C[o]) / d_a.
+template <class R>
+NMHD_HD R corner_adj(const GGrid<R> &g, const R *lamBn, int x, int y, int z, int a, int b, R h) {
+  const size_t N = (size_t)g.n;
+  const int e = cell_at(g, x, y, z);
+  const R la_here = lamBn[a * N + e], la_below = lamBn[a * N + shifted(g, x, y, z, b, -1)];
+  const R lb_here = lamBn[b * N + e], lb_below = lamBn[b * N + shifted(g, x, y, z, a, -1)];
+  const R ca = h * R(0.5f) / spacing(g, b);
+  const R cb = h * R(0.5f) / spacing(g, a);
+  return ca * (la_below - la_here) - cb * (lb_below - lb_here);
+}
+
+// Adjoint of the flux F_a(B_b) at the cell's lower a-face.
+template <class R>
+NMHD_HD R ct_flux_adj(const GGrid<R> &g, const R *win, const R *lamBn, int x, int y, int z, int a, int b, R h) {
+  const size_t N = (size_t)g.n;
+  const R *vb = win + (1 + b) * N;
+  R c0, c1, d0, d1;
+  corner_weights(g, vb, x, y, z, a, b, c0, c1);
+  const int xb = x + (b == 0), yb = y + (b == 1), zb = z + (b == 2);
+  corner_weights(g, vb, xb, yb, zb, a, b, d0, d1);
+  return c1 * corner_adj(g, lamBn, x, y, z, a, b, h) + d0 * corner_adj(g, lamBn, xb, yb, zb, a, b, h);
+}
+
+template <class R>
+NMHD_HD void a_flux_cell(const GGrid<R> &g, const R *win, const R *lamBn, const R *lamU, R *face, int x, int y,
+                         int z, R h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  for (int ax = 0; ax < 3; ++ax) {
+    const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
+    const int om = shifted(g, x, y, z, ax, -1);
+    const R c = h / spacing(g, ax);
+    R lfa[5];
+    for (int k = 0; k < 5; ++k) lfa[k] = c * (lamU[k * N + o] - lamU[k * N + om]);
+    R lf[7];
+    lf[0] = lfa[0];
+    lf[1] = lfa[1 + ax];
+    lf[2] = lfa[1 + e1];
+    lf[3] = lfa[1 + e2];
+    lf[4] = lfa[4];
+    lf[5] = ct_flux_adj(g, win, lamBn, x, y, z, ax, e1, h);
+    lf[6] = ct_flux_adj(g, win, lamBn, x, y, z, ax, e2, h);
+    HState<R> in;
+    R bn;
+    face_input(g, win, x, y, z, ax, h, in, bn);
+    HState<R> ls;
+    R lbn;
+    hlld_adjoint(g.gamma, bn, in, lf, ls, lbn);
+    R *fo = face + (size_t)(15 * ax) * N + o;
+    fo[0] = ls.dl; fo[N] = ls.dr; fo[2 * N] = ls.ul; fo[3 * N] = ls.ur;
+    fo[4 * N] = ls.vl; fo[5 * N] = ls.vr; fo[6 * N] = ls.wl; fo[7 * N] = ls.wr;
+    fo[8 * N] = ls.pl; fo[9 * N] = ls.pr; fo[10 * N] = ls.byl; fo[11 * N] = ls.byr;
+    fo[12 * N] = ls.bzl; fo[13 * N] = ls.bzr; fo[14 * N] = lbn;
+  }
+}
+
+// Minbee choice of absolute_smaller(a, b): 0 -> zero slope, 1 -> a, 2 -> b.
+template <class R>
+NMHD_HD int mm_choice(R a, R b) {
+  return a * b <= R(0) ? 0 : (gabs(a) < gabs(b) ? 1 : 2);
+}
+
+// Transpose of the reconstruction of one variable q along axis ax at cell c:
+// q7[k] = q at c + k - 3; lamL[j], lamR[j] = adjoints of the left / right
+// states of face c + j - 1 (j = 0..3).  Returns the adjoint of q[c].
+template <class R>
+NMHD_HD R recon_adj(int order2, const R q7[7], const R lamL[4], const R lamR[4]) {
+  if (!order2) return lamL[2] + lamR[1];  // left of face c+1, right of face c
+  R acc = R(0);
+  for (int j = 0; j < 4; ++j) {
+    // face f = c + j - 1 uses x0..x3 = q[f-2..f+1] = q7[j..j+3]; c is x_(3-j)
+    const R x0 = q7[j], x1 = q7[j + 1], x2 = q7[j + 2], x3 = q7[j + 3];
+    const int cl = mm_choice(x1 - x0, x2 - x1);
+    const int cr = mm_choice(x2 - x1, x3 - x2);
+    const int t = 3 - j;
+    R dl, dr;
+    // left = x1 + d1/2: d1 = 0 | x1 - x0 | x2 - x1
+    if (cl == 0) dl = (t == 1) ? R(1) : R(0);
+    else if (cl == 1) dl = (t == 0) ? R(-0.5f) : ((t == 1) ? R(1.5f) : R(0));
+    else dl = (t == 1 || t == 2) ? R(0.5f) : R(0);
+    // right = x2 - d2/2: d2 = 0 | x2 - x1 | x3 - x2
+    if (cr == 0) dr = (t == 2) ? R(1) : R(0);
+    else if (cr == 1) dr = (t == 1 || t == 2) ? R(0.5f) : R(0);
+    else dr = (t == 2) ? R(1.5f) : ((t == 3) ? R(-0.5f) : R(0));
+    acc += lamL[j] * dl + lamR[j] * dr;
+  }
+  return acc;
+}
+
+template <class R>
+NMHD_HD void a_recon_cell(const GGrid<R> &g, const R *win, const R *face, R *lin, R *lamBc, int x, int y, int z,
+                          R h) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  R lcell[5] = {R(0), R(0), R(0), R(0), R(0)};  // rho, vx, vy, vz, p
+  R lbc[3] = {R(0), R(0), R(0)};
+  for (int ax = 0; ax < 3; ++ax) {
+    const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
+    int c7[7];
+    for (int k = 0; k < 7; ++k) c7[k] = shifted(g, x, y, z, ax, k - 3);
+    int f4[4];  // faces c-1 .. c+2
+    for (int j = 0; j < 4; ++j) f4[j] = c7[j + 2];
+    const R *fa = face + (size_t)(15 * ax) * N;
+    // cell variables: rho, v_n, v_t1, v_t2, p
+    const int var[5] = {0, 1 + ax, 1 + e1, 1 + e2, 4};
+    for (int k = 0; k < 5; ++k) {
+      R q7[7], lL[4], lR[4];
+      for (int m = 0; m < 7; ++m) q7[m] = win[var[k] * N + c7[m]];
+      for (int j = 0; j < 4; ++j) {
+        lL[j] = fa[(2 * k) * N + f4[j]];
+        lR[j] = fa[(2 * k + 1) * N + f4[j]];
+      }
+      lcell[var[k]] += recon_adj(g.order2, q7, lL, lR);
+    }
+    // transverse B averages (components e1, e2)
+    for (int k = 0; k < 2; ++k) {
+      const int comp = k == 0 ? e1 : e2;
+      const R *b = win + (5 + comp) * N;
+      R q7[7], lL[4], lR[4];
+      for (int m = 0; m < 7; ++m) {
+        const int cx = x + (ax == 0 ? m - 3 : 0), cy = y + (ax == 1 ? m - 3 : 0), cz = z + (ax == 2 ? m - 3 : 0);
+        q7[m] = R(0.5f) * (b[c7[m]] + b[shifted(g, cx, cy, cz, comp, 1)]);
+      }
+      for (int j = 0; j < 4; ++j) {
+        lL[j] = fa[(10 + 2 * k) * N + f4[j]];
+        lR[j] = fa[(11 + 2 * k) * N + f4[j]];
+      }
+      lbc[comp] += recon_adj(g.order2, q7, lL, lR);
+    }
+    // face half-kick: mbv(f) = h/2 * acc(f), acc from the two cells of face f
+    if (g.shear && ax < 2) {
+      const R lm = (fa[2 * N + o] + fa[3 * N + o]) + (fa[2 * N + f4[2]] + fa[3 * N + f4[2]]);
+      // faces c (f4[1] = o) and c+1 (f4[2]); d acc / d v = -2 omega / 2 (ax 0, v_y) or +2 omega / 2 (ax 1, v_x)
+      const R c = R(0.5f) * h * (ax == 0 ? -g.omega : g.omega);
+      lcell[ax == 0 ? 2 : 1] += c * lm;
+    }
+    // normal field of face c
+    lin[(5 + ax) * N + o] += fa[14 * N + o];
+  }
+  for (int v = 0; v < 5; ++v) lin[v * N + o] += lcell[v];
+  for (int c = 0; c < 3; ++c) lamBc[c * N + o] = lbc[c];
+}
+
+template <class R>
+NMHD_HD void a_bc_cell(const GGrid<R> &g, const R *lamBc, R *lin, int x, int y, int z) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  for (int c = 0; c < 3; ++c)
+    lin[(5 + c) * N + o] += R(0.5f) * (lamBc[c * N + o] + lamBc[c * N + shifted(g, x, y, z, c, -1)]);
+}
+
+// Transpose of g_fill_z_item (one item; margins read, added to their sources
+// and cleared by the same thread).
+template <class R>
+NMHD_HD void a_fill_z_item(const GGrid<R> &g, R *lam, int idx) {
+  const size_t n = (size_t)g.n, unit = (size_t)g.sx * g.sy * g.mz;
+  for (int v = 0; v < 8; ++v) {
+    R *var = lam + v * n;
+    const R lo = var[idx], hi = var[n - unit + idx];
+    var[idx] = R(0);
+    var[n - unit + idx] = R(0);
+    var[n - 2 * unit + idx] += lo;
+    var[unit + idx] += hi;
+  }
+}
+
+// Transpose of g_fill_y_item, gathered at the source: item (xs, sy, sz)
+// covers source cells (xs, Sy-2M+sy, sz) (-> bottom margin row sy) and
+// (xs, M+sy, sz) (-> top margin row Sy-M+sy).  Each margin cell is the image
+// of exactly one item, which clears it after reading.
+template <class R>
+NMHD_HD void a_fill_y_item(const GGrid<R> &g, double time, R *lam, int idx) {
+  const int M = g.my;
+  const int xs = idx % g.sx;
+  const int sy = (idx / g.sx) % M;
+  const int sz = idx / (g.sx * M);
+  int dint;
+  R f;
+  shear_shift(g, time, dint, f);
+  const R coef = (R(1.0f) - f) + f;  // d/dv of (1-f) v + f v
+  const int sx_lo = wrapc((xs - dint) % g.sx, g.sx);      // (sx_lo + dint) mod Sx = xs
+  const int sx_hi = wrapc((xs + dint + 1) % g.sx, g.sx);  // (sx_hi - dint - 1) mod Sx = xs
+  const size_t N = (size_t)g.n;
+  const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + xs;
+  const int src_dec = (sz * g.sy + (M + sy)) * g.sx + xs;
+  const int dst_lo = (sz * g.sy + sy) * g.sx + sx_lo;
+  const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx_hi;
+  for (int v = 0; v < 8; ++v) {
+    R *var = lam + v * N;
+    const R llo = var[dst_lo];
+    var[dst_lo] = R(0);
+    var[src_inc] += coef * llo;
+    if (!(v == 6 && sy == 0)) {
+      const R lhi = var[dst_hi];
+      var[dst_hi] = R(0);
+      var[src_dec] += coef * lhi;
+    }
+  }
+}
+
+// Gradient of s * sum over interior cells of -(Bx By at the cell centre)
+// with respect to the face fields of cell (x, y, z), added to lam.
+template <class R>
+NMHD_HD void a_stress_cell(const GGrid<R> &g, const R *w, R *lam, int x, int y, int z, double s) {
+  const size_t N = (size_t)g.n;
+  const int o = cell_at(g, x, y, z);
+  auto inner = [&](int yy, int zz) {
+    return yy >= g.my && yy < g.sy - g.my && zz >= g.mz && zz < g.sz - g.mz;
+  };
+  double gx = 0.0, gy = 0.0;
+  // cells using Bx[o]: (x, y, z) as its low face, (x-1, y, z) as its high face
+  for (int k = 0; k < 2; ++k) {
+    const int cx = x - k;
+    if (!inner(y, z)) break;
+    const double byl = (double)w[6 * N + cell_at(g, cx, y, z)], byh = (double)w[6 * N + cell_at(g, cx, y + 1, z)];
+    gx += -0.25 * (byl + byh);
+  }
+  for (int k = 0; k < 2; ++k) {
+    const int cy = wrapc(y - k, g.sy);
+    if (!inner(cy, z)) continue;
+    const double bxl = (double)w[5 * N + cell_at(g, x, cy, z)], bxh = (double)w[5 * N + cell_at(g, x + 1, cy, z)];
+    gy += -0.25 * (bxl + bxh);
+  }
+  lam[5 * N + o] += (R)(s * gx);
+  lam[6 * N + o] += (R)(s * gy);
+}
+
+}  // namespace ad
+}  // namespace nmhd

@@ -1,0 +1,562 @@
+// HLLD flux over a generic scalar type, and its hand-written adjoint.
+//
+// hlld_tape() evaluates src/library/hlld.inl:7-284 (the `#if 1` fast
+// magnetosonic bounds) keeping every intermediate; it is operation for
+// operation the production hlld_flux() of mhd_math.cuh, including the
+// reference's double-literal promotions (done in Traits<T>::wide), so with
+// T = float it reproduces the production flux and its fan region bit for bit,
+// and with T = double the reference's Real = double build.
+//
+// hlld_adjoint() is reverse-mode differentiation of that evaluation with the
+// fan region, the min/max choices and sign(Bx) frozen at the values taken:
+// given the adjoint of the 7 fluxes it returns the adjoint of the 14 left /
+// right states and of the normal field.  The derivation is written out step by
+// step below; every forward intermediate is read from the tape.
+#pragma once
+#include "ad_scalar.cuh"
+
+namespace nmhd {
+namespace ad {
+
+// Left/right Riemann states: rho, v_n, v_t1, v_t2, p, B_t1, B_t2.
+template <class T>
+struct HState {
+  T dl, dr, ul, ur, vl, vr, wl, wr, pl, pr, byl, byr, bzl, bzr;
+};
+
+// Per-side intermediates (names follow hlld.inl with the side suffix dropped).
+template <class T>
+struct HSide {
+  T d, u, v, w, p, by, bz;                           // state
+  T mx, my, mz, B2, v2, e, gp, gpb, disc, sq, num, cf, pT;
+  T sv, sm, ds, dn, vs, ws, q, bys, bzs, vB, vBs, es, sd, Ss;
+};
+
+template <class T>
+struct HTape {
+  HSide<T> L, R;
+  T Bx, B2x, absBx, sgn, cfmax, S_L, S_R, den, SMn, S_M, pTn, pT_s;
+  T fr, vss, wss, sdLR, Byss, Bzss, vBss, eLss, eRss;
+  int region;
+};
+
+template <class T>
+NMHD_HD void hlld_side_pre(const T gamma, const T gm1, const T Bx, const T B2x, HSide<T> &s) {
+  typedef typename Traits<T>::wide W;
+  s.mx = s.d * s.u;
+  s.my = s.d * s.v;
+  s.mz = s.d * s.w;
+  s.B2 = B2x + s.by * s.by + s.bz * s.bz;
+  s.v2 = s.u * s.u + s.v * s.v + s.w * s.w;
+  // etot = p/(gamma-1) + 0.5*rho*v2 + 0.5*B2, the last two terms in double
+  s.e = to<T>(to<W>(s.p / gm1) + W(0.5) * to<W>(s.d) * to<W>(s.v2) + W(0.5) * to<W>(s.B2));
+  s.gp = gamma * s.p;
+  s.gpb = s.gp + s.B2;
+  s.disc = s.gpb * s.gpb - T(4.0f) * s.gp * B2x;
+  s.sq = gsqrt(s.disc);
+  s.num = s.gpb + s.sq;
+  s.cf = gsqrt(s.num / (T(2.0f) * s.d));
+  s.pT = to<T>(to<W>(s.p) + W(0.5) * to<W>(s.B2));
+  (void)Bx;
+}
+
+// Star state of one side; S = S_L or S_R, sign = -1 (left) or +1 (right).
+template <class T>
+NMHD_HD void hlld_side_star(const T Bx, const T B2x, const T TINY, const T S, const T S_M, HSide<T> &s) {
+  s.sm = S - S_M;
+  s.ds = s.d * s.sv / s.sm;
+  s.dn = s.d * s.sv * s.sm - B2x + TINY;
+  s.vs = s.v - Bx * s.by * (S_M - s.u) / s.dn;
+  s.ws = s.w - Bx * s.bz * (S_M - s.u) / s.dn;
+  s.q = s.d * (s.sv * s.sv) - B2x;
+  s.bys = s.by * s.q / s.dn;
+  s.bzs = s.bz * s.q / s.dn;
+}
+
+template <class T>
+NMHD_HD void hlld_side_energy(const T Bx, const T S_M, const T pT_s, HSide<T> &s) {
+  s.vB = s.u * Bx + s.v * s.by + s.w * s.bz;
+  s.vBs = S_M * Bx + s.vs * s.bys + s.ws * s.bzs;
+  s.es = (s.sv * s.e - s.pT * s.u + pT_s * S_M + Bx * (s.vB - s.vBs)) / s.sm;
+  s.sd = gsqrt(s.ds);
+}
+
+template <class T>
+NMHD_HD void hlld_tape(const T gamma, const T Bx, const HState<T> &in, HTape<T> &t) {
+  typedef typename Traits<T>::wide W;
+  typedef typename Traits<T>::real R;
+  const T TINY = to<T>((R)1.0e-10);
+  t.Bx = Bx;
+  const R bxv = val(Bx);
+  t.sgn = to<T>(bxv > R(0) ? R(1) : (bxv < R(0) ? R(-1) : R(0)));
+  t.absBx = gabs(Bx);
+  t.L.d = in.dl; t.L.u = in.ul; t.L.v = in.vl; t.L.w = in.wl; t.L.p = in.pl; t.L.by = in.byl; t.L.bz = in.bzl;
+  t.R.d = in.dr; t.R.u = in.ur; t.R.v = in.vr; t.R.w = in.wr; t.R.p = in.pr; t.R.by = in.byr; t.R.bz = in.bzr;
+  t.B2x = Bx * Bx;
+  const T gm1 = gamma - T(1.0f);
+  hlld_side_pre(gamma, gm1, Bx, t.B2x, t.L);
+  hlld_side_pre(gamma, gm1, Bx, t.B2x, t.R);
+  const T fsig = to<T>(1.41421354f);  // (float)sqrt(2.0) in both reference builds
+  t.cfmax = fsig * gmax(t.L.cf, t.R.cf);
+  t.S_L = gmin(t.L.u, t.R.u) - t.cfmax;
+  t.S_R = gmax(t.L.u, t.R.u) + t.cfmax;
+  t.R.sv = t.S_R - t.R.u;
+  t.L.sv = t.S_L - t.L.u;
+  t.den = t.R.sv * t.R.d - t.L.sv * t.L.d;
+  const W rden = W(1.0) / to<W>(t.den);
+  t.SMn = t.R.sv * t.R.mx - t.L.sv * t.L.mx - t.R.pT + t.L.pT;
+  t.S_M = to<T>(to<W>(t.SMn) * rden);
+  t.pTn = t.R.sv * t.R.d * t.L.pT - t.L.sv * t.L.d * t.R.pT;
+  t.pTn = t.pTn + t.L.d * t.R.d * t.R.sv * t.L.sv * (t.R.u - t.L.u);
+  t.pT_s = to<T>(to<W>(t.pTn) * rden);
+  hlld_side_star(Bx, t.B2x, TINY, t.S_L, t.S_M, t.L);
+  hlld_side_star(Bx, t.B2x, TINY, t.S_R, t.S_M, t.R);
+  hlld_side_energy(Bx, t.S_M, t.pT_s, t.L);
+  hlld_side_energy(Bx, t.S_M, t.pT_s, t.R);
+  t.L.Ss = t.S_M - t.absBx / t.L.sd;
+  t.R.Ss = t.S_M + t.absBx / t.R.sd;
+  const R SL = val(t.S_L), SLs = val(t.L.Ss), SM = val(t.S_M), SRs = val(t.R.Ss), SR = val(t.S_R);
+  int region;
+  if (SL > R(0)) region = 0;
+  else if (SL <= R(0) && R(0) <= SLs) region = 1;
+  else if (SLs <= R(0) && R(0) <= SM) region = 2;
+  else if (SM <= R(0) && R(0) <= SRs) region = 3;
+  else if (SRs <= R(0) && R(0) <= SR) region = 4;
+  else region = 5;
+  t.region = region;
+  if (region == 2 || region == 3) {
+    const T sgn = t.sgn;
+    t.fr = T(1.0f) / (t.L.sd + t.R.sd);
+    t.vss = t.fr * (t.L.sd * t.L.vs + t.R.sd * t.R.vs + (t.R.bys - t.L.bys) * sgn);
+    t.wss = t.fr * (t.L.sd * t.L.ws + t.R.sd * t.R.ws + (t.R.bzs - t.L.bzs) * sgn);
+    t.sdLR = gsqrt(t.L.ds * t.R.ds);
+    t.Byss = t.fr * (t.L.sd * t.R.bys + t.R.sd * t.L.bys + t.sdLR * (t.R.vs - t.L.vs) * sgn);
+    t.Bzss = t.fr * (t.L.sd * t.R.bzs + t.R.sd * t.L.bzs + t.sdLR * (t.R.ws - t.L.ws) * sgn);
+    t.vBss = t.S_M * Bx + t.vss * t.Byss + t.wss * t.Bzss;
+    t.eLss = t.L.es - t.L.sd * (t.L.vBs - t.vBss) * sgn;
+    t.eRss = t.R.es + t.R.sd * (t.R.vBs - t.vBss) * sgn;
+  }
+}
+
+// The flux of the region on the tape (hlld.inl:229-284); kLeft selects the
+// side at compile time (regions 0-2 use the left state, 3-5 the right).
+template <bool kLeft, class T>
+NMHD_HD void hlld_flux_side(const HTape<T> &t, T f[7]) {
+  const HSide<T> &s = kLeft ? t.L : t.R;
+  const T Bx = t.Bx;
+  const T F0 = s.d * s.u;
+  const T F1 = s.mx * s.u + s.pT - t.B2x;
+  const T F2 = s.my * s.u - Bx * s.by;
+  const T F3 = s.mz * s.u - Bx * s.bz;
+  const T F4 = s.e * s.u + s.pT * s.u - Bx * s.vB;
+  const T F5 = s.by * s.u - Bx * s.v;
+  const T F6 = s.bz * s.u - Bx * s.w;
+  if (t.region == 0 || t.region == 5) {
+    f[0] = F0; f[1] = F1; f[2] = F2; f[3] = F3; f[4] = F4; f[5] = F5; f[6] = F6;
+    return;
+  }
+  const T S = kLeft ? t.S_L : t.S_R;
+  const T Us1 = s.ds * t.S_M, Us2 = s.ds * s.vs, Us3 = s.ds * s.ws;
+  if (t.region == 1 || t.region == 4) {
+    f[0] = F0 + S * s.ds - S * s.d;
+    f[1] = F1 + S * Us1 - S * s.mx;
+    f[2] = F2 + S * Us2 - S * s.my;
+    f[3] = F3 + S * Us3 - S * s.mz;
+    f[4] = F4 + S * s.es - S * s.e;
+    f[5] = F5 + S * s.bys - S * s.by;
+    f[6] = F6 + S * s.bzs - S * s.bz;
+    return;
+  }
+  const T Sss = s.Ss;
+  const T ess = kLeft ? t.eLss : t.eRss;
+  const T Sd = Sss - S;
+  f[0] = F0 + Sss * s.ds - Sd * s.ds - S * s.d;
+  f[1] = F1 + Sss * Us1 - Sd * Us1 - S * s.mx;
+  f[2] = F2 + Sss * (s.ds * t.vss) - Sd * Us2 - S * s.my;
+  f[3] = F3 + Sss * (s.ds * t.wss) - Sd * Us3 - S * s.mz;
+  f[4] = F4 + Sss * ess - Sd * s.es - S * s.e;
+  f[5] = F5 + Sss * t.Byss - Sd * s.bys - S * s.by;
+  f[6] = F6 + Sss * t.Bzss - Sd * s.bzs - S * s.bz;
+}
+
+template <class T>
+NMHD_HD void hlld_flux_of(const HTape<T> &t, T f[7]) {
+  if (t.region <= 2) hlld_flux_side<true>(t, f);
+  else hlld_flux_side<false>(t, f);
+}
+
+template <class T>
+NMHD_HD void hlld_g(const T gamma, const T Bx, const HState<T> &in, T f[7]) {
+  HTape<T> t;
+  hlld_tape(gamma, Bx, in, t);
+  hlld_flux_of(t, f);
+}
+
+// ---------------------------------------------------------------------------
+// Adjoint.  A<R> holds the adjoints of one side's intermediates.
+template <class R>
+struct HAdj {
+  R d, u, v, w, p, by, bz, mx, my, mz, B2, v2, e, pT, vB, sv, sm, ds, dn, vs, ws, q, bys, bzs, vBs, es, sd, cf;
+};
+
+template <class R>
+NMHD_HD void hadj_zero(HAdj<R> &a) {
+  a.d = a.u = a.v = a.w = a.p = a.by = a.bz = a.mx = a.my = a.mz = R(0);
+  a.B2 = a.v2 = a.e = a.pT = a.vB = a.sv = a.sm = a.ds = a.dn = a.vs = a.ws = R(0);
+  a.q = a.bys = a.bzs = a.vBs = a.es = a.sd = a.cf = R(0);
+}
+
+// Reverse of hlld_side_energy and hlld_side_star for one side.
+template <class R>
+NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, const R pT_s, HAdj<R> &a, R &aSM,
+                                R &apTs, R &aBx, R &aB2x, R &aS) {
+  // sd = sqrt(ds)
+  if (s.sd > R(0)) a.ds += a.sd / (s.sd + s.sd);
+  // es = (sv*e - pT*u + pT_s*S_M + Bx*(vB - vBs)) / sm
+  {
+    const R t = a.es / s.sm;
+    a.sv += t * s.e;
+    a.e += t * s.sv;
+    a.pT -= t * s.u;
+    a.u -= t * s.pT;
+    apTs += t * S_M;
+    aSM += t * pT_s;
+    aBx += t * (s.vB - s.vBs);
+    a.vB += t * Bx;
+    a.vBs -= t * Bx;
+    a.sm -= t * s.es;
+  }
+  // vBs = S_M*Bx + vs*bys + ws*bzs
+  aSM += a.vBs * Bx;
+  aBx += a.vBs * S_M;
+  a.vs += a.vBs * s.bys;
+  a.bys += a.vBs * s.vs;
+  a.ws += a.vBs * s.bzs;
+  a.bzs += a.vBs * s.ws;
+  // bys = by*q/dn, bzs = bz*q/dn
+  a.by += a.bys * s.q / s.dn;
+  a.q += a.bys * s.by / s.dn;
+  a.dn -= a.bys * s.bys / s.dn;
+  a.bz += a.bzs * s.q / s.dn;
+  a.q += a.bzs * s.bz / s.dn;
+  a.dn -= a.bzs * s.bzs / s.dn;
+  // q = d*sv^2 - B2x
+  a.d += a.q * s.sv * s.sv;
+  a.sv += a.q * R(2) * s.d * s.sv;
+  aB2x -= a.q;
+  // vs = v - Bx*by*(S_M - u)/dn, ws = w - Bx*bz*(S_M - u)/dn
+  {
+    const R g = (S_M - s.u) / s.dn;
+    const R tv = -a.vs, tw = -a.ws;
+    a.v += a.vs;
+    a.w += a.ws;
+    aBx += tv * s.by * g + tw * s.bz * g;
+    a.by += tv * Bx * g;
+    a.bz += tw * Bx * g;
+    const R c = (tv * Bx * s.by + tw * Bx * s.bz) / s.dn;
+    aSM += c;
+    a.u -= c;
+    a.dn -= c * g;
+  }
+  // dn = d*sv*sm - B2x + TINY
+  a.d += a.dn * s.sv * s.sm;
+  a.sv += a.dn * s.d * s.sm;
+  a.sm += a.dn * s.d * s.sv;
+  aB2x -= a.dn;
+  // ds = d*sv/sm
+  a.d += a.ds * s.sv / s.sm;
+  a.sv += a.ds * s.d / s.sm;
+  a.sm -= a.ds * s.ds / s.sm;
+  // sm = S - S_M
+  aS += a.sm;
+  aSM -= a.sm;
+}
+
+// Reverse of vB = u*Bx + v*by + w*bz (used by the flux of every region).
+template <class R>
+NMHD_HD void hlld_side_vB_rev(const HSide<R> &s, const R Bx, HAdj<R> &a, R &aBx) {
+  a.u += a.vB * Bx;
+  aBx += a.vB * s.u;
+  a.v += a.vB * s.by;
+  a.by += a.vB * s.v;
+  a.w += a.vB * s.bz;
+  a.bz += a.vB * s.w;
+}
+
+// Reverse of hlld_side_pre (after pT, cf, e, mx.. have their adjoints).
+template <class R>
+NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R gm1, const R B2x, HAdj<R> &a,
+                               R &aB2x) {
+  // pT = p + 0.5*B2
+  a.p += a.pT;
+  a.B2 += R(0.5) * a.pT;
+  // cf = sqrt(num/(2d))
+  if (s.cf > R(0)) {
+    const R aQ = a.cf / (s.cf + s.cf);
+    const R twod = R(2) * s.d;
+    const R Q = s.num / twod;
+    const R anum = aQ / twod;
+    a.d -= aQ * Q / s.d;
+    // num = gpb + sq; sq = sqrt(disc); disc = gpb^2 - 4 gp B2x; gpb = gp + B2
+    R agpb = anum, agp = R(0);
+    if (s.sq > R(0)) {
+      const R adisc = anum / (s.sq + s.sq);
+      agpb += adisc * R(2) * s.gpb;
+      agp -= adisc * R(4) * B2x;
+      aB2x -= adisc * R(4) * s.gp;
+    }
+    agp += agpb;
+    a.B2 += agpb;
+    a.p += gamma * agp;
+  }
+  // e = p/gm1 + 0.5*d*v2 + 0.5*B2
+  a.p += a.e / gm1;
+  a.d += R(0.5) * a.e * s.v2;
+  a.v2 += R(0.5) * a.e * s.d;
+  a.B2 += R(0.5) * a.e;
+  // v2, B2, momenta
+  a.u += R(2) * s.u * a.v2;
+  a.v += R(2) * s.v * a.v2;
+  a.w += R(2) * s.w * a.v2;
+  aB2x += a.B2;
+  a.by += R(2) * s.by * a.B2;
+  a.bz += R(2) * s.bz * a.B2;
+  a.d += a.mx * s.u + a.my * s.v + a.mz * s.w;
+  a.u += a.mx * s.d;
+  a.v += a.my * s.d;
+  a.w += a.mz * s.d;
+}
+
+// Reverse of the region flux (hlld_flux_side) and of the double-star states.
+template <bool kLeft, class R>
+NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj<R> &aR, R &aBx, R &aB2x,
+                             R &aSM, R &aSL, R &aSR, R &aabs) {
+  const int rg = t.region;
+  const HSide<R> &s = kLeft ? t.L : t.R;
+  HAdj<R> &aX = kLeft ? aL : aR;
+  const R Bx = t.Bx, sgn = t.sgn;
+  R aSss = R(0), aess = R(0), avss = R(0), awss = R(0), aByss = R(0), aBzss = R(0);
+  // F = F(U) of side X
+  aX.d += lf[0] * s.u;
+  aX.u += lf[0] * s.d + lf[1] * s.mx + lf[2] * s.my + lf[3] * s.mz + lf[4] * (s.e + s.pT) + lf[5] * s.by +
+          lf[6] * s.bz;
+  aX.mx += lf[1] * s.u;
+  aX.pT += lf[1] + lf[4] * s.u;
+  aB2x -= lf[1];
+  aX.my += lf[2] * s.u;
+  aX.mz += lf[3] * s.u;
+  aBx -= lf[2] * s.by + lf[3] * s.bz + lf[4] * s.vB + lf[5] * s.v + lf[6] * s.w;
+  aX.by += lf[5] * s.u - lf[2] * Bx;
+  aX.bz += lf[6] * s.u - lf[3] * Bx;
+  aX.e += lf[4] * s.u;
+  aX.vB -= lf[4] * Bx;
+  aX.v -= lf[5] * Bx;
+  aX.w -= lf[6] * Bx;
+  if (rg == 0 || rg == 5) return;
+  const R S = kLeft ? t.S_L : t.S_R;
+  const R Us1 = s.ds * t.S_M, Us2 = s.ds * s.vs, Us3 = s.ds * s.ws;
+  // -S*U
+  aX.d -= S * lf[0];
+  aX.mx -= S * lf[1];
+  aX.my -= S * lf[2];
+  aX.mz -= S * lf[3];
+  aX.e -= S * lf[4];
+  aX.by -= S * lf[5];
+  aX.bz -= S * lf[6];
+  // d/dS of S*(U* - U) (regions 1, 4) and of -(Sss - S)*U* - S*U (regions 2, 3)
+  const R aS = lf[0] * (s.ds - s.d) + lf[1] * (Us1 - s.mx) + lf[2] * (Us2 - s.my) + lf[3] * (Us3 - s.mz) +
+               lf[4] * (s.es - s.e) + lf[5] * (s.bys - s.by) + lf[6] * (s.bzs - s.bz);
+  if (kLeft) aSL += aS; else aSR += aS;
+  R cs = S;  // coefficient of U*
+  const bool dstar = rg == 2 || rg == 3;
+  if (dstar) {
+    const R Sss = s.Ss;
+    const R ess = kLeft ? t.eLss : t.eRss;
+    cs = -(Sss - S);
+    aSss = lf[2] * (s.ds * t.vss - Us2) + lf[3] * (s.ds * t.wss - Us3) + lf[4] * (ess - s.es) +
+           lf[5] * (t.Byss - s.bys) + lf[6] * (t.Bzss - s.bzs);
+    // Sss * U**
+    aX.ds += Sss * (lf[0] + lf[1] * t.S_M + lf[2] * t.vss + lf[3] * t.wss);
+    aSM += Sss * lf[1] * s.ds;
+    avss = Sss * lf[2] * s.ds;
+    awss = Sss * lf[3] * s.ds;
+    aess = Sss * lf[4];
+    aByss = Sss * lf[5];
+    aBzss = Sss * lf[6];
+  }
+  aX.ds += cs * (lf[0] + lf[1] * t.S_M + lf[2] * s.vs + lf[3] * s.ws);
+  aSM += cs * lf[1] * s.ds;
+  aX.vs += cs * lf[2] * s.ds;
+  aX.ws += cs * lf[3] * s.ds;
+  aX.es += cs * lf[4];
+  aX.bys += cs * lf[5];
+  aX.bzs += cs * lf[6];
+  if (!dstar) return;
+
+  R avBss = R(0), afr = R(0), asdLR = R(0);
+  // ess = eLs - sdL*(vBLs - vBss)*sgn (left), eRs + sdR*(vBRs - vBss)*sgn (right)
+  aX.es += aess;
+  if (kLeft) {
+    aX.sd -= aess * (s.vBs - t.vBss) * sgn;
+    aX.vBs -= aess * s.sd * sgn;
+    avBss += aess * s.sd * sgn;
+  } else {
+    aX.sd += aess * (s.vBs - t.vBss) * sgn;
+    aX.vBs += aess * s.sd * sgn;
+    avBss -= aess * s.sd * sgn;
+  }
+  // vBss = S_M*Bx + vss*Byss + wss*Bzss
+  aSM += avBss * Bx;
+  aBx += avBss * t.S_M;
+  avss += avBss * t.Byss;
+  aByss += avBss * t.vss;
+  awss += avBss * t.Bzss;
+  aBzss += avBss * t.wss;
+  // Bzss = fr*(sdL*bzRs + sdR*bzLs + sdLR*(wRs - wLs)*sgn)
+  {
+    const R n = t.L.sd * t.R.bzs + t.R.sd * t.L.bzs + t.sdLR * (t.R.ws - t.L.ws) * sgn;
+    afr += aBzss * n;
+    const R c = aBzss * t.fr;
+    aL.sd += c * t.R.bzs;
+    aR.bzs += c * t.L.sd;
+    aR.sd += c * t.L.bzs;
+    aL.bzs += c * t.R.sd;
+    asdLR += c * (t.R.ws - t.L.ws) * sgn;
+    aR.ws += c * t.sdLR * sgn;
+    aL.ws -= c * t.sdLR * sgn;
+  }
+  // Byss = fr*(sdL*byRs + sdR*byLs + sdLR*(vRs - vLs)*sgn)
+  {
+    const R n = t.L.sd * t.R.bys + t.R.sd * t.L.bys + t.sdLR * (t.R.vs - t.L.vs) * sgn;
+    afr += aByss * n;
+    const R c = aByss * t.fr;
+    aL.sd += c * t.R.bys;
+    aR.bys += c * t.L.sd;
+    aR.sd += c * t.L.bys;
+    aL.bys += c * t.R.sd;
+    asdLR += c * (t.R.vs - t.L.vs) * sgn;
+    aR.vs += c * t.sdLR * sgn;
+    aL.vs -= c * t.sdLR * sgn;
+  }
+  // wss = fr*(sdL*wLs + sdR*wRs + (bzRs - bzLs)*sgn)
+  {
+    const R n = t.L.sd * t.L.ws + t.R.sd * t.R.ws + (t.R.bzs - t.L.bzs) * sgn;
+    afr += awss * n;
+    const R c = awss * t.fr;
+    aL.sd += c * t.L.ws;
+    aL.ws += c * t.L.sd;
+    aR.sd += c * t.R.ws;
+    aR.ws += c * t.R.sd;
+    aR.bzs += c * sgn;
+    aL.bzs -= c * sgn;
+  }
+  // vss = fr*(sdL*vLs + sdR*vRs + (byRs - byLs)*sgn)
+  {
+    const R n = t.L.sd * t.L.vs + t.R.sd * t.R.vs + (t.R.bys - t.L.bys) * sgn;
+    afr += avss * n;
+    const R c = avss * t.fr;
+    aL.sd += c * t.L.vs;
+    aL.vs += c * t.L.sd;
+    aR.sd += c * t.R.vs;
+    aR.vs += c * t.R.sd;
+    aR.bys += c * sgn;
+    aL.bys -= c * sgn;
+  }
+  // sdLR = sqrt(dLs*dRs)
+  if (t.sdLR > R(0)) {
+    const R c = asdLR / (t.sdLR + t.sdLR);
+    aL.ds += c * t.R.ds;
+    aR.ds += c * t.L.ds;
+  }
+  // fr = 1/(sdL + sdR)
+  {
+    const R c = -afr * t.fr * t.fr;
+    aL.sd += c;
+    aR.sd += c;
+  }
+  // Sss = S_L* = S_M - |Bx|/sdL (left) or S_R* = S_M + |Bx|/sdR (right)
+  aSM += aSss;
+  if (kLeft) {
+    aabs -= aSss / s.sd;
+    aX.sd += aSss * t.absBx / (s.sd * s.sd);
+  } else {
+    aabs += aSss / s.sd;
+    aX.sd -= aSss * t.absBx / (s.sd * s.sd);
+  }
+}
+
+// Adjoint of hlld_g: ls and lBx receive d<lf, f>/d(state) and d<lf, f>/dBx.
+template <class R>
+NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const R lf[7], HState<R> &ls,
+                          R &lBx) {
+  HTape<R> t;
+  hlld_tape(gamma, Bx, in, t);
+  const int rg = t.region;
+  const bool left = rg <= 2;
+  HAdj<R> aL, aR;
+  hadj_zero(aL);
+  hadj_zero(aR);
+  R aBx = R(0), aB2x = R(0), aSM = R(0), apTs = R(0), aSL = R(0), aSR = R(0), aabs = R(0);
+  const R sgn = t.sgn;
+  if (left) hlld_region_rev<true>(t, lf, aL, aR, aBx, aB2x, aSM, aSL, aSR, aabs);
+  else hlld_region_rev<false>(t, lf, aL, aR, aBx, aB2x, aSM, aSL, aSR, aabs);
+  if (rg != 0 && rg != 5) {  // regions 0 and 5 use no wave speed or star state
+    // --- star states of both sides ---------------------------------------------
+    hlld_side_star_rev(t.L, Bx, t.S_M, t.pT_s, aL, aSM, apTs, aBx, aB2x, aSL);
+    hlld_side_star_rev(t.R, Bx, t.S_M, t.pT_s, aR, aSM, apTs, aBx, aB2x, aSR);
+
+    // --- S_M = SMn/den, pT* = pTn/den ---------------------------------------------
+    {
+      const R aSMn = aSM / t.den, apTn = apTs / t.den;
+      const R aden = -(aSM * t.S_M + apTs * t.pT_s) / t.den;
+      const R dl = t.L.d, dr = t.R.d, sLv = t.L.sv, sRv = t.R.sv, du = t.R.u - t.L.u;
+      // pTn = sRv*dr*pTL - sLv*dl*pTR + dl*dr*sRv*sLv*(ur - ul)
+      aR.sv += apTn * (dr * t.L.pT + dl * dr * sLv * du);
+      aR.d += apTn * (sRv * t.L.pT + dl * sRv * sLv * du);
+      aL.pT += apTn * sRv * dr;
+      aL.sv += apTn * (-dl * t.R.pT + dl * dr * sRv * du);
+      aL.d += apTn * (-sLv * t.R.pT + dr * sRv * sLv * du);
+      aR.pT -= apTn * sLv * dl;
+      aR.u += apTn * dl * dr * sRv * sLv;
+      aL.u -= apTn * dl * dr * sRv * sLv;
+      // SMn = sRv*mxR - sLv*mxL - pTR + pTL
+      aR.sv += aSMn * t.R.mx;
+      aR.mx += aSMn * sRv;
+      aL.sv -= aSMn * t.L.mx;
+      aL.mx -= aSMn * sLv;
+      aR.pT -= aSMn;
+      aL.pT += aSMn;
+      // den = sRv*dr - sLv*dl
+      aR.sv += aden * dr;
+      aR.d += aden * sRv;
+      aL.sv -= aden * dl;
+      aL.d -= aden * sLv;
+    }
+    // sv = S - u
+    aSR += aR.sv;
+    aR.u -= aR.sv;
+    aSL += aL.sv;
+    aL.u -= aL.sv;
+    // S_L = min(uL, uR) - cfmax, S_R = max(uL, uR) + cfmax, cfmax = fsig*max(cfL, cfR)
+    {
+      if (t.R.u < t.L.u) aR.u += aSL; else aL.u += aSL;
+      if (t.R.u > t.L.u) aR.u += aSR; else aL.u += aSR;
+      const R acf = R(1.41421354f) * (aSR - aSL);
+      if (t.R.cf > t.L.cf) aR.cf += acf; else aL.cf += acf;
+    }
+  }
+  hlld_side_vB_rev(t.L, Bx, aL, aBx);
+  hlld_side_vB_rev(t.R, Bx, aR, aBx);
+  const R gm1 = gamma - R(1);
+  hlld_side_pre_rev(t.L, gamma, gm1, t.B2x, aL, aB2x);
+  hlld_side_pre_rev(t.R, gamma, gm1, t.B2x, aR, aB2x);
+  aBx += R(2) * Bx * aB2x + aabs * sgn;
+
+  ls.dl = aL.d; ls.dr = aR.d; ls.ul = aL.u; ls.ur = aR.u; ls.vl = aL.v; ls.vr = aR.v;
+  ls.wl = aL.w; ls.wr = aR.w; ls.pl = aL.p; ls.pr = aR.p; ls.byl = aL.by; ls.byr = aR.by;
+  ls.bzl = aL.bz; ls.bzr = aR.bz;
+  lBx = aBx;
+}
+
+}  // namespace ad
+}  // namespace nmhd

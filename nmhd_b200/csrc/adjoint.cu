@@ -1,0 +1,527 @@
+// Differentiation of the B200 time step (sm_100a): FP32 and FP64 adjoint runs
+// with checkpointed recomputation, and the FP64 tangent-linear run.
+//
+// FP32 runs step with the production kernels (cell_stage.cu) on explicit
+// buffers, so the forward trajectory, its CFL time steps and its loss are
+// bitwise those of nmhd_proceed; the dt is then frozen through StepCtl::dt_seq
+// for the recomputation.  FP64 and tangent-linear runs step with the generic
+// kernels of ad_driver.cuh over double and Dual<double>.  The adjoint kernels
+// are the transposes in ad_cell.cuh / ad_hlld.cuh, one launch per pass.
+//
+// Memory: checkpoints (8 fields) every K steps, plus one segment's tape (66
+// fields per step: filled input, predictor, raw output, both stages' fluxes),
+// plus 3 adjoint states and 57 scratch fields.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/nmhd.h"
+#include "ad_driver.cuh"
+#include "solver_impl.h"
+#include "step.cuh"
+
+using nmhd::GridParams;
+using nmhd::StepCtl;
+using namespace nmhd::ad;
+
+namespace {
+
+constexpr int BX = 32, BY = 4, BZ = 2;
+
+template <class F>
+__global__ void __launch_bounds__(BX *BY *BZ) k_ad_cells(F f, int sx, int sy, int sz) {
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int y = blockIdx.y * BY + threadIdx.y;
+  const int z = blockIdx.z * BZ + threadIdx.z;
+  if (x < sx && y < sy && z < sz) f(x, y, z);
+}
+
+template <class F>
+__global__ void __launch_bounds__(256) k_ad_items(F f, int n) {
+  const int i = blockIdx.x * 256 + threadIdx.x;
+  if (i < n) f(i);
+}
+
+// Deterministic reduction of a per-cell value: a fixed tree per block into
+// partial[], then one block folds partial[] in a fixed order into *acc.
+template <class D, class F>
+__global__ void __launch_bounds__(256) k_ad_reduce(F f, int sx, int sy, int sz, D *partial) {
+  __shared__ double raw[256 * sizeof(D) / sizeof(double)];
+  D *sh = reinterpret_cast<D *>(raw);
+  const int tid = threadIdx.x;
+  const long long i = (long long)blockIdx.x * 256 + tid;
+  const long long n = (long long)sx * sy * sz;
+  D v = to<D>(0.0);
+  if (i < n) {
+    const int x = (int)(i % sx), y = (int)((i / sx) % sy), z = (int)(i / ((long long)sx * sy));
+    v = f(x, y, z);
+  }
+  sh[tid] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s) sh[tid] = sh[tid] + sh[tid + s];
+    __syncthreads();
+  }
+  if (tid == 0) partial[blockIdx.x] = sh[0];
+}
+
+template <class D>
+__global__ void __launch_bounds__(256) k_ad_reduce_final(const D *partial, int nb, D *acc, double scale) {
+  __shared__ double raw[256 * sizeof(D) / sizeof(double)];
+  D *sh = reinterpret_cast<D *>(raw);
+  const int tid = threadIdx.x;
+  D v = to<D>(0.0);
+  for (int i = tid; i < nb; i += 256) v = v + partial[i];
+  sh[tid] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if (tid < s) sh[tid] = sh[tid] + sh[tid + s];
+    __syncthreads();
+  }
+  if (tid == 0) acc[0] = acc[0] + sh[0] * to<D>(scale);
+}
+
+template <class T>
+struct OpWiden {  // float state -> T (with an optional tangent)
+  const float *src;
+  const double *dir;
+  T *dst;
+  NMHD_HD void operator()(int i) const;
+};
+template <>
+NMHD_HD void OpWiden<double>::operator()(int i) const { dst[i] = (double)src[i]; }
+template <>
+NMHD_HD void OpWiden<Dual<double>>::operator()(int i) const {
+  dst[i] = Dual<double>((double)src[i], dir ? dir[i] : 0.0);
+}
+
+struct GpuExec {
+  cudaStream_t st;
+  template <class R, class F>
+  void cells(const GGrid<R> &g, const F &f) {
+    const dim3 grid((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (g.sz + BZ - 1) / BZ);
+    k_ad_cells<<<grid, dim3(BX, BY, BZ), 0, st>>>(f, g.sx, g.sy, g.sz);
+  }
+  template <class F>
+  void items(int n, const F &f) {
+    if (n > 0) k_ad_items<<<(n + 255) / 256, 256, 0, st>>>(f, n);
+  }
+  template <class T>
+  void zero(T *p, size_t n) {
+    cudaMemsetAsync(p, 0, n * sizeof(T), st);
+  }
+  template <class D, class R, class F>
+  void reduce(const GGrid<R> &g, const F &f, D *partial, D *acc, double scale) {
+    const long long n = (long long)g.sx * g.sy * g.sz;
+    const int nb = (int)((n + 255) / 256);
+    k_ad_reduce<D, F><<<nb, 256, 0, st>>>(f, g.sx, g.sy, g.sz, partial);
+    k_ad_reduce_final<D><<<1, 256, 0, st>>>(partial, nb, acc, scale);
+  }
+};
+
+// ---------------------------------------------------------------------------
+struct Workspace {
+  void *mem = nullptr;
+  size_t bytes = 0;
+  StepCtl *ctl = nullptr;
+  float *dt_dev = nullptr, *hist_dummy = nullptr;
+  double ms[4] = {0, 0, 0, 0};
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+};
+
+Workspace &workspace(nmhd_solver *s) {
+  if (!s->adjoint) s->adjoint = new Workspace();
+  return *static_cast<Workspace *>(s->adjoint);
+}
+
+nmhd_status set_err(nmhd_solver *s, nmhd_status st, const std::string &m) {
+  s->err = m;
+  return st;
+}
+
+#define AD_CUDA(call)                                                                                \
+  do {                                                                                               \
+    cudaError_t e_ = (call);                                                                         \
+    if (e_ != cudaSuccess)                                                                           \
+      return set_err(s, e_ == cudaErrorMemoryAllocation ? NMHD_ERR_OUT_OF_MEMORY : NMHD_ERR_CUDA,    \
+                     std::string(#call) + ": " + cudaGetErrorString(e_));                            \
+  } while (0)
+
+// One arena per run: the run's buffers are carved from it in order.
+struct Arena {
+  char *base;
+  size_t off;
+  template <class T>
+  T *take(size_t count) {
+    off = (off + 255) & ~(size_t)255;
+    T *p = reinterpret_cast<T *>(base + off);
+    off += count * sizeof(T);
+    return p;
+  }
+};
+
+nmhd_status reserve(nmhd_solver *s, Workspace &w, size_t bytes) {
+  if (!w.ctl) {
+    AD_CUDA(cudaMalloc(&w.ctl, sizeof(StepCtl)));
+    AD_CUDA(cudaMalloc(&w.dt_dev, sizeof(float) * nmhd::kDtHistCap));
+    AD_CUDA(cudaMalloc(&w.hist_dummy, sizeof(float) * nmhd::kDtHistCap));
+    for (auto &e : w.ev) AD_CUDA(cudaEventCreate(&e));
+  }
+  if (w.bytes >= bytes) return NMHD_OK;
+  if (w.mem) {
+    AD_CUDA(cudaStreamSynchronize(s->stream));
+    cudaFree(w.mem);
+    w.mem = nullptr;
+    w.bytes = 0;
+  }
+  AD_CUDA(cudaMalloc(&w.mem, bytes));
+  w.bytes = bytes;
+  return NMHD_OK;
+}
+
+nmhd_status validate(nmhd_solver *s, int nsteps, int ckpt, const nmhd_loss_spec *l) {
+  if (!s) return NMHD_ERR_INVALID_ARGUMENT;
+  if (!l) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "loss spec is NULL");
+  if (nsteps < 1 || nsteps > NMHD_ADJOINT_MAX_STEPS)
+    return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "nsteps must be in [1, NMHD_ADJOINT_MAX_STEPS]");
+  if (ckpt < 1) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "ckpt_every must be >= 1");
+  if (l->kind != NMHD_LOSS_MAXWELL_STRESS) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "unknown loss kind");
+  if (l->first_step < 0 || l->first_step > l->last_step || l->last_step > nsteps)
+    return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "loss window must satisfy 0 <= first <= last <= nsteps");
+  if (s->cfg.size_y - 2 * s->cfg.margin_y < 1 || s->cfg.size_z - 2 * s->cfg.margin_z < 1)
+    return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "no interior cells");
+  return NMHD_OK;
+}
+
+// The solver's current state (device) and clock.
+nmhd_status solver_state(nmhd_solver *s, const float **cur, double *time) {
+  StepCtl h;
+  AD_CUDA(cudaMemcpyAsync(&h, s->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
+  AD_CUDA(cudaStreamSynchronize(s->stream));
+  if (h.status) return set_err(s, NMHD_ERR_NUMERICAL, "state is not valid (set a new state)");
+  *cur = h.parity ? s->w1 : s->w0;
+  *time = h.time;
+  return NMHD_OK;
+}
+
+nmhd_status write_ctl(nmhd_solver *s, Workspace &w, double time, long long gen, bool frozen) {
+  StepCtl h;
+  std::memset(&h, 0, sizeof(h));
+  h.time = time;
+  h.generation = gen;
+  h.cfl_cur = h.cfl_next = 0x7f800000u;
+  h.goal = INFINITY;
+  h.hist_cap = nmhd::kDtHistCap;
+  h.dt_seq = frozen ? w.dt_dev : nullptr;
+  h.dt_seq_base = 0;
+  AD_CUDA(cudaMemcpyAsync(w.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
+  AD_CUDA(cudaStreamSynchronize(s->stream));
+  return NMHD_OK;
+}
+
+// One FP32 step with the production kernels on explicit buffers: t.wf holds
+// W^n (its margins are filled in place), the raw W^{n+1} goes to t.wo.
+void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl) {
+  const GridParams &g = s->g;
+  cudaStream_t st = s->stream;
+  float *hist = cfl ? w.dt_dev : w.hist_dummy;
+  cudaMemsetAsync(&w.ctl->parity, 0, sizeof(int), st);  // buffer 0 = t.wf, 1 = t.wo, 2 = t.ws
+  if (g.my > 0 || g.mz > 0) {
+    nmhd::launch_fill(g, w.ctl, t.wf, t.wo, st);
+    if (cfl) nmhd::launch_cfl_margin(g, w.ctl, t.wf, t.wo, st);
+  }
+  if (s->cfg.time_order == 1) {
+    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f1, 0, 0, st);
+    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f1, hist, 0, 1, 0, 1, st);
+  } else {
+    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f1, 0, 1, st);
+    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f1, hist, 0, 2, 1, 0, st);
+    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f2, 2, 0, st);
+    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f2, hist, 2, 1, 0, 1, st);
+  }
+}
+
+float elapsed(cudaEvent_t a, cudaEvent_t b) {
+  float ms = 0.0f;
+  cudaEventElapsedTime(&ms, a, b);
+  return ms;
+}
+
+// ---------------------------------------------------------------------------
+// FP32 (production forward) and FP64 (generic forward) adjoint runs share this
+// driver; Prec selects the forward and the real type.
+template <class R>
+struct Prec;
+
+template <>
+struct Prec<float> {
+  static constexpr bool kProduction = true;
+};
+template <>
+struct Prec<double> {
+  static constexpr bool kProduction = false;
+};
+
+template <class R>
+nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, const float *dt_seq, double *loss_out,
+                float *dt_out, R *const grad[8], int grad_on_device, bool want_grad) {
+  Workspace &w = workspace(s);
+  const size_t n = (size_t)s->g.n;
+  const GGrid<R> gg = make_ggrid<R>(s->cfg);
+  const int nseg = (nsteps + K - 1) / K;
+  const int tape_steps = want_grad ? std::min(K, nsteps) : 1;
+  const bool frozen = dt_seq != nullptr;
+  if (!Prec<R>::kProduction && !frozen)
+    return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "dt_seq is required for FP64 runs");
+  // arena
+  const size_t nb = (n + 255) / 256;
+  size_t need = 0;
+  need += sizeof(R) * (want_grad ? (size_t)nseg * 8 * n : 0) + 256;  // checkpoints
+  need += sizeof(R) * (size_t)tape_steps * kTapeFields * n + 256;     // tape
+  need += sizeof(R) * (want_grad ? (24 + kAdjScratchFields) * n : 8 * n) + 512;
+  need += sizeof(double) * (nb + 8) + 512;
+  nmhd_status st = reserve(s, w, need);
+  if (st != NMHD_OK) return st;
+  Arena ar{static_cast<char *>(w.mem), 0};
+  R *ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
+  R *tape = ar.take<R>((size_t)tape_steps * kTapeFields * n);
+  R *spare = ar.take<R>(8 * n);  // ping-pong partner of the primal pass
+  R *lam = want_grad ? ar.take<R>(24 * n) : nullptr;
+  R *scr = want_grad ? ar.take<R>((size_t)kAdjScratchFields * n) : nullptr;
+  double *partial = ar.take<double>(nb);
+  double *acc = ar.take<double>(1);
+
+  const float *cur;
+  double t0;
+  st = solver_state(s, &cur, &t0);
+  if (st != NMHD_OK) return st;
+  cudaStream_t q = s->stream;
+  GpuExec ex{q};
+  const double scale = stress_scale(s->cfg, L);
+  if (frozen) AD_CUDA(cudaMemcpyAsync(w.dt_dev, dt_seq, sizeof(float) * nsteps, cudaMemcpyHostToDevice, q));
+  st = write_ctl(s, w, t0, 0, frozen);
+  if (st != NMHD_OK) return st;
+  AD_CUDA(cudaMemsetAsync(acc, 0, sizeof(double), q));
+
+  // ---- forward run with checkpoints -------------------------------------------
+  AD_CUDA(cudaEventRecord(w.ev[0], q));
+  StepTape<R> t0tape = tape_at(tape, n);
+  R *A = t0tape.wf, *B = spare;
+  if constexpr (Prec<R>::kProduction) {
+    AD_CUDA(cudaMemcpyAsync(A, cur, sizeof(float) * 8 * n, cudaMemcpyDeviceToDevice, q));
+  } else {
+    ex.items((int)(8 * n), OpWiden<R>{cur, nullptr, A});
+  }
+  if (in_window(L, 0)) ex.reduce(gg, OpStress<R, R>{gg, A}, partial, acc, scale);
+  std::vector<float> dts(nsteps);
+  if (frozen) std::copy(dt_seq, dt_seq + nsteps, dts.begin());
+  if constexpr (Prec<R>::kProduction) {
+    if (!frozen) {
+      // CFL time of the fresh state after its margins are filled (as nmhd_proceed)
+      AD_CUDA(cudaMemsetAsync(&w.ctl->parity, 0, sizeof(int), q));
+      nmhd::launch_fill(s->g, w.ctl, A, B, q);
+      nmhd::launch_cfl_all(s->g, w.ctl, A, B, q);
+    }
+  }
+  std::vector<double> tn(nsteps + 1);
+  tn[0] = t0;
+  for (int i = 0; i < nsteps; ++i) {
+    if (want_grad && i % K == 0)
+      AD_CUDA(cudaMemcpyAsync(ckpt + (size_t)(i / K) * 8 * n, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+    StepTape<R> t = {A, t0tape.f1, t0tape.ws, t0tape.f2, B};
+    if constexpr (Prec<R>::kProduction) {
+      prod_step(s, w, t, !frozen);
+    } else {
+      tn[i + 1] = tn[i] + (double)dts[i];
+      fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
+    }
+    if (in_window(L, i + 1)) ex.reduce(gg, OpStress<R, R>{gg, B}, partial, acc, scale);
+    std::swap(A, B);
+  }
+  AD_CUDA(cudaGetLastError());
+  AD_CUDA(cudaEventRecord(w.ev[1], q));
+  if constexpr (Prec<R>::kProduction) {
+    StepCtl h;
+    AD_CUDA(cudaMemcpyAsync(&h, w.ctl, sizeof(h), cudaMemcpyDeviceToHost, q));
+    AD_CUDA(cudaStreamSynchronize(q));
+    if (h.status)
+      return set_err(s, NMHD_ERR_NUMERICAL, "non-finite state, density <= 0 or pressure <= 0 in the forward run");
+    if (!frozen) AD_CUDA(cudaMemcpy(dts.data(), w.dt_dev, sizeof(float) * nsteps, cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nsteps; ++i) tn[i + 1] = tn[i] + (double)dts[i];
+  }
+  AD_CUDA(cudaMemcpyAsync(loss_out, acc, sizeof(double), cudaMemcpyDeviceToHost, q));
+  AD_CUDA(cudaStreamSynchronize(q));
+  if (dt_out) std::copy(dts.begin(), dts.end(), dt_out);
+  w.ms[0] = elapsed(w.ev[0], w.ev[1]);
+  w.ms[1] = w.ms[2] = 0.0;
+  w.ms[3] = w.ms[0];
+  if (!want_grad) return NMHD_OK;
+  if (Prec<R>::kProduction && !frozen) {
+    // the recomputation replays these steps with dt frozen
+    AD_CUDA(cudaMemcpyAsync(w.dt_dev, dts.data(), sizeof(float) * nsteps, cudaMemcpyHostToDevice, q));
+  }
+
+  // ---- reverse sweep ---------------------------------------------------------------
+  R *lamA = lam, *lamS = lam + 8 * n, *lamF = lam + 16 * n;
+  const AdjScratch<R> sc = scratch_at(scr, n);
+  ex.zero(lamA, 8 * n);
+  double ms_re = 0.0, ms_adj = 0.0;
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
+    if (Prec<R>::kProduction) {
+      st = write_ctl(s, w, tn[n0], n0, true);
+      if (st != NMHD_OK) return st;
+    }
+    AD_CUDA(cudaEventRecord(w.ev[2], q));
+    AD_CUDA(cudaMemcpyAsync(tape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+    for (int i = n0; i < n1; ++i) {
+      const StepTape<R> t = tape_at(tape + (size_t)(i - n0) * kTapeFields * n, n);
+      if constexpr (Prec<R>::kProduction)
+        prod_step(s, w, t, false);
+      else
+        fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
+      if (i + 1 < n1) {
+        const StepTape<R> tn1 = tape_at(tape + (size_t)(i + 1 - n0) * kTapeFields * n, n);
+        AD_CUDA(cudaMemcpyAsync(tn1.wf, t.wo, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+      }
+    }
+    AD_CUDA(cudaEventRecord(w.ev[3], q));
+    for (int i = n1 - 1; i >= n0; --i) {
+      const StepTape<R> t = tape_at(tape + (size_t)(i - n0) * kTapeFields * n, n);
+      if (in_window(L, i + 1)) ex.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
+      adj_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
+      std::swap(lamA, lamF);
+    }
+    AD_CUDA(cudaGetLastError());
+    AD_CUDA(cudaEventRecord(w.ev[1], q));
+    AD_CUDA(cudaEventSynchronize(w.ev[1]));
+    ms_re += elapsed(w.ev[2], w.ev[3]);
+    ms_adj += elapsed(w.ev[3], w.ev[1]);
+  }
+  if (in_window(L, 0)) ex.cells(gg, OpAStress<R>{gg, ckpt, lamA, scale});
+  for (int v = 0; v < 8; ++v)
+    AD_CUDA(cudaMemcpyAsync(grad[v], lamA + (size_t)v * n, sizeof(R) * n,
+                            grad_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, q));
+  AD_CUDA(cudaStreamSynchronize(q));
+  w.ms[1] = ms_re;
+  w.ms[2] = ms_adj;
+  w.ms[3] = w.ms[0] + ms_re + ms_adj;
+  return NMHD_OK;
+}
+
+}  // namespace
+
+void nmhd_adjoint_release(nmhd_solver *s) {
+  if (!s || !s->adjoint) return;
+  Workspace *w = static_cast<Workspace *>(s->adjoint);
+  cudaFree(w->mem);
+  cudaFree(w->ctl);
+  cudaFree(w->dt_dev);
+  cudaFree(w->hist_dummy);
+  for (auto &e : w->ev)
+    if (e) cudaEventDestroy(e);
+  delete w;
+  s->adjoint = nullptr;
+}
+
+extern "C" {
+
+nmhd_status nmhd_loss_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
+                          double *loss_out, float *dt_out) {
+  nmhd_status st = validate(s, nsteps, 1, loss);
+  if (st != NMHD_OK) return st;
+  if (!loss_out) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "loss_out is NULL");
+  return run<float>(s, nsteps, nsteps, *loss, dt_seq, loss_out, dt_out, nullptr, 0, false);
+}
+
+nmhd_status nmhd_adjoint_run(nmhd_solver *s, int32_t nsteps, int32_t ckpt_every, const nmhd_loss_spec *loss,
+                             const float *dt_seq, double *loss_out, float *dt_out, float *const grad[8],
+                             int on_device) {
+  nmhd_status st = validate(s, nsteps, ckpt_every, loss);
+  if (st != NMHD_OK) return st;
+  if (!loss_out || !grad) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "NULL output");
+  for (int v = 0; v < 8; ++v)
+    if (!grad[v]) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "grad field pointer is NULL");
+  return run<float>(s, nsteps, ckpt_every, *loss, dt_seq, loss_out, dt_out, grad, on_device, true);
+}
+
+nmhd_status nmhd_adjoint_run_f64(nmhd_solver *s, int32_t nsteps, int32_t ckpt_every,
+                                 const nmhd_loss_spec *loss, const float *dt_seq, double *loss_out,
+                                 double *const grad[8]) {
+  nmhd_status st = validate(s, nsteps, ckpt_every, loss);
+  if (st != NMHD_OK) return st;
+  if (!loss_out || !grad || !dt_seq) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  for (int v = 0; v < 8; ++v)
+    if (!grad[v]) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "grad field pointer is NULL");
+  return run<double>(s, nsteps, ckpt_every, *loss, dt_seq, loss_out, nullptr, grad, 0, true);
+}
+
+nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
+                         const double *const dir[8], double *loss_out, double *dloss_out) {
+  nmhd_status st = validate(s, nsteps, 1, loss);
+  if (st != NMHD_OK) return st;
+  if (!loss_out || !dt_seq) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
+  typedef Dual<double> D;
+  Workspace &w = workspace(s);
+  const size_t n = (size_t)s->g.n;
+  const size_t nb = (n + 255) / 256;
+  const size_t need = sizeof(D) * (kTapeFields + 8) * n + sizeof(double) * 8 * n + sizeof(D) * (nb + 4) + 2048;
+  st = reserve(s, w, need);
+  if (st != NMHD_OK) return st;
+  Arena ar{static_cast<char *>(w.mem), 0};
+  D *tape = ar.take<D>((size_t)kTapeFields * n);
+  D *spare = ar.take<D>(8 * n);
+  double *dir_dev = ar.take<double>(8 * n);
+  D *partial = ar.take<D>(nb);
+  D *acc = ar.take<D>(1);
+  const float *cur;
+  double t0;
+  st = solver_state(s, &cur, &t0);
+  if (st != NMHD_OK) return st;
+  cudaStream_t q = s->stream;
+  GpuExec ex{q};
+  const GGrid<double> gg = make_ggrid<double>(s->cfg);
+  const double scale = stress_scale(s->cfg, *loss);
+  if (dir)
+    for (int v = 0; v < 8; ++v) {
+      if (!dir[v]) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "dir field pointer is NULL");
+      AD_CUDA(cudaMemcpyAsync(dir_dev + (size_t)v * n, dir[v], sizeof(double) * n, cudaMemcpyHostToDevice, q));
+    }
+  StepTape<D> t = tape_at(tape, n);
+  D *A = t.wf, *B = spare;
+  ex.items((int)(8 * n), OpWiden<D>{cur, dir ? dir_dev : nullptr, A});
+  AD_CUDA(cudaMemsetAsync(acc, 0, sizeof(D), q));
+  if (in_window(*loss, 0)) ex.reduce(gg, OpStress<D, double>{gg, A}, partial, acc, scale);
+  double time = t0;
+  for (int i = 0; i < nsteps; ++i) {
+    const StepTape<D> ti = {A, t.f1, t.ws, t.f2, B};
+    fwd_step(ex, gg, s->cfg.time_order, time, (double)dt_seq[i], ti);
+    time = time + (double)dt_seq[i];
+    if (in_window(*loss, i + 1)) ex.reduce(gg, OpStress<D, double>{gg, B}, partial, acc, scale);
+    std::swap(A, B);
+  }
+  AD_CUDA(cudaGetLastError());
+  D h;
+  AD_CUDA(cudaMemcpyAsync(&h, acc, sizeof(D), cudaMemcpyDeviceToHost, q));
+  AD_CUDA(cudaStreamSynchronize(q));
+  *loss_out = h.v;
+  if (dloss_out) *dloss_out = h.d;
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_adjoint_timing(const nmhd_solver *s, double ms_out[4]) {
+  if (!s || !ms_out) return NMHD_ERR_INVALID_ARGUMENT;
+  if (!s->adjoint) {
+    for (int i = 0; i < 4; ++i) ms_out[i] = 0.0;
+    return NMHD_OK;
+  }
+  const Workspace *w = static_cast<const Workspace *>(s->adjoint);
+  for (int i = 0; i < 4; ++i) ms_out[i] = w->ms[i];
+  return NMHD_OK;
+}
+
+}  // extern "C"

@@ -53,6 +53,10 @@ __device__ __forceinline__ float divs(float x, float d, float inv) {
 // Time step of the current step: min(goal, CFL), clamped to the goal
 // (src/library/mhd_solver.inlrb:870-901).
 __device__ __forceinline__ float step_dt(const StepCtl *c, bool *last) {
+  if (c->dt_seq) {
+    if (last) *last = false;
+    return c->dt_seq[c->generation - c->dt_seq_base];
+  }
   const float cmin = __uint_as_float(c->cfl_cur);
   float dt = fminf(c->goal, cmin);
   const double next_time = c->time + (double)dt;

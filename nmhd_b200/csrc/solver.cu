@@ -18,26 +18,11 @@
 #include <vector>
 
 #include "../../include/nmhd.h"
+#include "solver_impl.h"
 #include "step.cuh"
 
 using nmhd::GridParams;
 using nmhd::StepCtl;
-
-struct nmhd_solver {
-  nmhd_config cfg;
-  GridParams g;
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool own_stream = false;
-  float *w0 = nullptr, *w1 = nullptr, *wp = nullptr, *flux = nullptr, *dt_hist = nullptr;
-  StepCtl *ctl = nullptr;
-  double *diag = nullptr;
-  bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
-  int variant = 2;         // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks
-  nmhd::TileShape shape = {8, 16};
-  std::map<int, cudaGraphExec_t> graphs;
-  std::string err;
-};
 
 namespace {
 
@@ -271,6 +256,7 @@ void nmhd_destroy(nmhd_solver *s) {
   if (!s) return;
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graphs(s);
+  nmhd_adjoint_release(s);
   cudaFree(s->w0);
   cudaFree(s->w1);
   cudaFree(s->wp);

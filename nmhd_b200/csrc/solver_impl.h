@@ -1,0 +1,31 @@
+// Host-side state of one nmhd_solver handle, shared by the translation units
+// that implement its C ABI (solver.cu: stepping, I/O, autotuning; adjoint.cu:
+// differentiation).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <map>
+#include <string>
+
+#include "../../include/nmhd.h"
+#include "step.cuh"
+
+struct nmhd_solver {
+  nmhd_config cfg;
+  nmhd::GridParams g;
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool own_stream = false;
+  float *w0 = nullptr, *w1 = nullptr, *wp = nullptr, *flux = nullptr, *dt_hist = nullptr;
+  nmhd::StepCtl *ctl = nullptr;
+  double *diag = nullptr;
+  bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
+  int variant = 2;         // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks
+  nmhd::TileShape shape = {8, 16};
+  std::map<int, cudaGraphExec_t> graphs;
+  std::string err;
+  void *adjoint = nullptr;  // differentiation workspace (adjoint.cu), allocated on first use
+};
+
+// Frees the differentiation workspace of a handle (adjoint.cu).
+void nmhd_adjoint_release(nmhd_solver *s);

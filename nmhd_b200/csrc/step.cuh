@@ -40,6 +40,10 @@ struct StepCtl {
   int status;                 // kStatus* bits
   unsigned blocks_done;       // last-block detection in the final stage
   int hist_cap;
+  // Frozen time steps (adjoint and its finite-difference checks): when dt_seq
+  // is set, step n uses dt_seq[generation - dt_seq_base] instead of the CFL dt.
+  const float *dt_seq;
+  long long dt_seq_base;
 };
 
 enum : int { kStatusNumerical = 1, kStatusBadDt = 2 };

@@ -35,6 +35,10 @@ __device__ __forceinline__ int wrapi(int v, int s) {
 }
 
 __device__ __forceinline__ float dt_of(const StepCtl *c, bool *last) {
+  if (c->dt_seq) {
+    if (last) *last = false;
+    return c->dt_seq[c->generation - c->dt_seq_base];
+  }
   const float cmin = __uint_as_float(c->cfl_cur);
   float dt = fminf(c->goal, cmin);
   const double next_time = c->time + (double)dt;

@@ -217,3 +217,80 @@ class MHDSolver:
 
     def set_stream(self, stream_ptr):
         _check(self._L, self._h, self._L.nmhd_set_stream(self._h, ctypes.c_void_p(stream_ptr)))
+
+    # -- differentiation (no counterpart in the reference) ------------------
+    def _loss(self, nsteps, window):
+        first, last = (0, nsteps) if window is None else window
+        return _lib.LossSpec(_lib.LOSS_MAXWELL_STRESS, int(first), int(last), 0)
+
+    @staticmethod
+    def _dts(dt, nsteps):
+        if dt is None:
+            return None
+        d = np.ascontiguousarray(dt, np.float32)
+        if d.shape != (nsteps,):
+            raise ValueError(f"dt must have {nsteps} entries")
+        return d
+
+    def loss_run(self, nsteps, window=None, dt=None):
+        """FP32 forward run of ``nsteps`` steps from the current state (which
+        stays unchanged).  Returns (J, dts): J the mean over the states
+        window=(first, last) of the Maxwell stress -<Bx By> (default: all
+        states 0..nsteps), dts the time steps taken (``dt`` freezes them)."""
+        spec = self._loss(nsteps, window)
+        d = self._dts(dt, nsteps)
+        loss = ctypes.c_double()
+        dts = np.zeros(nsteps, np.float32)
+        _check(self._L, self._h, self._L.nmhd_loss_run(
+            self._h, int(nsteps), ctypes.byref(spec), None if d is None else d.ctypes.data,
+            ctypes.byref(loss), dts.ctypes.data))
+        return loss.value, dts
+
+    def adjoint(self, nsteps, window=None, dt=None, ckpt_every=20, out=None):
+        """FP32 adjoint: (J, dJ/d(initial state) as (8, Sz, Sy, Sx) float32, dts)."""
+        spec = self._loss(nsteps, window)
+        d = self._dts(dt, nsteps)
+        if out is None:
+            out = np.zeros((8,) + self.config.shape, np.float32)
+        loss = ctypes.c_double()
+        dts = np.zeros(nsteps, np.float32)
+        _check(self._L, self._h, self._L.nmhd_adjoint_run(
+            self._h, int(nsteps), int(ckpt_every), ctypes.byref(spec), None if d is None else d.ctypes.data,
+            ctypes.byref(loss), dts.ctypes.data, self._ptrs(out), 0))
+        return loss.value, out, dts
+
+    def adjoint_f64(self, nsteps, dt, window=None, ckpt_every=20):
+        """FP64 adjoint with the time steps frozen to ``dt``: (J, gradient float64)."""
+        spec = self._loss(nsteps, window)
+        d = self._dts(dt, nsteps)
+        out = np.zeros((8,) + self.config.shape, np.float64)
+        n = self.config.cells
+        ptrs = (ctypes.c_void_p * 8)(*[out.ctypes.data + 8 * n * v for v in range(8)])
+        loss = ctypes.c_double()
+        _check(self._L, self._h, self._L.nmhd_adjoint_run_f64(
+            self._h, int(nsteps), int(ckpt_every), ctypes.byref(spec), d.ctypes.data, ctypes.byref(loss), ptrs))
+        return loss.value, out
+
+    def tlm(self, nsteps, dt, direction=None, window=None):
+        """FP64 tangent-linear run with frozen ``dt``: (J, dJ[direction])."""
+        spec = self._loss(nsteps, window)
+        d = self._dts(dt, nsteps)
+        ptrs = None
+        if direction is not None:
+            dr = np.ascontiguousarray(direction, np.float64)
+            if dr.shape != (8,) + self.config.shape:
+                raise ValueError("direction must have the state's shape")
+            n = self.config.cells
+            ptrs = (ctypes.c_void_p * 8)(*[dr.ctypes.data + 8 * n * v for v in range(8)])
+        loss = ctypes.c_double()
+        dloss = ctypes.c_double()
+        _check(self._L, self._h, self._L.nmhd_tlm_run(
+            self._h, int(nsteps), ctypes.byref(spec), d.ctypes.data, ptrs, ctypes.byref(loss),
+            ctypes.byref(dloss)))
+        return loss.value, dloss.value
+
+    def adjoint_timing(self):
+        """Device ms of the last adjoint run: forward, recompute, adjoint, total."""
+        ms = np.zeros(4, np.float64)
+        _check(self._L, self._h, self._L.nmhd_adjoint_timing(self._h, ms.ctypes.data))
+        return {"forward": ms[0], "recompute": ms[1], "adjoint": ms[2], "total": ms[3]}
