@@ -42,6 +42,12 @@ WORKLOADS = {
 }
 REF_BINARY = {"mri_shearing_box_128x256x64": "shear256x128x64"}
 ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0)}
+# Differentiation: 64^3 shearing box of the MRI physics (Lx = Ly = Lz = 1,
+# seed 2), 200 FP32 steps, loss = Maxwell stress averaged over states 151..200,
+# checkpoints every 20 steps; 16 central-difference directions (seeds
+# 100..115) with eps = 1e-3 relative to the velocity noise.
+ADJOINTS = {"mri_adjoint_64": dict(n=64, seed=2, steps=200, window=(151, 200), ckpt=20, fd_dirs=16,
+                                   fd_eps=1e-3, tlm_dirs=4)}
 BYTES_PER_CELL_UPDATE = 160  # 8 FP32 state words: stage 1 read+write, stage 2 2x read + write
 
 
@@ -365,6 +371,121 @@ def run_ensemble_arm(args):
         dist.destroy_process_group()
 
 
+def run_adjoint_arm(args):
+    """Adjoint / forward time ratio on the 64^3 shearing box, with the
+    gradient's checks: central differences of the FP32 and FP64 losses along
+    16 seeded initial-velocity directions, the FP64 tangent-linear run along 4
+    of them, and the FP64 adjoint-vs-tangent transpose identity."""
+    import torch
+    from nmhd_b200.problems import shearing_box
+    from nmhd_b200.solver import MHDSolver
+
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    spec = ADJOINTS[args.workload]
+    n = spec["n"]
+    cfg, s = shearing_box(n_radial=n, n_azimuthal=n, n_vertical=n, l_radial=1.0, l_azimuthal=1.0,
+                          l_vertical=1.0, seed=spec["seed"])
+    steps, window, K = spec["steps"], spec["window"], spec["ckpt"]
+    if args.adjoint_steps:  # shorter runs (profiling): the window keeps its length, at the end
+        steps = args.adjoint_steps
+        window = (max(0, steps - (window[1] - window[0])), steps)
+    stream = torch.cuda.Stream(device=dev)
+    sol = MHDSolver(cfg)
+    sol.set_stream(stream.cuda_stream)
+    sol.set_state(s)
+    for _ in range(args.warmup):
+        sol.adjoint(steps, window=window, ckpt_every=K)
+    # forward: the production path (nmhd_proceed, CUDA graphs) over the same steps
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    fwd = []
+    reps = max(1, args.steps // 100)
+    with ClockSampler(dev.index) as clocks:
+        for _ in range(reps):
+            sol.set_state(s)
+            sol.set_time(0.0, 0)
+            sol.step(3)  # builds this box's graphs, then restart
+            sol.set_state(s)
+            sol.set_time(0.0, 0)
+            torch.cuda.synchronize(dev)
+            e0.record(stream)
+            sol.step(steps)
+            e1.record(stream)
+            torch.cuda.synchronize(dev)
+            fwd.append(e0.elapsed_time(e1))
+        sol.set_state(s)
+        sol.set_time(0.0, 0)
+        adj = []
+        for _ in range(reps):
+            J, g, dts = sol.adjoint(steps, window=window, ckpt_every=K)
+            adj.append(sol.adjoint_timing())
+    fwd_ms = statistics.median(fwd)
+    tot = statistics.median([a["total"] for a in adj])
+    rev = statistics.median([a["recompute"] + a["adjoint"] for a in adj])
+    line = {
+        "metric": "adjoint/forward time ratio", "value": tot / fwd_ms, "unit": "x",
+        "n_gpus": world, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing box)",
+        "config": {"workload": args.workload, "cells_interior": cfg.interior_cells,
+                   "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
+                   "ckpt_every": K, "parallelism": "replicas" if world > 1 else "single"},
+        "forward_ms": fwd_ms, "adjoint_total_ms": tot, "adjoint_reverse_ms": rev,
+        "reverse_over_forward": rev / fwd_ms, "phases_ms": adj[-1], "loss": J,
+        "clocks": clocks.summary(),
+    }
+    if not args.no_checks:
+        line["gradient_checks"] = adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg)
+    sol.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg):
+    """Directions dv = sigma * N(0, 1) on the three initial velocity fields,
+    sigma = the noise amplitude 0.01 c_s; eps is relative to it.  The float32
+    rounding of v +- eps dv is part of the perturbation applied."""
+    gd = g.astype(np.float64)
+    sigma = 0.01 * math.sqrt(cfg.gamma)
+    eps = spec["fd_eps"]
+    rows = []
+    for k in range(spec["fd_dirs"]):
+        rng = np.random.default_rng(100 + k)
+        d = np.zeros(s.shape)
+        d[1:4] = sigma * rng.normal(0.0, 1.0, s[1:4].shape)
+        sp = (s + eps * d).astype(np.float32)
+        sm = (s - eps * d).astype(np.float32)
+        d_applied = (sp.astype(np.float64) - sm.astype(np.float64)) / (2 * eps)
+        sol.set_state(sp)
+        jp32, _ = sol.loss_run(steps, window=window, dt=dts)
+        jp64, _ = sol.tlm(steps, dts, None, window=window)
+        sol.set_state(sm)
+        jm32, _ = sol.loss_run(steps, window=window, dt=dts)
+        jm64, _ = sol.tlm(steps, dts, None, window=window)
+        sol.set_state(s)
+        row = {"fd32": (jp32 - jm32) / (2 * eps), "fd64": (jp64 - jm64) / (2 * eps),
+               "adjoint32": float(np.sum(gd * d_applied))}
+        if k < spec["tlm_dirs"]:
+            row["tlm64"] = sol.tlm(steps, dts, d_applied, window=window)[1]
+        rows.append(row)
+
+    def rel(a, b):
+        v = np.array([abs(r[a] - r[b]) / abs(r[b]) for r in rows if a in r and b in r])
+        return {"median": float(np.median(v)), "max": float(np.max(v)), "n": int(len(v)),
+                "within_1e-3": int(np.sum(v < 1e-3))}
+    rng = np.random.default_rng(99)
+    d = np.zeros(s.shape)
+    d[1:4] = sigma * rng.normal(0.0, 1.0, s[1:4].shape)
+    _, dJ64 = sol.tlm(steps, dts, d, window=window)
+    _, g64 = sol.adjoint_f64(steps, dts, window=window, ckpt_every=K)
+    return {"directions": spec["fd_dirs"], "eps_relative_to_noise": eps, "noise_sigma": sigma,
+            "adjoint32_vs_fd32": rel("adjoint32", "fd32"), "adjoint32_vs_fd64": rel("adjoint32", "fd64"),
+            "adjoint32_vs_tlm64": rel("adjoint32", "tlm64"), "tlm64_vs_fd64": rel("tlm64", "fd64"),
+            "fd32_vs_fd64": rel("fd32", "fd64"),
+            "fp64_adjoint_transpose_rel": abs(float(np.sum(g64 * d)) - dJ64) / abs(dJ64)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -372,15 +493,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="nmhd", choices=["nmhd", "reference"])
     ap.add_argument("--workload", default="mri_shearing_box_128x256x64",
-                    choices=sorted(WORKLOADS) + sorted(ENSEMBLES))
+                    choices=sorted(WORKLOADS) + sorted(ENSEMBLES) + sorted(ADJOINTS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
+    ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
+    ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint workload: steps per run (default 200)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":
         run_reference_arm(args)
     elif args.workload in ENSEMBLES:
         run_ensemble_arm(args)
+    elif args.workload in ADJOINTS:
+        run_adjoint_arm(args)
     else:
         run_gpu_arm(args)
 

@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -151,9 +152,10 @@ nmhd_status set_err(nmhd_solver *s, nmhd_status st, const std::string &m) {
                      std::string(#call) + ": " + cudaGetErrorString(e_));                            \
   } while (0)
 
-// One arena per run: the run's buffers are carved from it in order.
+// One arena per run: the run's buffers are carved from it in order.  A dry
+// run with base 0 measures the bytes the same carve sequence needs.
 struct Arena {
-  char *base;
+  uintptr_t base;
   size_t off;
   template <class T>
   T *take(size_t count) {
@@ -277,23 +279,26 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   const bool frozen = dt_seq != nullptr;
   if (!Prec<R>::kProduction && !frozen)
     return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "dt_seq is required for FP64 runs");
-  // arena
+  // arena: checkpoints, one segment's tape, the primal pass's ping-pong
+  // partner, 3 adjoint states, adjoint scratch, reduction partials
   const size_t nb = (n + 255) / 256;
-  size_t need = 0;
-  need += sizeof(R) * (want_grad ? (size_t)nseg * 8 * n : 0) + 256;  // checkpoints
-  need += sizeof(R) * (size_t)tape_steps * kTapeFields * n + 256;     // tape
-  need += sizeof(R) * (want_grad ? (24 + kAdjScratchFields) * n : 8 * n) + 512;
-  need += sizeof(double) * (nb + 8) + 512;
-  nmhd_status st = reserve(s, w, need);
+  R *ckpt = nullptr, *tape = nullptr, *spare = nullptr, *lam = nullptr, *scr = nullptr;
+  double *partial = nullptr, *acc = nullptr;
+  auto carve = [&](Arena &ar) {
+    ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
+    tape = ar.take<R>((size_t)tape_steps * kTapeFields * n);
+    spare = ar.take<R>(8 * n);
+    lam = want_grad ? ar.take<R>(24 * n) : nullptr;
+    scr = want_grad ? ar.take<R>((size_t)kAdjScratchFields * n) : nullptr;
+    partial = ar.take<double>(nb);
+    acc = ar.take<double>(1);
+  };
+  Arena probe{0, 0};
+  carve(probe);
+  nmhd_status st = reserve(s, w, probe.off + 256);
   if (st != NMHD_OK) return st;
-  Arena ar{static_cast<char *>(w.mem), 0};
-  R *ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
-  R *tape = ar.take<R>((size_t)tape_steps * kTapeFields * n);
-  R *spare = ar.take<R>(8 * n);  // ping-pong partner of the primal pass
-  R *lam = want_grad ? ar.take<R>(24 * n) : nullptr;
-  R *scr = want_grad ? ar.take<R>((size_t)kAdjScratchFields * n) : nullptr;
-  double *partial = ar.take<double>(nb);
-  double *acc = ar.take<double>(1);
+  Arena ar{reinterpret_cast<uintptr_t>(w.mem), 0};
+  carve(ar);
 
   const float *cur;
   double t0;
@@ -469,15 +474,21 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
   Workspace &w = workspace(s);
   const size_t n = (size_t)s->g.n;
   const size_t nb = (n + 255) / 256;
-  const size_t need = sizeof(D) * (kTapeFields + 8) * n + sizeof(double) * 8 * n + sizeof(D) * (nb + 4) + 2048;
-  st = reserve(s, w, need);
+  D *tape = nullptr, *spare = nullptr, *partial = nullptr, *acc = nullptr;
+  double *dir_dev = nullptr;
+  auto carve = [&](Arena &ar) {
+    tape = ar.take<D>((size_t)kTapeFields * n);
+    spare = ar.take<D>(8 * n);
+    dir_dev = ar.take<double>(8 * n);
+    partial = ar.take<D>(nb);
+    acc = ar.take<D>(1);
+  };
+  Arena probe{0, 0};
+  carve(probe);
+  st = reserve(s, w, probe.off + 256);
   if (st != NMHD_OK) return st;
-  Arena ar{static_cast<char *>(w.mem), 0};
-  D *tape = ar.take<D>((size_t)kTapeFields * n);
-  D *spare = ar.take<D>(8 * n);
-  double *dir_dev = ar.take<double>(8 * n);
-  D *partial = ar.take<D>(nb);
-  D *acc = ar.take<D>(1);
+  Arena ar{reinterpret_cast<uintptr_t>(w.mem), 0};
+  carve(ar);
   const float *cur;
   double t0;
   st = solver_state(s, &cur, &t0);
