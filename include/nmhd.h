@@ -251,9 +251,11 @@ nmhd_status nmhd_adjoint_run_f64(nmhd_solver *s, int32_t nsteps, int32_t ckpt_ev
                                  double *const grad[8]);
 /* FP64 tangent-linear run: J and its directional derivative dJ[dir] along
  * dir[8] (host, 8 fields of Sx*Sy*Sz doubles; NULL: J only), forward mode in
- * double from the float initial state.  dt_seq is required. */
+ * double.  The run starts from the solver's float state plus shift*dir, in
+ * double, so central differences of J in FP64 can use perturbations far below
+ * float rounding (shift is ignored when dir is NULL).  dt_seq is required. */
 nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
-                         const double *const dir[8], double *loss_out, double *dloss_out);
+                         const double *const dir[8], double shift, double *loss_out, double *dloss_out);
 /* Device time of the last nmhd_adjoint_run / nmhd_adjoint_run_f64 in ms:
  * [0] forward run with checkpoints, [1] segment recomputation, [2] adjoint
  * kernels, [3] the whole run. */

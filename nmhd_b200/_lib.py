@@ -67,7 +67,7 @@ _SIGS = [
                                         ctypes.POINTER(ctypes.c_double), _P, ctypes.POINTER(_P), ctypes.c_int]),
     ("nmhd_adjoint_run_f64", ctypes.c_int, [_P, ctypes.c_int32, ctypes.c_int32, _P, _P,
                                             ctypes.POINTER(ctypes.c_double), ctypes.POINTER(_P)]),
-    ("nmhd_tlm_run", ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.POINTER(_P),
+    ("nmhd_tlm_run", ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.POINTER(_P), ctypes.c_double,
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("nmhd_adjoint_timing", ctypes.c_int, [_P, _P]),
     ("nmhd_batch_create", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),

@@ -33,6 +33,7 @@ template <class R>
 struct GGrid {
   int sx, sy, sz, n, my, mz, shear, order2;
   R dx, dy, dz, gamma, cfl, q, omega, corner_y, extent_x;
+  R idx, idy, idz;  // 1/dx, 1/dy, 1/dz (adjoint only; the forward divides)
   double rel_vel;
 };
 
@@ -56,6 +57,11 @@ NMHD_HD int shifted(const GGrid<R> &g, int x, int y, int z, int a, int k) {
 template <class R>
 NMHD_HD R spacing(const GGrid<R> &g, int a) {
   return a == 0 ? g.dx : (a == 1 ? g.dy : g.dz);
+}
+
+template <class R>
+NMHD_HD R inv_spacing(const GGrid<R> &g, int a) {
+  return a == 0 ? g.idx : (a == 1 ? g.idy : g.idz);
 }
 
 // ---------------------------------------------------------------------------
@@ -435,8 +441,8 @@ NMHD_HD R corner_adj(const GGrid<R> &g, const R *lamBn, int x, int y, int z, int
   const int e = cell_at(g, x, y, z);
   const R la_here = lamBn[a * N + e], la_below = lamBn[a * N + shifted(g, x, y, z, b, -1)];
   const R lb_here = lamBn[b * N + e], lb_below = lamBn[b * N + shifted(g, x, y, z, a, -1)];
-  const R ca = h * R(0.5f) / spacing(g, b);
-  const R cb = h * R(0.5f) / spacing(g, a);
+  const R ca = h * R(0.5f) * inv_spacing(g, b);
+  const R cb = h * R(0.5f) * inv_spacing(g, a);
   return ca * (la_below - la_here) - cb * (lb_below - lb_here);
 }
 
@@ -460,7 +466,7 @@ NMHD_HD void a_flux_cell(const GGrid<R> &g, const R *win, const R *lamBn, const 
   for (int ax = 0; ax < 3; ++ax) {
     const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
     const int om = shifted(g, x, y, z, ax, -1);
-    const R c = h / spacing(g, ax);
+    const R c = h * inv_spacing(g, ax);
     R lfa[5];
     for (int k = 0; k < 5; ++k) lfa[k] = c * (lamU[k * N + o] - lamU[k * N + om]);
     R lf[7];

@@ -82,6 +82,9 @@ GGrid<R> make_ggrid(const nmhd_config &c) {
   g.dx = d[0];
   g.dy = d[1];
   g.dz = d[2];
+  g.idx = (R)1 / g.dx;
+  g.idy = (R)1 / g.dy;
+  g.idz = (R)1 / g.dz;
   g.extent_x = comp[0];
   g.corner_y = -comp[1] / (R)2;
   g.gamma = (R)c.gamma;

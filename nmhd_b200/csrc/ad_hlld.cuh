@@ -206,15 +206,18 @@ NMHD_HD void hadj_zero(HAdj<R> &a) {
   a.q = a.bys = a.bzs = a.vBs = a.es = a.sd = a.cf = R(0);
 }
 
-// Reverse of hlld_side_energy and hlld_side_star for one side.
+// Reverse of hlld_side_energy and hlld_side_star for one side.  The reverse
+// sweep needs no correctly rounded quotients: each denominator is inverted
+// once and multiplied (the forward tape above keeps the exact divisions).
 template <class R>
 NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, const R pT_s, HAdj<R> &a, R &aSM,
                                 R &apTs, R &aBx, R &aB2x, R &aS) {
+  const R ism = R(1) / s.sm, idn = R(1) / s.dn;
   // sd = sqrt(ds)
-  if (s.sd > R(0)) a.ds += a.sd / (s.sd + s.sd);
+  if (s.sd > R(0)) a.ds += a.sd * (R(0.5) / s.sd);
   // es = (sv*e - pT*u + pT_s*S_M + Bx*(vB - vBs)) / sm
   {
-    const R t = a.es / s.sm;
+    const R t = a.es * ism;
     a.sv += t * s.e;
     a.e += t * s.sv;
     a.pT -= t * s.u;
@@ -234,26 +237,24 @@ NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, cons
   a.ws += a.vBs * s.bzs;
   a.bzs += a.vBs * s.ws;
   // bys = by*q/dn, bzs = bz*q/dn
-  a.by += a.bys * s.q / s.dn;
-  a.q += a.bys * s.by / s.dn;
-  a.dn -= a.bys * s.bys / s.dn;
-  a.bz += a.bzs * s.q / s.dn;
-  a.q += a.bzs * s.bz / s.dn;
-  a.dn -= a.bzs * s.bzs / s.dn;
+  a.by += a.bys * s.q * idn;
+  a.bz += a.bzs * s.q * idn;
+  a.q += (a.bys * s.by + a.bzs * s.bz) * idn;
+  a.dn -= (a.bys * s.bys + a.bzs * s.bzs) * idn;
   // q = d*sv^2 - B2x
   a.d += a.q * s.sv * s.sv;
   a.sv += a.q * R(2) * s.d * s.sv;
   aB2x -= a.q;
   // vs = v - Bx*by*(S_M - u)/dn, ws = w - Bx*bz*(S_M - u)/dn
   {
-    const R g = (S_M - s.u) / s.dn;
+    const R g = (S_M - s.u) * idn;
     const R tv = -a.vs, tw = -a.ws;
     a.v += a.vs;
     a.w += a.ws;
-    aBx += tv * s.by * g + tw * s.bz * g;
+    aBx += (tv * s.by + tw * s.bz) * g;
     a.by += tv * Bx * g;
     a.bz += tw * Bx * g;
-    const R c = (tv * Bx * s.by + tw * Bx * s.bz) / s.dn;
+    const R c = (tv * s.by + tw * s.bz) * Bx * idn;
     aSM += c;
     a.u -= c;
     a.dn -= c * g;
@@ -264,9 +265,12 @@ NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, cons
   a.sm += a.dn * s.d * s.sv;
   aB2x -= a.dn;
   // ds = d*sv/sm
-  a.d += a.ds * s.sv / s.sm;
-  a.sv += a.ds * s.d / s.sm;
-  a.sm -= a.ds * s.ds / s.sm;
+  {
+    const R t = a.ds * ism;
+    a.d += t * s.sv;
+    a.sv += t * s.d;
+    a.sm -= t * s.ds;
+  }
   // sm = S - S_M
   aS += a.sm;
   aSM -= a.sm;
@@ -285,22 +289,22 @@ NMHD_HD void hlld_side_vB_rev(const HSide<R> &s, const R Bx, HAdj<R> &a, R &aBx)
 
 // Reverse of hlld_side_pre (after pT, cf, e, mx.. have their adjoints).
 template <class R>
-NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R gm1, const R B2x, HAdj<R> &a,
+NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R igm1, const R B2x, HAdj<R> &a,
                                R &aB2x) {
   // pT = p + 0.5*B2
   a.p += a.pT;
   a.B2 += R(0.5) * a.pT;
   // cf = sqrt(num/(2d))
   if (s.cf > R(0)) {
-    const R aQ = a.cf / (s.cf + s.cf);
-    const R twod = R(2) * s.d;
-    const R Q = s.num / twod;
-    const R anum = aQ / twod;
-    a.d -= aQ * Q / s.d;
+    const R id = R(1) / s.d;
+    const R aQ = a.cf * (R(0.5) / s.cf);
+    const R Q = R(0.5) * s.num * id;
+    const R anum = R(0.5) * aQ * id;
+    a.d -= aQ * Q * id;
     // num = gpb + sq; sq = sqrt(disc); disc = gpb^2 - 4 gp B2x; gpb = gp + B2
     R agpb = anum, agp = R(0);
     if (s.sq > R(0)) {
-      const R adisc = anum / (s.sq + s.sq);
+      const R adisc = anum * (R(0.5) / s.sq);
       agpb += adisc * R(2) * s.gpb;
       agp -= adisc * R(4) * B2x;
       aB2x -= adisc * R(4) * s.gp;
@@ -310,7 +314,7 @@ NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R gm1, co
     a.p += gamma * agp;
   }
   // e = p/gm1 + 0.5*d*v2 + 0.5*B2
-  a.p += a.e / gm1;
+  a.p += a.e * igm1;
   a.d += R(0.5) * a.e * s.v2;
   a.v2 += R(0.5) * a.e * s.d;
   a.B2 += R(0.5) * a.e;
@@ -326,6 +330,7 @@ NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R gm1, co
   a.v += a.my * s.d;
   a.w += a.mz * s.d;
 }
+
 
 // Reverse of the region flux (hlld_flux_side) and of the double-star states.
 template <bool kLeft, class R>
@@ -464,7 +469,7 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
   }
   // sdLR = sqrt(dLs*dRs)
   if (t.sdLR > R(0)) {
-    const R c = asdLR / (t.sdLR + t.sdLR);
+    const R c = asdLR * (R(0.5) / t.sdLR);
     aL.ds += c * t.R.ds;
     aR.ds += c * t.L.ds;
   }
@@ -476,12 +481,15 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
   }
   // Sss = S_L* = S_M - |Bx|/sdL (left) or S_R* = S_M + |Bx|/sdR (right)
   aSM += aSss;
-  if (kLeft) {
-    aabs -= aSss / s.sd;
-    aX.sd += aSss * t.absBx / (s.sd * s.sd);
-  } else {
-    aabs += aSss / s.sd;
-    aX.sd -= aSss * t.absBx / (s.sd * s.sd);
+  {
+    const R isd = R(1) / s.sd;
+    if (kLeft) {
+      aabs -= aSss * isd;
+      aX.sd += aSss * t.absBx * isd * isd;
+    } else {
+      aabs += aSss * isd;
+      aX.sd -= aSss * t.absBx * isd * isd;
+    }
   }
 }
 
@@ -507,8 +515,9 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
 
     // --- S_M = SMn/den, pT* = pTn/den ---------------------------------------------
     {
-      const R aSMn = aSM / t.den, apTn = apTs / t.den;
-      const R aden = -(aSM * t.S_M + apTs * t.pT_s) / t.den;
+      const R iden = R(1) / t.den;
+      const R aSMn = aSM * iden, apTn = apTs * iden;
+      const R aden = -(aSM * t.S_M + apTs * t.pT_s) * iden;
       const R dl = t.L.d, dr = t.R.d, sLv = t.L.sv, sRv = t.R.sv, du = t.R.u - t.L.u;
       // pTn = sRv*dr*pTL - sLv*dl*pTR + dl*dr*sRv*sLv*(ur - ul)
       aR.sv += apTn * (dr * t.L.pT + dl * dr * sLv * du);
@@ -547,9 +556,9 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
   }
   hlld_side_vB_rev(t.L, Bx, aL, aBx);
   hlld_side_vB_rev(t.R, Bx, aR, aBx);
-  const R gm1 = gamma - R(1);
-  hlld_side_pre_rev(t.L, gamma, gm1, t.B2x, aL, aB2x);
-  hlld_side_pre_rev(t.R, gamma, gm1, t.B2x, aR, aB2x);
+  const R igm1 = R(1) / (gamma - R(1));
+  hlld_side_pre_rev(t.L, gamma, igm1, t.B2x, aL, aB2x);
+  hlld_side_pre_rev(t.R, gamma, igm1, t.B2x, aR, aB2x);
   aBx += R(2) * Bx * aB2x + aabs * sgn;
 
   ls.dl = aL.d; ls.dr = aR.d; ls.ul = aL.u; ls.ur = aR.u; ls.vl = aL.v; ls.vr = aR.v;

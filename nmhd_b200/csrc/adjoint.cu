@@ -33,8 +33,19 @@ namespace {
 
 constexpr int BX = 32, BY = 4, BZ = 2;
 
+// Resident CTAs per SM asked of the compiler: the FP32 HLLD adjoint is
+// latency-bound at one 256-thread CTA per SM, so it is held to 128 registers.
 template <class F>
-__global__ void __launch_bounds__(BX *BY *BZ) k_ad_cells(F f, int sx, int sy, int sz) {
+struct MinBlocks {
+  static constexpr int value = 1;
+};
+template <>
+struct MinBlocks<OpAFlux<float>> {
+  static constexpr int value = 2;
+};
+
+template <class F, int kMinBlocks>
+__global__ void __launch_bounds__(BX *BY *BZ, kMinBlocks) k_ad_cells(F f, int sx, int sy, int sz) {
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
   const int z = blockIdx.z * BZ + threadIdx.z;
@@ -87,9 +98,10 @@ __global__ void __launch_bounds__(256) k_ad_reduce_final(const D *partial, int n
 }
 
 template <class T>
-struct OpWiden {  // float state -> T (with an optional tangent)
+struct OpWiden {  // float state (+ shift * dir) -> T, with dir as the tangent
   const float *src;
   const double *dir;
+  double shift;
   T *dst;
   NMHD_HD void operator()(int i) const;
 };
@@ -97,7 +109,7 @@ template <>
 NMHD_HD void OpWiden<double>::operator()(int i) const { dst[i] = (double)src[i]; }
 template <>
 NMHD_HD void OpWiden<Dual<double>>::operator()(int i) const {
-  dst[i] = Dual<double>((double)src[i], dir ? dir[i] : 0.0);
+  dst[i] = dir ? Dual<double>((double)src[i] + shift * dir[i], dir[i]) : Dual<double>((double)src[i], 0.0);
 }
 
 struct GpuExec {
@@ -105,7 +117,7 @@ struct GpuExec {
   template <class R, class F>
   void cells(const GGrid<R> &g, const F &f) {
     const dim3 grid((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (g.sz + BZ - 1) / BZ);
-    k_ad_cells<<<grid, dim3(BX, BY, BZ), 0, st>>>(f, g.sx, g.sy, g.sz);
+    k_ad_cells<F, MinBlocks<F>::value><<<grid, dim3(BX, BY, BZ), 0, st>>>(f, g.sx, g.sy, g.sz);
   }
   template <class F>
   void items(int n, const F &f) {
@@ -319,7 +331,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   if constexpr (Prec<R>::kProduction) {
     AD_CUDA(cudaMemcpyAsync(A, cur, sizeof(float) * 8 * n, cudaMemcpyDeviceToDevice, q));
   } else {
-    ex.items((int)(8 * n), OpWiden<R>{cur, nullptr, A});
+    ex.items((int)(8 * n), OpWiden<R>{cur, nullptr, 0.0, A});
   }
   if (in_window(L, 0)) ex.reduce(gg, OpStress<R, R>{gg, A}, partial, acc, scale);
   std::vector<float> dts(nsteps);
@@ -466,7 +478,7 @@ nmhd_status nmhd_adjoint_run_f64(nmhd_solver *s, int32_t nsteps, int32_t ckpt_ev
 }
 
 nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
-                         const double *const dir[8], double *loss_out, double *dloss_out) {
+                         const double *const dir[8], double shift, double *loss_out, double *dloss_out) {
   nmhd_status st = validate(s, nsteps, 1, loss);
   if (st != NMHD_OK) return st;
   if (!loss_out || !dt_seq) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "NULL argument");
@@ -504,7 +516,7 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
     }
   StepTape<D> t = tape_at(tape, n);
   D *A = t.wf, *B = spare;
-  ex.items((int)(8 * n), OpWiden<D>{cur, dir ? dir_dev : nullptr, A});
+  ex.items((int)(8 * n), OpWiden<D>{cur, dir ? dir_dev : nullptr, shift, A});
   AD_CUDA(cudaMemsetAsync(acc, 0, sizeof(D), q));
   if (in_window(*loss, 0)) ex.reduce(gg, OpStress<D, double>{gg, A}, partial, acc, scale);
   double time = t0;

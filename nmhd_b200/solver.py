@@ -271,8 +271,9 @@ class MHDSolver:
             self._h, int(nsteps), int(ckpt_every), ctypes.byref(spec), d.ctypes.data, ctypes.byref(loss), ptrs))
         return loss.value, out
 
-    def tlm(self, nsteps, dt, direction=None, window=None):
-        """FP64 tangent-linear run with frozen ``dt``: (J, dJ[direction])."""
+    def tlm(self, nsteps, dt, direction=None, window=None, shift=0.0):
+        """FP64 tangent-linear run with frozen ``dt`` from the current state
+        plus ``shift * direction`` (in double): (J, dJ[direction])."""
         spec = self._loss(nsteps, window)
         d = self._dts(dt, nsteps)
         ptrs = None
@@ -285,7 +286,7 @@ class MHDSolver:
         loss = ctypes.c_double()
         dloss = ctypes.c_double()
         _check(self._L, self._h, self._L.nmhd_tlm_run(
-            self._h, int(nsteps), ctypes.byref(spec), d.ctypes.data, ptrs, ctypes.byref(loss),
+            self._h, int(nsteps), ctypes.byref(spec), d.ctypes.data, ptrs, float(shift), ctypes.byref(loss),
             ctypes.byref(dloss)))
         return loss.value, dloss.value
 

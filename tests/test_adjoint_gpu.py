@@ -4,8 +4,8 @@ nmhd_adjoint_run, nmhd_adjoint_run_f64, nmhd_tlm_run).
 The FP32 runs use the production kernels for the forward pass, so their time
 steps and trajectory are the oracle's; the adjoint kernels are checked against
 the host build of the same per-cell adjoint (tests/native), against the GPU
-tangent-linear run (transpose identity in FP64), and against central finite
-differences of the FP32 loss along initial-velocity directions.  A
+tangent-linear run (transpose identity in FP64), and against FP64 central
+differences of the loss along initial-velocity directions.  A
 torch.autograd.Function wrapper (test harness only) exposes the adjoint as a
 backward pass.
 """
@@ -110,29 +110,27 @@ def test_fp64_adjoint_is_the_transpose_of_the_gpu_tangent_linear_run(gpu, case):
     assert dJ == pytest.approx(dJh, rel=1e-10, abs=1e-13 * abs(J) + 1e-300)
 
 
-def test_fp32_gradient_agrees_with_fd_and_fp64_tangent_on_a_shearing_box(gpu):
+def test_gradient_agrees_with_fp64_central_differences_on_a_shearing_box(gpu):
+    """Central differences in FP64 around the same float state (shift), with
+    eps far below the perturbation at which limiter, upwind-corner or sign(Bx)
+    choices start to flip: the discrete step is only piecewise smooth, so a
+    larger eps measures those jumps, not the derivative."""
     cfg, s = shearing_box(n_radial=24, n_azimuthal=32, n_vertical=16, l_radial=1.0, l_azimuthal=1.0, seed=2)
     steps, window = 30, (21, 30)
     with MHDSolver(cfg) as sol:
         sol.set_state(s)
         J, g, dts = sol.adjoint(steps, window=window, ckpt_every=10)
+        _, g64 = sol.adjoint_f64(steps, dts, window=window, ckpt_every=10)
         for k in range(3):
             d = _velocity_direction(s.shape, 100 + k)
-            eps = 1e-3
-            sp = (s + eps * d).astype(np.float32)
-            sm = (s - eps * d).astype(np.float32)
-            sol.set_state(sp)
-            Jp, _ = sol.loss_run(steps, window=window, dt=dts)
-            sol.set_state(sm)
-            Jm, _ = sol.loss_run(steps, window=window, dt=dts)
-            sol.set_state(s)
+            eps = 1e-8
+            Jp, _ = sol.tlm(steps, dts, d, window=window, shift=eps)
+            Jm, _ = sol.tlm(steps, dts, d, window=window, shift=-eps)
             fd = (Jp - Jm) / (2 * eps)
-            # the float32 rounding of s +- eps d is part of the perturbation applied
-            d_applied = (sp.astype(np.float64) - sm.astype(np.float64)) / (2 * eps)
             _, dJ = sol.tlm(steps, dts, d, window=window)
-            ad = float(np.sum(g.astype(np.float64) * d))
-            assert ad == pytest.approx(dJ, rel=1e-3)
-            assert float(np.sum(g.astype(np.float64) * d_applied)) == pytest.approx(fd, rel=1e-2)
+            assert dJ == pytest.approx(fd, rel=1e-4)
+            assert float(np.sum(g64 * d)) == pytest.approx(fd, rel=1e-4)
+            assert float(np.sum(g.astype(np.float64) * d)) == pytest.approx(fd, rel=1e-2)
 
 
 def test_window_edges_and_initial_state_term(gpu):
