@@ -445,7 +445,7 @@ def run_adjoint_arm(args):
 def adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg):
     """Directions dv = sigma * N(0, 1) on the three initial velocity fields,
     sigma = the noise amplitude 0.01 c_s.  The derivative is checked against
-    FP64 central differences around the same float state with eps = 1e-8
+    FP64 central differences around the same float state with eps = 1e-9
     (relative to sigma), below the scale at which limiter, upwind-corner and
     sign(Bx) choices flip; differences at the nominal eps = 1e-3 (FP32 and
     FP64) are reported beside them: they measure those jumps of the piecewise
@@ -453,7 +453,7 @@ def adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg):
     gd = g.astype(np.float64)
     sigma = 0.01 * math.sqrt(cfg.gamma)
     eps = spec["fd_eps"]
-    eps_small = 1e-8
+    eps_small = 1e-9
     rows = []
     for k in range(spec["fd_dirs"]):
         rng = np.random.default_rng(100 + k)

@@ -14,9 +14,10 @@
 // and results are deterministic:
 //   a_prim_cell    to_primitive + kick + conserved update (per cell)
 //   a_bface_cell   face-B adjoint: output B, energy terms of old and new B
-//   a_flux_cell    CT transpose and flux divergence transpose -> adjoint of the
-//                  21 face fluxes of the cell -> HLLD adjoint per face
-//   a_recon_cell   minbee reconstruction, face kick and normal-B transposes
+//   a_flux_face    CT transpose and flux divergence transpose -> adjoint of the
+//                  7 fluxes of one face of the cell -> HLLD adjoint (per axis)
+//   a_recon_face   minbee reconstruction, face kick and normal-B transposes
+//                  (per axis)
 //   a_bc_cell      transverse cell-centred B average transpose
 //   a_fill_*       transpose of the shearing-periodic and Z margin fills
 // References: src/library/mhd_solver.inlrb:140-155 (reconstruction), 184-259
@@ -420,75 +421,148 @@ NMHD_HD void a_bface_cell(const GGrid<R> &g, const R *wb, const R *wo, const R *
   }
 }
 
-// Upwind weights of the corner at edge (x, y, z): c0 on F[e - b], c1 on F[e].
-template <class R>
-NMHD_HD void corner_weights(const GGrid<R> &g, const R *vb, int x, int y, int z, int a, int b, R &c0, R &c1) {
-  const int e = cell_at(g, x, y, z);
-  const int eb = shifted(g, x, y, z, b, -1);
-  const int ea = shifted(g, x, y, z, a, -1);
-  const int eab = cell_at(g, x - (a == 0 || b == 0), y - (a == 1 || b == 1), z - (a == 2 || b == 2));
-  const R w = vb[e] + vb[eb] + vb[ea] + vb[eab];
-  c0 = w > R(0) ? R(1) : (w < R(0) ? R(0) : R(0.5f));
-  c1 = w > R(0) ? R(0) : (w < R(0) ? R(1) : R(0.5f));
-}
-
-// Adjoint of the corner value C = F_a(B_b) at edge (x, y, z).  In every
-// family (XY, YX, XZ, ZX, YZ, ZY) the corner enters the face-B updates as
-//   dB_a[o] = +h/2 (C[o+b] - C[o]) / d_b,   dB_b[o] = -h/2 (C[o+a] - C[o]) / d_a.
-template <class R>
-NMHD_HD R corner_adj(const GGrid<R> &g, const R *lamBn, int x, int y, int z, int a, int b, R h) {
-  const size_t N = (size_t)g.n;
-  const int e = cell_at(g, x, y, z);
-  const R la_here = lamBn[a * N + e], la_below = lamBn[a * N + shifted(g, x, y, z, b, -1)];
-  const R lb_here = lamBn[b * N + e], lb_below = lamBn[b * N + shifted(g, x, y, z, a, -1)];
-  const R ca = h * R(0.5f) * inv_spacing(g, b);
-  const R cb = h * R(0.5f) * inv_spacing(g, a);
-  return ca * (la_below - la_here) - cb * (lb_below - lb_here);
-}
-
-// Adjoint of the flux F_a(B_b) at the cell's lower a-face.
-template <class R>
-NMHD_HD R ct_flux_adj(const GGrid<R> &g, const R *win, const R *lamBn, int x, int y, int z, int a, int b, R h) {
-  const size_t N = (size_t)g.n;
-  const R *vb = win + (1 + b) * N;
-  R c0, c1, d0, d1;
-  corner_weights(g, vb, x, y, z, a, b, c0, c1);
-  const int xb = x + (b == 0), yb = y + (b == 1), zb = z + (b == 2);
-  corner_weights(g, vb, xb, yb, zb, a, b, d0, d1);
-  return c1 * corner_adj(g, lamBn, x, y, z, a, b, h) + d0 * corner_adj(g, lamBn, xb, yb, zb, a, b, h);
-}
+// Periodic neighbour offsets of one cell, computed once per thread: the
+// address of (x+i, y+j, z+k), |i|, |j|, |k| <= 3, is o + d[0][i+3] + d[1][j+3]
+// + d[2][k+3] (the axes wrap independently, so displacements along different
+// axes add).  With the axis a template parameter the table stays in registers.
+struct Nbr {
+  int o;
+  int d[3][7];
+};
 
 template <class R>
-NMHD_HD void a_flux_cell(const GGrid<R> &g, const R *win, const R *lamBn, const R *lamU, R *face, int x, int y,
-                         int z, R h) {
-  const size_t N = (size_t)g.n;
-  const int o = cell_at(g, x, y, z);
-  for (int ax = 0; ax < 3; ++ax) {
-    const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
-    const int om = shifted(g, x, y, z, ax, -1);
-    const R c = h * inv_spacing(g, ax);
-    R lfa[5];
-    for (int k = 0; k < 5; ++k) lfa[k] = c * (lamU[k * N + o] - lamU[k * N + om]);
-    R lf[7];
-    lf[0] = lfa[0];
-    lf[1] = lfa[1 + ax];
-    lf[2] = lfa[1 + e1];
-    lf[3] = lfa[1 + e2];
-    lf[4] = lfa[4];
-    lf[5] = ct_flux_adj(g, win, lamBn, x, y, z, ax, e1, h);
-    lf[6] = ct_flux_adj(g, win, lamBn, x, y, z, ax, e2, h);
-    HState<R> in;
-    R bn;
-    face_input(g, win, x, y, z, ax, h, in, bn);
-    HState<R> ls;
-    R lbn;
-    hlld_adjoint(g.gamma, bn, in, lf, ls, lbn);
-    R *fo = face + (size_t)(15 * ax) * N + o;
-    fo[0] = ls.dl; fo[N] = ls.dr; fo[2 * N] = ls.ul; fo[3 * N] = ls.ur;
-    fo[4 * N] = ls.vl; fo[5 * N] = ls.vr; fo[6 * N] = ls.wl; fo[7 * N] = ls.wr;
-    fo[8 * N] = ls.pl; fo[9 * N] = ls.pr; fo[10 * N] = ls.byl; fo[11 * N] = ls.byr;
-    fo[12 * N] = ls.bzl; fo[13 * N] = ls.bzr; fo[14 * N] = lbn;
+NMHD_HD Nbr make_nbr(const GGrid<R> &g, int x, int y, int z) {
+  Nbr n;
+  n.o = (z * g.sy + y) * g.sx + x;
+  const int sxy = g.sx * g.sy;
+#pragma unroll
+  for (int k = -3; k <= 3; ++k) {
+    n.d[0][k + 3] = wrapc(x + k, g.sx) - x;
+    n.d[1][k + 3] = (wrapc(y + k, g.sy) - y) * g.sx;
+    n.d[2][k + 3] = (wrapc(z + k, g.sz) - z) * sxy;
   }
+  return n;
+}
+
+// face_input for the lower AX-face, addresses from the offset table (the same
+// arithmetic as face_input).
+template <int AX, class T, class R>
+NMHD_HD void face_input_nb(const GGrid<R> &g, const T *w, const Nbr &nb, int y, const T &h, HState<T> &in,
+                           T &bn) {
+  constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
+  const size_t N = (size_t)g.n;
+  int c[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) c[t] = nb.o + nb.d[AX][t + 1];
+  const int t1 = nb.d[E1][4], t2 = nb.d[E2][4];
+  const T *rho = w, *p = w + 4 * N;
+  const T *vn = w + (1 + AX) * N, *v1 = w + (1 + E1) * N, *v2 = w + (1 + E2) * N;
+  const T *b1 = w + (5 + E1) * N, *b2 = w + (5 + E2) * N;
+  T bc1[4], bc2[4];
+#pragma unroll
+  for (int t = 0; t < 4; ++t) {
+    bc1[t] = to<T>(0.5f) * (b1[c[t]] + b1[c[t] + t1]);
+    bc2[t] = to<T>(0.5f) * (b2[c[t]] + b2[c[t] + t2]);
+  }
+  if (g.order2) {
+    reconstruct4_g(rho[c[0]], rho[c[1]], rho[c[2]], rho[c[3]], in.dl, in.dr);
+    reconstruct4_g(vn[c[0]], vn[c[1]], vn[c[2]], vn[c[3]], in.ul, in.ur);
+    reconstruct4_g(v1[c[0]], v1[c[1]], v1[c[2]], v1[c[3]], in.vl, in.vr);
+    reconstruct4_g(v2[c[0]], v2[c[1]], v2[c[2]], v2[c[3]], in.wl, in.wr);
+    reconstruct4_g(p[c[0]], p[c[1]], p[c[2]], p[c[3]], in.pl, in.pr);
+    reconstruct4_g(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
+    reconstruct4_g(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
+  } else {
+    in.dl = rho[c[1]]; in.dr = rho[c[2]];
+    in.ul = vn[c[1]]; in.ur = vn[c[2]];
+    in.vl = v1[c[1]]; in.vr = v1[c[2]];
+    in.wl = v2[c[1]]; in.wr = v2[c[2]];
+    in.pl = p[c[1]]; in.pr = p[c[2]];
+    in.byl = bc1[1]; in.byr = bc1[2];
+    in.bzl = bc2[1]; in.bzr = bc2[2];
+  }
+  if (g.shear) {
+    T acc;
+    if (AX == 0) {
+      const T vY = to<T>(0.5f) * (w[2 * N + c[1]] + w[2 * N + c[2]]);
+      acc = to<T>(-2.0f) * to<T>(g.omega) * vY;
+    } else if (AX == 1) {
+      const T vX = to<T>(0.5f) * (w[N + c[1]] + w[N + c[2]]);
+      acc = to<T>(2.0f) * to<T>(g.omega) * vX +
+            to<T>(R(2.0f) * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((R)y + R(0.5f))));
+    } else {
+      acc = to<T>(R(0));
+    }
+    const T mbv = to<T>(0.5f) * h * acc;
+    in.ul = in.ul + mbv;
+    in.ur = in.ur + mbv;
+  }
+  bn = w[(5 + AX) * N + c[2]];
+}
+
+// Adjoint of the flux F_A(B_B) at the cell's lower A-face: the CT transpose.
+// The corner value C = F_A(B_B) at an edge e is F[e - B] (4-cell wind sum of
+// v_B > 0), F[e] (< 0) or their mean; it enters the face-B updates as
+//   dB_A[o] = +h/2 (C[o+B] - C[o]) / d_B,   dB_B[o] = -h/2 (C[o+A] - C[o]) / d_A
+// in every family (XY, YX, XZ, ZX, YZ, ZY).  F at the cell's face enters the
+// corners at the cell's edge (as F[e]) and one step up B (as F[e - B]).
+template <int A, int B, class R>
+NMHD_HD R ct_flux_adj_nb(const GGrid<R> &g, const R *win, const R *lamBn, const Nbr &nb, R h) {
+  const size_t N = (size_t)g.n;
+  const R *vb = win + (1 + B) * N;
+  const R *lA = lamBn + A * N, *lB = lamBn + B * N;
+  const R ca = h * R(0.5f) * inv_spacing(g, B);
+  const R cb = h * R(0.5f) * inv_spacing(g, A);
+  R acc = R(0);
+#pragma unroll
+  for (int db = 0; db < 2; ++db) {  // edge at displacement db along B (0 or +1)
+    const int e = nb.o + nb.d[B][db + 3];
+    const int eb = nb.o + nb.d[B][db + 2];
+    const int ea = nb.o + nb.d[A][2] + nb.d[B][db + 3];
+    const int eab = nb.o + nb.d[A][2] + nb.d[B][db + 2];
+    const R wind = vb[e] + vb[eb] + vb[ea] + vb[eab];
+    // weight of this face's F in the corner: F[e] for db = 0, F[e - B] for db = 1
+    const R wgt = db == 0 ? (wind > R(0) ? R(0) : (wind < R(0) ? R(1) : R(0.5f)))
+                          : (wind > R(0) ? R(1) : (wind < R(0) ? R(0) : R(0.5f)));
+    const R lam_c = ca * (lA[eb] - lA[e]) - cb * (lB[ea] - lB[e]);
+    acc += wgt * lam_c;
+  }
+  return acc;
+}
+
+// Adjoint of the lower AX-face flux of the cell: flux-divergence and CT
+// transposes give the adjoint of its 7 fluxes, the HLLD adjoint that of the
+// Riemann input, stored at face + (15*AX + k)*N.
+template <int AX, class R>
+NMHD_HD void a_flux_face(const GGrid<R> &g, const R *win, const R *lamBn, const R *lamU, R *face, int x, int y,
+                         int z, R h) {
+  constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
+  const size_t N = (size_t)g.n;
+  const Nbr nb = make_nbr(g, x, y, z);
+  const int o = nb.o, om = o + nb.d[AX][2];
+  const R c = h * inv_spacing(g, AX);
+  R lfa[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) lfa[k] = c * (lamU[k * N + o] - lamU[k * N + om]);
+  R lf[7];
+  lf[0] = lfa[0];
+  lf[1] = lfa[1 + AX];
+  lf[2] = lfa[1 + E1];
+  lf[3] = lfa[1 + E2];
+  lf[4] = lfa[4];
+  lf[5] = ct_flux_adj_nb<AX, E1>(g, win, lamBn, nb, h);
+  lf[6] = ct_flux_adj_nb<AX, E2>(g, win, lamBn, nb, h);
+  HState<R> in;
+  R bn;
+  face_input_nb<AX>(g, win, nb, y, h, in, bn);
+  HState<R> ls;
+  R lbn;
+  hlld_adjoint(g.gamma, bn, in, lf, ls, lbn);
+  R *fo = face + (size_t)(15 * AX) * N + o;
+  fo[0] = ls.dl; fo[N] = ls.dr; fo[2 * N] = ls.ul; fo[3 * N] = ls.ur;
+  fo[4 * N] = ls.vl; fo[5 * N] = ls.vr; fo[6 * N] = ls.wl; fo[7 * N] = ls.wr;
+  fo[8 * N] = ls.pl; fo[9 * N] = ls.pr; fo[10 * N] = ls.byl; fo[11 * N] = ls.byr;
+  fo[12 * N] = ls.bzl; fo[13 * N] = ls.bzr; fo[14 * N] = lbn;
 }
 
 // Minbee choice of absolute_smaller(a, b): 0 -> zero slope, 1 -> a, 2 -> b.
@@ -497,13 +571,14 @@ NMHD_HD int mm_choice(R a, R b) {
   return a * b <= R(0) ? 0 : (gabs(a) < gabs(b) ? 1 : 2);
 }
 
-// Transpose of the reconstruction of one variable q along axis ax at cell c:
+// Transpose of the reconstruction of one variable q along an axis at cell c:
 // q7[k] = q at c + k - 3; lamL[j], lamR[j] = adjoints of the left / right
 // states of face c + j - 1 (j = 0..3).  Returns the adjoint of q[c].
 template <class R>
 NMHD_HD R recon_adj(int order2, const R q7[7], const R lamL[4], const R lamR[4]) {
   if (!order2) return lamL[2] + lamR[1];  // left of face c+1, right of face c
   R acc = R(0);
+#pragma unroll
   for (int j = 0; j < 4; ++j) {
     // face f = c + j - 1 uses x0..x3 = q[f-2..f+1] = q7[j..j+3]; c is x_(3-j)
     const R x0 = q7[j], x1 = q7[j + 1], x2 = q7[j + 2], x3 = q7[j + 3];
@@ -524,58 +599,63 @@ NMHD_HD R recon_adj(int order2, const R q7[7], const R lamL[4], const R lamR[4])
   return acc;
 }
 
-template <class R>
-NMHD_HD void a_recon_cell(const GGrid<R> &g, const R *win, const R *face, R *lin, R *lamBc, int x, int y, int z,
+// Transposes of the AX-face reconstruction at cell (x, y, z): the cell's
+// primitives (into lin), its cell-centred transverse B averages (into lamBc),
+// the face half-kick and the normal field of its lower AX-face.  Called for
+// AX = 0, 1, 2 in turn; lin and lamBc accumulate.
+template <int AX, class R>
+NMHD_HD void a_recon_face(const GGrid<R> &g, const R *win, const R *face, R *lin, R *lamBc, int x, int y, int z,
                           R h) {
+  constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
   const size_t N = (size_t)g.n;
-  const int o = cell_at(g, x, y, z);
-  R lcell[5] = {R(0), R(0), R(0), R(0), R(0)};  // rho, vx, vy, vz, p
-  R lbc[3] = {R(0), R(0), R(0)};
-  for (int ax = 0; ax < 3; ++ax) {
-    const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
-    int c7[7];
-    for (int k = 0; k < 7; ++k) c7[k] = shifted(g, x, y, z, ax, k - 3);
-    int f4[4];  // faces c-1 .. c+2
-    for (int j = 0; j < 4; ++j) f4[j] = c7[j + 2];
-    const R *fa = face + (size_t)(15 * ax) * N;
-    // cell variables: rho, v_n, v_t1, v_t2, p
-    const int var[5] = {0, 1 + ax, 1 + e1, 1 + e2, 4};
-    for (int k = 0; k < 5; ++k) {
-      R q7[7], lL[4], lR[4];
-      for (int m = 0; m < 7; ++m) q7[m] = win[var[k] * N + c7[m]];
-      for (int j = 0; j < 4; ++j) {
-        lL[j] = fa[(2 * k) * N + f4[j]];
-        lR[j] = fa[(2 * k + 1) * N + f4[j]];
-      }
-      lcell[var[k]] += recon_adj(g.order2, q7, lL, lR);
+  const Nbr nb = make_nbr(g, x, y, z);
+  const int o = nb.o;
+  int c7[7];
+#pragma unroll
+  for (int k = 0; k < 7; ++k) c7[k] = o + nb.d[AX][k];
+  const R *fa = face + (size_t)(15 * AX) * N;
+  const int var[5] = {0, 1 + AX, 1 + E1, 1 + E2, 4};
+  R lcell[5];
+#pragma unroll
+  for (int k = 0; k < 5; ++k) {
+    R q7[7], lL[4], lR[4];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) q7[m] = win[var[k] * N + c7[m]];
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      lL[j] = fa[(2 * k) * N + c7[j + 2]];
+      lR[j] = fa[(2 * k + 1) * N + c7[j + 2]];
     }
-    // transverse B averages (components e1, e2)
-    for (int k = 0; k < 2; ++k) {
-      const int comp = k == 0 ? e1 : e2;
-      const R *b = win + (5 + comp) * N;
-      R q7[7], lL[4], lR[4];
-      for (int m = 0; m < 7; ++m) {
-        const int cx = x + (ax == 0 ? m - 3 : 0), cy = y + (ax == 1 ? m - 3 : 0), cz = z + (ax == 2 ? m - 3 : 0);
-        q7[m] = R(0.5f) * (b[c7[m]] + b[shifted(g, cx, cy, cz, comp, 1)]);
-      }
-      for (int j = 0; j < 4; ++j) {
-        lL[j] = fa[(10 + 2 * k) * N + f4[j]];
-        lR[j] = fa[(11 + 2 * k) * N + f4[j]];
-      }
-      lbc[comp] += recon_adj(g.order2, q7, lL, lR);
-    }
-    // face half-kick: mbv(f) = h/2 * acc(f), acc from the two cells of face f
-    if (g.shear && ax < 2) {
-      const R lm = (fa[2 * N + o] + fa[3 * N + o]) + (fa[2 * N + f4[2]] + fa[3 * N + f4[2]]);
-      // faces c (f4[1] = o) and c+1 (f4[2]); d acc / d v = -2 omega / 2 (ax 0, v_y) or +2 omega / 2 (ax 1, v_x)
-      const R c = R(0.5f) * h * (ax == 0 ? -g.omega : g.omega);
-      lcell[ax == 0 ? 2 : 1] += c * lm;
-    }
-    // normal field of face c
-    lin[(5 + ax) * N + o] += fa[14 * N + o];
+    lcell[k] = recon_adj(g.order2, q7, lL, lR);
   }
-  for (int v = 0; v < 5; ++v) lin[v * N + o] += lcell[v];
-  for (int c = 0; c < 3; ++c) lamBc[c * N + o] = lbc[c];
+  // face half-kick: mbv(f) = h/2 * acc(f), acc from the two cells of face f;
+  // cell c takes part in faces c and c + 1.  d acc / d v = -omega per cell on
+  // v_y for AX 0 (slot v_E1) and +omega on v_x for AX 1 (slot v_E2).
+  if (g.shear && AX < 2) {
+    const R lm = (fa[2 * N + o] + fa[3 * N + o]) + (fa[2 * N + c7[4]] + fa[3 * N + c7[4]]);
+    const R c = R(0.5f) * h * (AX == 0 ? -g.omega : g.omega);
+    lcell[AX == 0 ? 2 : 3] += c * lm;
+  }
+#pragma unroll
+  for (int k = 0; k < 5; ++k) lin[var[k] * N + o] += lcell[k];
+  // transverse B averages (components E1, E2)
+#pragma unroll
+  for (int k = 0; k < 2; ++k) {
+    const int comp = k == 0 ? E1 : E2;
+    const int tp = k == 0 ? nb.d[E1][4] : nb.d[E2][4];
+    const R *b = win + (5 + comp) * N;
+    R q7[7], lL[4], lR[4];
+#pragma unroll
+    for (int m = 0; m < 7; ++m) q7[m] = R(0.5f) * (b[c7[m]] + b[c7[m] + tp]);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+      lL[j] = fa[(10 + 2 * k) * N + c7[j + 2]];
+      lR[j] = fa[(11 + 2 * k) * N + c7[j + 2]];
+    }
+    lamBc[comp * N + o] += recon_adj(g.order2, q7, lL, lR);
+  }
+  // normal field of face c
+  lin[(5 + AX) * N + o] += fa[14 * N + o];
 }
 
 template <class R>

@@ -160,21 +160,21 @@ struct OpABface {
   R *lamBn, *lb;
   NMHD_HD void operator()(int x, int y, int z) const { a_bface_cell(g, wb, wo, lout, lamU, lamE, lamBn, lb, x, y, z); }
 };
-template <class R>
+template <class R, int AX>
 struct OpAFlux {
   GGrid<R> g;
   const R *win, *lamBn, *lamU;
   R *face;
   R h;
-  NMHD_HD void operator()(int x, int y, int z) const { a_flux_cell(g, win, lamBn, lamU, face, x, y, z, h); }
+  NMHD_HD void operator()(int x, int y, int z) const { a_flux_face<AX>(g, win, lamBn, lamU, face, x, y, z, h); }
 };
-template <class R>
+template <class R, int AX>
 struct OpARecon {
   GGrid<R> g;
   const R *win, *face;
   R *lin, *lamBc;
   R h;
-  NMHD_HD void operator()(int x, int y, int z) const { a_recon_cell(g, win, face, lin, lamBc, x, y, z, h); }
+  NMHD_HD void operator()(int x, int y, int z) const { a_recon_face<AX>(g, win, face, lin, lamBc, x, y, z, h); }
 };
 template <class R>
 struct OpABc {
@@ -240,8 +240,13 @@ void adj_stage(Ex &ex, const GGrid<R> &g, const R *win, const R *wb, const R *wo
                const R *lout, R *lin, R *lb, const AdjScratch<R> &sc) {
   ex.cells(g, OpAPrim<R>{g, wb, flux, lout, sc.lamU, sc.lamE, lb, h});
   ex.cells(g, OpABface<R>{g, wb, wo, lout, sc.lamU, sc.lamE, sc.lamBn, lb});
-  ex.cells(g, OpAFlux<R>{g, win, sc.lamBn, sc.lamU, sc.face, h});
-  ex.cells(g, OpARecon<R>{g, win, sc.face, lin, sc.lamBc, h});
+  ex.cells(g, OpAFlux<R, 0>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.cells(g, OpAFlux<R, 1>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.cells(g, OpAFlux<R, 2>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.zero(sc.lamBc, (size_t)3 * g.n);
+  ex.cells(g, OpARecon<R, 0>{g, win, sc.face, lin, sc.lamBc, h});
+  ex.cells(g, OpARecon<R, 1>{g, win, sc.face, lin, sc.lamBc, h});
+  ex.cells(g, OpARecon<R, 2>{g, win, sc.face, lin, sc.lamBc, h});
   ex.cells(g, OpABc<R>{g, sc.lamBc, lin});
 }
 

@@ -39,8 +39,8 @@ template <class F>
 struct MinBlocks {
   static constexpr int value = 1;
 };
-template <>
-struct MinBlocks<OpAFlux<float>> {
+template <int AX>
+struct MinBlocks<OpAFlux<float, AX>> {
   static constexpr int value = 2;
 };
 
