@@ -349,9 +349,11 @@ NMHD_HD typename Wide64<T>::type g_stress_cell(const GGrid<R> &g, const T *w, in
 //         before it;
 //   lamE  1 field: adjoint of the internal energy;
 //   lamBn 3 fields: adjoint of the new face B (x, y, z);
-//   face  45 fields: per axis ax, 15 values at face + (15*ax + k)*N: the
-//         adjoints of the Riemann input (dl, dr, ul, ur, vl, vr, wl, wr, pl,
-//         pr, byl, byr, bzl, bzr) and of the normal face B;
+//   face  30 fields, one face axis at a time: for the 7 reconstructed
+//         variables (rho, v_n, v_t1, v_t2, p, B_t1, B_t2 averages) the
+//         contributions to the 4 cells the face's reconstruction reads
+//         (4*v + k: cell face - 2 + k), then the half-kick (28) and the normal
+//         face field (29);
 //   lamBc 3 fields: adjoint of the cell-centred transverse B averages.
 
 template <class R>
@@ -361,12 +363,14 @@ NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R 
   const int o = cell_at(g, x, y, z);
   const int oxp = cell_at(g, x + 1, y, z), oyp = cell_at(g, x, y + 1, z), ozp = cell_at(g, x, y, z + 1);
   const R *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
+  // the linearisation point: the updated conserved state (inverse spacings:
+  // the adjoint needs no correctly rounded quotients)
   R pace[4];
   for (int v = 0; v < 4; ++v) {
     R pc = R(0);
-    pc = pc + (Fx[v * N + o] - Fx[v * N + oxp]) / g.dx;
-    pc = pc + (Fy[v * N + o] - Fy[v * N + oyp]) / g.dy;
-    pc = pc + (Fz[v * N + o] - Fz[v * N + ozp]) / g.dz;
+    pc = pc + (Fx[v * N + o] - Fx[v * N + oxp]) * g.idx;
+    pc = pc + (Fy[v * N + o] - Fy[v * N + oyp]) * g.idy;
+    pc = pc + (Fz[v * N + o] - Fz[v * N + ozp]) * g.idz;
     pace[v] = pc;
   }
   const R gm1 = g.gamma - R(1.0f);
@@ -386,12 +390,12 @@ NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R 
     l_vy = ly;
   }
   const R l_eint = gm1 * lout[4 * N + o];
-  const R r2 = rho * rho;
-  const R l_mx = l_vx / rho - l_eint * mx / rho;
-  const R l_my = l_vy / rho - l_eint * my / rho;
-  const R l_mz = l_vz / rho - l_eint * mz / rho;
-  const R l_rho = lout[o] - (l_vx * mx + l_vy * my + l_vz * mz) / r2 +
-                  l_eint * R(0.5f) * (mx * mx + my * my + mz * mz) / r2;
+  const R ir = R(1) / rho;
+  const R l_mx = (l_vx - l_eint * mx) * ir;
+  const R l_my = (l_vy - l_eint * my) * ir;
+  const R l_mz = (l_vz - l_eint * mz) * ir;
+  const R l_rho = lout[o] + (l_eint * R(0.5f) * (mx * mx + my * my + mz * mz) -
+                             (l_vx * mx + l_vy * my + l_vz * mz)) * (ir * ir);
   const R l_ene = l_eint;
   lamU[o] = l_rho;
   lamU[N + o] = l_mx;
@@ -404,7 +408,7 @@ NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R 
   lb[N + o] += (l_mx + l_ene * vx0) * rho0;
   lb[2 * N + o] += (l_my + l_ene * vy0) * rho0;
   lb[3 * N + o] += (l_mz + l_ene * vz0) * rho0;
-  lb[4 * N + o] += l_ene / gm1;
+  lb[4 * N + o] += l_ene * (R(1) / gm1);
 }
 
 template <class R>
@@ -446,9 +450,19 @@ NMHD_HD Nbr make_nbr(const GGrid<R> &g, int x, int y, int z) {
 
 // face_input for the lower AX-face, addresses from the offset table (the same
 // arithmetic as face_input).
+// Minbee choices of one reconstruction (same operations as reconstruct4_g),
+// packed as cl | cr << 2 (0: zero slope, 1: first difference, 2: second).
+template <class R>
+NMHD_HD unsigned mm_choices(R x0, R x1, R x2, R x3) {
+  const R d01 = x1 - x0, d12 = x2 - x1, d23 = x3 - x2;
+  const unsigned cl = d01 * d12 <= R(0) ? 0u : (gabs(d01) < gabs(d12) ? 1u : 2u);
+  const unsigned cr = d12 * d23 <= R(0) ? 0u : (gabs(d12) < gabs(d23) ? 1u : 2u);
+  return cl | (cr << 2);
+}
+
 template <int AX, class T, class R>
 NMHD_HD void face_input_nb(const GGrid<R> &g, const T *w, const Nbr &nb, int y, const T &h, HState<T> &in,
-                           T &bn) {
+                           T &bn, unsigned *choices = nullptr) {
   constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
   const size_t N = (size_t)g.n;
   int c[4];
@@ -472,6 +486,15 @@ NMHD_HD void face_input_nb(const GGrid<R> &g, const T *w, const Nbr &nb, int y, 
     reconstruct4_g(p[c[0]], p[c[1]], p[c[2]], p[c[3]], in.pl, in.pr);
     reconstruct4_g(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
     reconstruct4_g(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
+    if (choices) {
+      *choices = mm_choices(val(rho[c[0]]), val(rho[c[1]]), val(rho[c[2]]), val(rho[c[3]])) |
+                 mm_choices(val(vn[c[0]]), val(vn[c[1]]), val(vn[c[2]]), val(vn[c[3]])) << 4 |
+                 mm_choices(val(v1[c[0]]), val(v1[c[1]]), val(v1[c[2]]), val(v1[c[3]])) << 8 |
+                 mm_choices(val(v2[c[0]]), val(v2[c[1]]), val(v2[c[2]]), val(v2[c[3]])) << 12 |
+                 mm_choices(val(p[c[0]]), val(p[c[1]]), val(p[c[2]]), val(p[c[3]])) << 16 |
+                 mm_choices(val(bc1[0]), val(bc1[1]), val(bc1[2]), val(bc1[3])) << 20 |
+                 mm_choices(val(bc2[0]), val(bc2[1]), val(bc2[2]), val(bc2[3])) << 24;
+    }
   } else {
     in.dl = rho[c[1]]; in.dr = rho[c[2]];
     in.ul = vn[c[1]]; in.ur = vn[c[2]];
@@ -480,6 +503,7 @@ NMHD_HD void face_input_nb(const GGrid<R> &g, const T *w, const Nbr &nb, int y, 
     in.pl = p[c[1]]; in.pr = p[c[2]];
     in.byl = bc1[1]; in.byr = bc1[2];
     in.bzl = bc2[1]; in.bzr = bc2[2];
+    if (choices) *choices = 0u;  // left = x1, right = x2: the zero-slope weights
   }
   if (g.shear) {
     T acc;
@@ -554,108 +578,75 @@ NMHD_HD void a_flux_face(const GGrid<R> &g, const R *win, const R *lamBn, const 
   lf[6] = ct_flux_adj_nb<AX, E2>(g, win, lamBn, nb, h);
   HState<R> in;
   R bn;
-  face_input_nb<AX>(g, win, nb, y, h, in, bn);
+  unsigned ch;
+  face_input_nb<AX>(g, win, nb, y, h, in, bn, &ch);
   HState<R> ls;
   R lbn;
   hlld_adjoint(g.gamma, bn, in, lf, ls, lbn);
-  R *fo = face + (size_t)(15 * AX) * N + o;
-  fo[0] = ls.dl; fo[N] = ls.dr; fo[2 * N] = ls.ul; fo[3 * N] = ls.ur;
-  fo[4 * N] = ls.vl; fo[5 * N] = ls.vr; fo[6 * N] = ls.wl; fo[7 * N] = ls.wr;
-  fo[8 * N] = ls.pl; fo[9 * N] = ls.pr; fo[10 * N] = ls.byl; fo[11 * N] = ls.byr;
-  fo[12 * N] = ls.bzl; fo[13 * N] = ls.bzr; fo[14 * N] = lbn;
-}
-
-// Minbee choice of absolute_smaller(a, b): 0 -> zero slope, 1 -> a, 2 -> b.
-template <class R>
-NMHD_HD int mm_choice(R a, R b) {
-  return a * b <= R(0) ? 0 : (gabs(a) < gabs(b) ? 1 : 2);
-}
-
-// Transpose of the reconstruction of one variable q along an axis at cell c:
-// q7[k] = q at c + k - 3; lamL[j], lamR[j] = adjoints of the left / right
-// states of face c + j - 1 (j = 0..3).  Returns the adjoint of q[c].
-template <class R>
-NMHD_HD R recon_adj(int order2, const R q7[7], const R lamL[4], const R lamR[4]) {
-  if (!order2) return lamL[2] + lamR[1];  // left of face c+1, right of face c
-  R acc = R(0);
+  // Transpose of the reconstruction of each variable at this face, split by
+  // the four cells x0..x3 (= face - 2 .. face + 1 along AX) it reads:
+  // left = x1 + d1/2 with d1 = 0 | x1 - x0 | x2 - x1, right = x2 - d2/2 with
+  // d2 = 0 | x2 - x1 | x3 - x2 (the choice frozen at the forward's).
+  const R lL[7] = {ls.dl, ls.ul, ls.vl, ls.wl, ls.pl, ls.byl, ls.bzl};
+  const R lR[7] = {ls.dr, ls.ur, ls.vr, ls.wr, ls.pr, ls.byr, ls.bzr};
+  R *fo = face + o;
 #pragma unroll
-  for (int j = 0; j < 4; ++j) {
-    // face f = c + j - 1 uses x0..x3 = q[f-2..f+1] = q7[j..j+3]; c is x_(3-j)
-    const R x0 = q7[j], x1 = q7[j + 1], x2 = q7[j + 2], x3 = q7[j + 3];
-    const int cl = mm_choice(x1 - x0, x2 - x1);
-    const int cr = mm_choice(x2 - x1, x3 - x2);
-    const int t = 3 - j;
-    R dl, dr;
-    // left = x1 + d1/2: d1 = 0 | x1 - x0 | x2 - x1
-    if (cl == 0) dl = (t == 1) ? R(1) : R(0);
-    else if (cl == 1) dl = (t == 0) ? R(-0.5f) : ((t == 1) ? R(1.5f) : R(0));
-    else dl = (t == 1 || t == 2) ? R(0.5f) : R(0);
-    // right = x2 - d2/2: d2 = 0 | x2 - x1 | x3 - x2
-    if (cr == 0) dr = (t == 2) ? R(1) : R(0);
-    else if (cr == 1) dr = (t == 1 || t == 2) ? R(0.5f) : R(0);
-    else dr = (t == 2) ? R(1.5f) : ((t == 3) ? R(-0.5f) : R(0));
-    acc += lamL[j] * dl + lamR[j] * dr;
+  for (int v = 0; v < 7; ++v) {
+    const unsigned cl = (ch >> (4 * v)) & 3u, cr = (ch >> (4 * v + 2)) & 3u;
+    const R a = lL[v], b = lR[v];
+    R t0 = R(0), t1 = R(0), t2 = R(0), t3 = R(0);
+    if (cl == 0u) { t1 += a; }
+    else if (cl == 1u) { t0 -= R(0.5f) * a; t1 += R(1.5f) * a; }
+    else { t1 += R(0.5f) * a; t2 += R(0.5f) * a; }
+    if (cr == 0u) { t2 += b; }
+    else if (cr == 1u) { t1 += R(0.5f) * b; t2 += R(0.5f) * b; }
+    else { t2 += R(1.5f) * b; t3 -= R(0.5f) * b; }
+    fo[(4 * v) * N] = t0;
+    fo[(4 * v + 1) * N] = t1;
+    fo[(4 * v + 2) * N] = t2;
+    fo[(4 * v + 3) * N] = t3;
   }
-  return acc;
+  fo[28 * N] = ls.ul + ls.ur;  // adjoint of the face half-kick
+  fo[29 * N] = lbn;            // adjoint of the normal face field
 }
 
-// Transposes of the AX-face reconstruction at cell (x, y, z): the cell's
-// primitives (into lin), its cell-centred transverse B averages (into lamBc),
-// the face half-kick and the normal field of its lower AX-face.  Called for
-// AX = 0, 1, 2 in turn; lin and lamBc accumulate.
+// Gather of the AX-face reconstruction transposes at cell c: each variable of
+// the cell receives the contributions of faces c + 2, c + 1, c, c - 1 (where
+// it is x0, x1, x2, x3), written by a_flux_face for this axis; the cell-centred
+// transverse B averages go to lamBc, the face half-kick to v_y (AX 0) or v_x
+// (AX 1), the normal field of face c to B_AX.  Called for AX = 0, 1, 2 in
+// turn, each after a_flux_face of the same axis; lin and lamBc accumulate.
 template <int AX, class R>
-NMHD_HD void a_recon_face(const GGrid<R> &g, const R *win, const R *face, R *lin, R *lamBc, int x, int y, int z,
-                          R h) {
+NMHD_HD void a_recon_face(const GGrid<R> &g, const R *face, R *lin, R *lamBc, int x, int y, int z, R h) {
   constexpr int E1 = (AX + 1) % 3, E2 = (AX + 2) % 3;
   const size_t N = (size_t)g.n;
   const Nbr nb = make_nbr(g, x, y, z);
   const int o = nb.o;
-  int c7[7];
+  int f[4];  // face of which this cell is x_k
 #pragma unroll
-  for (int k = 0; k < 7; ++k) c7[k] = o + nb.d[AX][k];
-  const R *fa = face + (size_t)(15 * AX) * N;
-  const int var[5] = {0, 1 + AX, 1 + E1, 1 + E2, 4};
-  R lcell[5];
+  for (int k = 0; k < 4; ++k) f[k] = o + nb.d[AX][5 - k];
+  R lv[7];
 #pragma unroll
-  for (int k = 0; k < 5; ++k) {
-    R q7[7], lL[4], lR[4];
+  for (int v = 0; v < 7; ++v) {
+    R acc = R(0);
 #pragma unroll
-    for (int m = 0; m < 7; ++m) q7[m] = win[var[k] * N + c7[m]];
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      lL[j] = fa[(2 * k) * N + c7[j + 2]];
-      lR[j] = fa[(2 * k + 1) * N + c7[j + 2]];
-    }
-    lcell[k] = recon_adj(g.order2, q7, lL, lR);
+    for (int k = 0; k < 4; ++k) acc += face[(4 * v + k) * N + f[k]];
+    lv[v] = acc;
   }
-  // face half-kick: mbv(f) = h/2 * acc(f), acc from the two cells of face f;
-  // cell c takes part in faces c and c + 1.  d acc / d v = -omega per cell on
-  // v_y for AX 0 (slot v_E1) and +omega on v_x for AX 1 (slot v_E2).
   if (g.shear && AX < 2) {
-    const R lm = (fa[2 * N + o] + fa[3 * N + o]) + (fa[2 * N + c7[4]] + fa[3 * N + c7[4]]);
-    const R c = R(0.5f) * h * (AX == 0 ? -g.omega : g.omega);
-    lcell[AX == 0 ? 2 : 3] += c * lm;
+    // mbv(f) = h/2 * acc(f); acc takes the mean of the two cells of face f,
+    // d acc / d v = -2 omega (AX 0, v_y) or +2 omega (AX 1, v_x)
+    const R lm = face[28 * N + o] + face[28 * N + f[1]];
+    lv[AX == 0 ? 2 : 3] += R(0.5f) * h * (AX == 0 ? -g.omega : g.omega) * lm;
   }
-#pragma unroll
-  for (int k = 0; k < 5; ++k) lin[var[k] * N + o] += lcell[k];
-  // transverse B averages (components E1, E2)
-#pragma unroll
-  for (int k = 0; k < 2; ++k) {
-    const int comp = k == 0 ? E1 : E2;
-    const int tp = k == 0 ? nb.d[E1][4] : nb.d[E2][4];
-    const R *b = win + (5 + comp) * N;
-    R q7[7], lL[4], lR[4];
-#pragma unroll
-    for (int m = 0; m < 7; ++m) q7[m] = R(0.5f) * (b[c7[m]] + b[c7[m] + tp]);
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      lL[j] = fa[(10 + 2 * k) * N + c7[j + 2]];
-      lR[j] = fa[(11 + 2 * k) * N + c7[j + 2]];
-    }
-    lamBc[comp * N + o] += recon_adj(g.order2, q7, lL, lR);
-  }
-  // normal field of face c
-  lin[(5 + AX) * N + o] += fa[14 * N + o];
+  lin[o] += lv[0];
+  lin[(1 + AX) * N + o] += lv[1];
+  lin[(1 + E1) * N + o] += lv[2];
+  lin[(1 + E2) * N + o] += lv[3];
+  lin[4 * N + o] += lv[4];
+  lamBc[E1 * N + o] += lv[5];
+  lamBc[E2 * N + o] += lv[6];
+  lin[(5 + AX) * N + o] += face[29 * N + o];
 }
 
 template <class R>
@@ -681,37 +672,35 @@ NMHD_HD void a_fill_z_item(const GGrid<R> &g, R *lam, int idx) {
   }
 }
 
-// Transpose of g_fill_y_item, gathered at the source: item (xs, sy, sz)
-// covers source cells (xs, Sy-2M+sy, sz) (-> bottom margin row sy) and
-// (xs, M+sy, sz) (-> top margin row Sy-M+sy).  Each margin cell is the image
-// of exactly one item, which clears it after reading.
+// Transpose of g_fill_y_item for field v, gathered at the source: item
+// (xs, sy, sz, v) covers source cells (xs, Sy-2M+sy, sz) (-> bottom margin row
+// sy) and (xs, M+sy, sz) (-> top margin row Sy-M+sy).  Each margin cell is the
+// image of exactly one item, which clears it after reading.  dint and f are
+// shear_shift() of the step's time.
 template <class R>
-NMHD_HD void a_fill_y_item(const GGrid<R> &g, double time, R *lam, int idx) {
+NMHD_HD void a_fill_y_item(const GGrid<R> &g, int dint, R f, R *lam, int idx) {
   const int M = g.my;
-  const int xs = idx % g.sx;
-  const int sy = (idx / g.sx) % M;
-  const int sz = idx / (g.sx * M);
-  int dint;
-  R f;
-  shear_shift(g, time, dint, f);
+  const int per_field = g.sx * M * g.sz;
+  const int v = idx / per_field;
+  const int r = idx - v * per_field;
+  const int xs = r % g.sx;
+  const int sy = (r / g.sx) % M;
+  const int sz = r / (g.sx * M);
   const R coef = (R(1.0f) - f) + f;  // d/dv of (1-f) v + f v
   const int sx_lo = wrapc((xs - dint) % g.sx, g.sx);      // (sx_lo + dint) mod Sx = xs
   const int sx_hi = wrapc((xs + dint + 1) % g.sx, g.sx);  // (sx_hi - dint - 1) mod Sx = xs
-  const size_t N = (size_t)g.n;
+  R *var = lam + (size_t)v * g.n;
   const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + xs;
   const int src_dec = (sz * g.sy + (M + sy)) * g.sx + xs;
   const int dst_lo = (sz * g.sy + sy) * g.sx + sx_lo;
   const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx_hi;
-  for (int v = 0; v < 8; ++v) {
-    R *var = lam + v * N;
-    const R llo = var[dst_lo];
-    var[dst_lo] = R(0);
-    var[src_inc] += coef * llo;
-    if (!(v == 6 && sy == 0)) {
-      const R lhi = var[dst_hi];
-      var[dst_hi] = R(0);
-      var[src_dec] += coef * lhi;
-    }
+  const R llo = var[dst_lo];
+  var[dst_lo] = R(0);
+  var[src_inc] += coef * llo;
+  if (!(v == 6 && sy == 0)) {
+    const R lhi = var[dst_hi];
+    var[dst_hi] = R(0);
+    var[src_dec] += coef * lhi;
   }
 }
 

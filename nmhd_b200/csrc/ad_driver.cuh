@@ -20,8 +20,8 @@ namespace ad {
 // Number of fields of one step's tape: filled input (8), stage-1 fluxes (21),
 // predictor (8), stage-2 fluxes (21), raw output (8).
 constexpr int kTapeFields = 66;
-// Scratch fields of the adjoint of a stage: lamU 5, lamE 1, lamBn 3, face 45, lamBc 3.
-constexpr int kAdjScratchFields = 57;
+// Scratch fields of the adjoint of a stage: lamU 5, lamE 1, lamBn 3, face 30, lamBc 3.
+constexpr int kAdjScratchFields = 42;
 
 template <class T>
 struct StepTape {
@@ -51,7 +51,7 @@ AdjScratch<R> scratch_at(R *base, size_t n) {
   s.lamE = base + 5 * n;
   s.lamBn = base + 6 * n;
   s.face = base + 9 * n;
-  s.lamBc = base + 54 * n;
+  s.lamBc = base + 39 * n;
   return s;
 }
 
@@ -171,10 +171,10 @@ struct OpAFlux {
 template <class R, int AX>
 struct OpARecon {
   GGrid<R> g;
-  const R *win, *face;
+  const R *face;
   R *lin, *lamBc;
   R h;
-  NMHD_HD void operator()(int x, int y, int z) const { a_recon_face<AX>(g, win, face, lin, lamBc, x, y, z, h); }
+  NMHD_HD void operator()(int x, int y, int z) const { a_recon_face<AX>(g, face, lin, lamBc, x, y, z, h); }
 };
 template <class R>
 struct OpABc {
@@ -186,9 +186,10 @@ struct OpABc {
 template <class R>
 struct OpAFillY {
   GGrid<R> g;
-  double time;
+  int dint;
+  R f;
   R *lam;
-  NMHD_HD void operator()(int i) const { a_fill_y_item(g, time, lam, i); }
+  NMHD_HD void operator()(int i) const { a_fill_y_item(g, dint, f, lam, i); }
 };
 template <class R>
 struct OpAFillZ {
@@ -240,13 +241,14 @@ void adj_stage(Ex &ex, const GGrid<R> &g, const R *win, const R *wb, const R *wo
                const R *lout, R *lin, R *lb, const AdjScratch<R> &sc) {
   ex.cells(g, OpAPrim<R>{g, wb, flux, lout, sc.lamU, sc.lamE, lb, h});
   ex.cells(g, OpABface<R>{g, wb, wo, lout, sc.lamU, sc.lamE, sc.lamBn, lb});
-  ex.cells(g, OpAFlux<R, 0>{g, win, sc.lamBn, sc.lamU, sc.face, h});
-  ex.cells(g, OpAFlux<R, 1>{g, win, sc.lamBn, sc.lamU, sc.face, h});
-  ex.cells(g, OpAFlux<R, 2>{g, win, sc.lamBn, sc.lamU, sc.face, h});
   ex.zero(sc.lamBc, (size_t)3 * g.n);
-  ex.cells(g, OpARecon<R, 0>{g, win, sc.face, lin, sc.lamBc, h});
-  ex.cells(g, OpARecon<R, 1>{g, win, sc.face, lin, sc.lamBc, h});
-  ex.cells(g, OpARecon<R, 2>{g, win, sc.face, lin, sc.lamBc, h});
+  // one face axis at a time through the shared face scratch
+  ex.cells(g, OpAFlux<R, 0>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.cells(g, OpARecon<R, 0>{g, sc.face, lin, sc.lamBc, h});
+  ex.cells(g, OpAFlux<R, 1>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.cells(g, OpARecon<R, 1>{g, sc.face, lin, sc.lamBc, h});
+  ex.cells(g, OpAFlux<R, 2>{g, win, sc.lamBn, sc.lamU, sc.face, h});
+  ex.cells(g, OpARecon<R, 2>{g, sc.face, lin, sc.lamBc, h});
   ex.cells(g, OpABc<R>{g, sc.lamBc, lin});
 }
 
@@ -267,7 +269,12 @@ void adj_step(Ex &ex, const GGrid<R> &g, int time_order, double time, R dt, cons
   }
   // margin fill: W_f = Fz(Fy(W^n)), so apply Fz^T then Fy^T
   if (g.mz > 0) ex.items(g.sx * g.sy * g.mz, OpAFillZ<R>{g, lam_f});
-  if (g.my > 0) ex.items(g.sx * g.my * g.sz, OpAFillY<R>{g, time, lam_f});
+  if (g.my > 0) {
+    int dint;
+    R f;
+    shear_shift(g, time, dint, f);
+    ex.items(8 * g.sx * g.my * g.sz, OpAFillY<R>{g, dint, f, lam_f});
+  }
 }
 
 // Loss: J = s * sum over the window's states of sum_cells -(Bx By)_centre,

@@ -10,7 +10,8 @@
 //
 // Memory: checkpoints (8 fields) every K steps, plus one segment's tape (66
 // fields per step: filled input, predictor, raw output, both stages' fluxes),
-// plus 3 adjoint states and 57 scratch fields.
+// plus 3 adjoint states and 42 scratch fields.  The forward run keeps the
+// last segment on the tape, so only the earlier segments are recomputed.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -346,18 +347,29 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   }
   std::vector<double> tn(nsteps + 1);
   tn[0] = t0;
+  // the last segment's steps are kept on the tape: the reverse sweep starts
+  // there without recomputing it
+  const int kept0 = want_grad ? (nseg - 1) * K : nsteps;
   for (int i = 0; i < nsteps; ++i) {
     if (want_grad && i % K == 0)
       AD_CUDA(cudaMemcpyAsync(ckpt + (size_t)(i / K) * 8 * n, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     StepTape<R> t = {A, t0tape.f1, t0tape.ws, t0tape.f2, B};
+    if (i >= kept0) {
+      t = tape_at(tape + (size_t)(i - kept0) * kTapeFields * n, n);
+      if (t.wf != A) AD_CUDA(cudaMemcpyAsync(t.wf, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+    }
     if constexpr (Prec<R>::kProduction) {
       prod_step(s, w, t, !frozen);
     } else {
       tn[i + 1] = tn[i] + (double)dts[i];
       fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
     }
-    if (in_window(L, i + 1)) ex.reduce(gg, OpStress<R, R>{gg, B}, partial, acc, scale);
-    std::swap(A, B);
+    if (in_window(L, i + 1)) ex.reduce(gg, OpStress<R, R>{gg, t.wo}, partial, acc, scale);
+    if (i >= kept0) {
+      A = t.wo;
+    } else {
+      std::swap(A, B);
+    }
   }
   AD_CUDA(cudaGetLastError());
   AD_CUDA(cudaEventRecord(w.ev[1], q));
@@ -389,13 +401,15 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   double ms_re = 0.0, ms_adj = 0.0;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
-    if (Prec<R>::kProduction) {
+    const bool kept = seg == nseg - 1;  // taped by the forward run
+    if (Prec<R>::kProduction && !kept) {
       st = write_ctl(s, w, tn[n0], n0, true);
       if (st != NMHD_OK) return st;
     }
     AD_CUDA(cudaEventRecord(w.ev[2], q));
-    AD_CUDA(cudaMemcpyAsync(tape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
-    for (int i = n0; i < n1; ++i) {
+    if (!kept)
+      AD_CUDA(cudaMemcpyAsync(tape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+    for (int i = n0; i < (kept ? n0 : n1); ++i) {
       const StepTape<R> t = tape_at(tape + (size_t)(i - n0) * kTapeFields * n, n);
       if constexpr (Prec<R>::kProduction)
         prod_step(s, w, t, false);
