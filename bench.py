@@ -443,26 +443,41 @@ def run_adjoint_arm(args):
 
 
 def adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg):
-    """Directions dv = sigma * N(0, 1) on the three initial velocity fields,
-    sigma = the noise amplitude 0.01 c_s.  The derivative is checked against
-    FP64 central differences around the same float state with eps = 1e-9
-    (relative to sigma), below the scale at which limiter, upwind-corner and
-    sign(Bx) choices flip; differences at the nominal eps = 1e-3 (FP32 and
-    FP64) are reported beside them: they measure those jumps of the piecewise
-    smooth discrete step as well as its derivative."""
+    """Gradient checks along directions dv = sigma * N(0, 1) on the three
+    initial velocity fields, sigma = the noise amplitude 0.01 c_s.
+
+    The discrete step is piecewise smooth: limiter, upwind-corner and sign(Bx)
+    choices jump when a perturbation moves a decision variable across zero, and
+    on the 64^3 box over 200 steps that happens for perturbations down to
+    ~1e-8 sigma.  The derivative is therefore checked against FP64 central
+    differences around the same float state with eps = 1e-9 sigma, accepted
+    only where the two one-sided differences agree to 1% (no jump inside
+    +-eps), else retried at eps/3 (twice).  Differences at the nominal
+    eps = 1e-3 (FP32 and FP64) are reported beside them: they measure those
+    jumps as well as the derivative."""
     gd = g.astype(np.float64)
     sigma = 0.01 * math.sqrt(cfg.gamma)
     eps = spec["fd_eps"]
-    eps_small = 1e-9
+    J0, _ = sol.tlm(steps, dts, None, window=window)
+    _, g64 = sol.adjoint_f64(steps, dts, window=window, ckpt_every=K)
     rows = []
     for k in range(spec["fd_dirs"]):
         rng = np.random.default_rng(100 + k)
         d = np.zeros(s.shape)
         d[1:4] = sigma * rng.normal(0.0, 1.0, s[1:4].shape)
-        row = {"adjoint32": float(np.sum(gd * d))}
-        jp, _ = sol.tlm(steps, dts, d, window=window, shift=eps_small)
-        jm, _ = sol.tlm(steps, dts, d, window=window, shift=-eps_small)
-        row["fd64_small"] = (jp - jm) / (2 * eps_small)
+        row = {"adjoint32": float(np.sum(gd * d)), "adjoint64": float(np.sum(g64 * d))}
+        e = 1e-9
+        for _ in range(3):
+            jp, _ = sol.tlm(steps, dts, d, window=window, shift=e)
+            jm, _ = sol.tlm(steps, dts, d, window=window, shift=-e)
+            sp_, sm_ = (jp - J0) / e, (J0 - jm) / e
+            smooth = abs(sp_ - sm_) <= 0.01 * abs(sp_ + sm_) / 2
+            if smooth:
+                break
+            e /= 3.0
+        row["eps_used"] = e
+        if smooth:
+            row["fd64"] = (jp - jm) / (2 * e)
         jp, _ = sol.tlm(steps, dts, d, window=window, shift=eps)
         jm, _ = sol.tlm(steps, dts, d, window=window, shift=-eps)
         row["fd64_nominal"] = (jp - jm) / (2 * eps)
@@ -488,12 +503,15 @@ def adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg):
     d = np.zeros(s.shape)
     d[1:4] = sigma * rng.normal(0.0, 1.0, s[1:4].shape)
     _, dJ64 = sol.tlm(steps, dts, d, window=window)
-    _, g64 = sol.adjoint_f64(steps, dts, window=window, ckpt_every=K)
-    return {"directions": spec["fd_dirs"], "noise_sigma": sigma, "eps_small": eps_small, "eps_nominal": eps,
-            "adjoint32_vs_fd64_small": rel("adjoint32", "fd64_small"),
-            "tlm64_vs_fd64_small": rel("tlm64", "fd64_small"),
+    return {"directions": spec["fd_dirs"], "noise_sigma": sigma, "eps_nominal": eps,
+            "fd64_flip_free_directions": int(sum("fd64" in r for r in rows)),
+            "eps_used": sorted({r["eps_used"] for r in rows}),
+            "adjoint64_vs_fd64": rel("adjoint64", "fd64"),
+            "adjoint32_vs_fd64": rel("adjoint32", "fd64"),
+            "tlm64_vs_fd64": rel("tlm64", "fd64"),
             "adjoint32_vs_tlm64": rel("adjoint32", "tlm64"),
-            "fd64_nominal_vs_fd64_small": rel("fd64_nominal", "fd64_small"),
+            "adjoint32_vs_adjoint64": rel("adjoint32", "adjoint64"),
+            "fd64_nominal_vs_fd64": rel("fd64_nominal", "fd64"),
             "adjoint32_vs_fd32_nominal": rel("adjoint32_applied", "fd32_nominal"),
             "fp64_adjoint_transpose_rel": abs(float(np.sum(g64 * d)) - dJ64) / abs(dJ64)}
 
