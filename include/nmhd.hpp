@@ -6,13 +6,19 @@
 //   proceed           -> bool (true when goal_time was reached; false on the
 //                        wallclock limit), wallclock_time_limit <= 0 ignored
 //   current_time      -> PreciseReal (double), generation -> int
-//   save_state/load_state(prefix) -> prefix.bin + prefix_setup.txt
+//   save_state/load_state(prefix) -> prefix.bin + prefix_setup.txt, the
+//                        reference's checkpoint files (see nmhd::checkpoint)
 // Problem hooks are not virtual here: the initial state is passed in with
 // initialize_state(fields) and the source term is chosen by nmhd_config.
 #ifndef NMHD_HPP
 #define NMHD_HPP
 
+#include <cmath>
 #include <cstdio>
+#include <fstream>
+#include <iomanip>
+#include <map>
+#include <sstream>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -20,6 +26,135 @@
 #include "nmhd.h"
 
 namespace nmhd {
+
+// The reference's checkpoint text, prefix_setup.txt: MHDSolver::save_state /
+// load_state (src/library/mhd_solver.inlrb:1023-1050) write GlobalSetup, a line
+// of "################", then LocalSetup, each as a member count followed by
+// "name value" lines with the default stream format (pod text of
+// src/nushio_script/persistent_pod.hrb:129-176).  load_state keeps only
+// generation and current_time (6 significant digits, so the reference's own
+// restarts are lossy).  Files written here add one GlobalSetup member,
+// current_time_exact (17 digits), which the reference's reader skips and this
+// reader prefers; a file written by either code loads in the other.
+namespace checkpoint {
+
+// Spacings, computational and local extents by the reference's float chains
+// (simulation_config_default.h:56-103) and the shear velocity -q Omega L_y.
+struct Derived {
+  float d[3], extent[3], local[3];
+  double rel_vel;
+};
+
+inline Derived derive(const nmhd_config &c) {
+  Derived r;
+  const int s[3] = {c.size_x, c.size_y, c.size_z};
+  const int gi[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
+  for (int i = 0; i < 3; ++i) {
+    volatile float per = L[i] / (float)gi[i];
+    volatile float comp = per * (float)s[i];
+    volatile float local = per * (float)gi[i];
+    volatile float d = comp / (float)s[i];
+    r.extent[i] = comp;
+    r.local[i] = local;
+    r.d[i] = d;
+  }
+  volatile float qo = -c.q * c.omega;
+  volatile float rv = qo * r.local[1];
+  r.rel_vel = c.problem == NMHD_PROBLEM_SHEARING_BOX ? (double)rv : 0.0;
+  return r;
+}
+
+// relative_displacement()'s normalized displacement of rank 0
+// (mhd_solver.inlrb:244-259), as the reference's float.
+inline float shear_displacement(const nmhd_config &c, double t) {
+  if (c.problem != NMHD_PROBLEM_SHEARING_BOX) return 0.0f;
+  const Derived d = derive(c);
+  const double d0 = 0.0 + t * d.rel_vel;
+  const int fold = (int)std::floor(d0 / (double)d.extent[0]);
+  const double d1 = d0 - (double)((float)fold * d.extent[0]);
+  return (float)d1;
+}
+
+// encode_member(std::string): bytes outside 33..126 and '%' as %xx.
+inline std::string encode(const std::string &s) {
+  std::string out;
+  char buf[4];
+  for (unsigned char ch : s) {
+    if (ch >= 33 && ch <= 126 && ch != '%') {
+      out += (char)ch;
+    } else {
+      std::snprintf(buf, sizeof buf, "%%%02x", ch);
+      out += buf;
+    }
+  }
+  return out;
+}
+
+inline std::string setup_text(const nmhd_config &c, int generation, double time, const std::string &dir) {
+  const Derived d = derive(c);
+  const int gs[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int sz[3] = {c.size_x, c.size_y, c.size_z};
+  const int mg[3] = {0, c.margin_y, c.margin_z};
+  const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
+  const char *ax[3] = {"x", "y", "z"}, *AX[3] = {"X", "Y", "Z"};
+  std::ostringstream o;
+  o << 21 << std::endl;
+  o << "generation " << generation << std::endl;
+  o << "real_size " << 4 << std::endl;
+  o << "real_precision float" << std::endl;
+  o << "current_time " << time << std::endl;
+  o << "parallel_size " << 1 << std::endl;
+  for (int k = 0; k < 3; ++k) {
+    o << "global_size_" << ax[k] << " " << gs[k] << std::endl;
+    o << "parallel_size_" << ax[k] << " " << 1 << std::endl;
+    o << "global_extent_" << ax[k] << " " << L[k] << std::endl;
+    o << "global_corner_" << ax[k] << " " << 0.0f << std::endl;
+    o << "d" << AX[k] << " " << d.d[k] << std::endl;
+  }
+  o << "current_time_exact " << std::setprecision(17) << time << std::setprecision(6) << std::endl;
+  o << std::endl << "################" << std::endl;
+  o << 21 << std::endl;
+  o << "mpi_rank " << 0 << std::endl;
+  o << "output_directory " << encode(dir) << std::endl;
+  o << "mpi_prefix " << encode("0000") << std::endl;
+  o << "relative_displacement " << (double)shear_displacement(c, time) << std::endl;
+  o << "relative_velocity " << d.rel_vel << std::endl;
+  o << "computational_size " << (size_t)c.size_x * c.size_y * c.size_z << std::endl;
+  for (int k = 0; k < 3; ++k) {
+    volatile float corner = (float)(-mg[k]) * d.d[k];
+    o << "computational_size_" << ax[k] << " " << sz[k] << std::endl;
+    o << "margin_" << ax[k] << " " << mg[k] << std::endl;
+    o << "computational_corner_" << ax[k] << " " << (float)corner << std::endl;
+    o << "computational_extent_" << ax[k] << " " << d.extent[k] << std::endl;
+    o << "d" << AX[k] << " " << d.d[k] << std::endl;
+  }
+  o << std::endl;
+  return o.str();
+}
+
+// The clock load_state restores: generation and current_time (the exact
+// member when present).  False when the pod cannot be read.
+inline bool clock_from_setup(std::istream &is, int &generation, double &time) {
+  int n;
+  if (!(is >> n) || n < 0) return false;
+  std::map<std::string, std::string> m;
+  for (int i = 0; i < n; ++i) {
+    std::string k, v;
+    if (!(is >> k >> v)) return false;
+    m[k] = v;
+  }
+  if (!m.count("generation") || !m.count("current_time")) return false;
+  try {
+    generation = std::stoi(m["generation"]);
+    time = std::stod(m.count("current_time_exact") ? m["current_time_exact"] : m["current_time"]);
+  } catch (const std::exception &) {
+    return false;
+  }
+  return true;
+}
+
+}  // namespace checkpoint
 
 class Error : public std::runtime_error {
  public:
@@ -74,22 +209,22 @@ class MHDSolver {
   long long last_steps() const { return last_steps_; }
 
   // save_state/load_state (mhd_solver.inlrb:1023-1050): the .bin dump plus
-  // the clock as text (generation and current_time, %.17g).
+  // the reference's setup text (nmhd::checkpoint).
   bool save_state(const std::string &prefix) {
     if (!write(prefix + ".bin")) return false;
-    FILE *fp = std::fopen((prefix + "_setup.txt").c_str(), "w");
-    if (!fp) return false;
-    std::fprintf(fp, "generation %d\ncurrent_time %.17g\n", generation(), current_time());
-    return std::fclose(fp) == 0;
+    std::ofstream ofs((prefix + "_setup.txt").c_str());
+    if (!ofs) return false;
+    const std::string::size_type slash = prefix.rfind('/');
+    const std::string dir = slash == std::string::npos ? "." : prefix.substr(0, slash);
+    ofs << checkpoint::setup_text(cfg_, generation(), current_time(), dir);
+    return (bool)ofs;
   }
   bool load_state(const std::string &prefix) {
-    FILE *fp = std::fopen((prefix + "_setup.txt").c_str(), "r");
-    if (!fp) return false;
+    std::ifstream ifs((prefix + "_setup.txt").c_str());
     int gen = 0;
     double t = 0;
-    const bool ok = std::fscanf(fp, "generation %d current_time %lf", &gen, &t) == 2;
-    std::fclose(fp);
-    if (!ok || !read(prefix + ".bin")) return false;
+    if (!ifs || !checkpoint::clock_from_setup(ifs, gen, t)) return false;
+    if (!read(prefix + ".bin")) return false;
     check(nmhd_set_time(s_, t, gen));
     return true;
   }

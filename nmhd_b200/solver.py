@@ -14,13 +14,12 @@ the GPU.
 from __future__ import annotations
 
 import ctypes
-import json
 import math
 import os
 
 import numpy as np
 
-from . import _lib
+from . import _lib, checkpoint
 from .config import SolverConfig
 
 
@@ -166,27 +165,36 @@ class MHDSolver:
 
     # -- checkpoint ------------------------------------------------------
     def save_state(self, prefix) -> bool:
-        """MHDSolver::save_state: ``prefix.bin`` plus ``prefix_setup.json`` with
-        the clock (generation, current_time) and the configuration."""
-        if not self.write(str(prefix) + ".bin"):
+        """MHDSolver::save_state (src/library/mhd_solver.inlrb:1023-1036):
+        ``prefix.bin`` plus ``prefix_setup.txt`` in the reference's pod text
+        (see :mod:`nmhd_b200.checkpoint`); the reference's load_state reads
+        both."""
+        prefix = str(prefix)
+        if not self.write(prefix + ".bin"):
             return False
-        meta = {"generation": self.generation(), "current_time": self.current_time(),
-                "config": self.config.__dict__}
-        with open(str(prefix) + "_setup.json", "w") as fp:
-            json.dump(meta, fp)
+        text = checkpoint.setup_text(self.config, self.generation(), self.current_time(),
+                                     output_directory=os.path.dirname(os.path.abspath(prefix)))
+        try:
+            with open(prefix + "_setup.txt", "w") as fp:
+                fp.write(text)
+        except OSError:
+            return False
         return True
 
     def load_state(self, prefix) -> bool:
-        """MHDSolver::load_state: restores the clock and the state; False (and
-        the state unchanged) when the files cannot be read."""
+        """MHDSolver::load_state (mhd_solver.inlrb:1038-1050): the clock from
+        ``prefix_setup.txt`` (written here or by the reference) and the state
+        from ``prefix.bin``; False, with state and clock unchanged, when a file
+        cannot be read."""
+        prefix = str(prefix)
         try:
-            with open(str(prefix) + "_setup.json") as fp:
-                meta = json.load(fp)
-        except OSError:
+            with open(prefix + "_setup.txt") as fp:
+                gen, t = checkpoint.clock_from_setup(fp.read())
+        except (OSError, ValueError, KeyError, IndexError):
             return False
-        if not self.read(str(prefix) + ".bin"):
+        if not self.read(prefix + ".bin"):
             return False
-        self.set_time(meta["current_time"], meta["generation"])
+        self.set_time(t, gen)
         return True
 
     def set_kernel(self, variant=0, tile_rows=8, z_chunk=16):

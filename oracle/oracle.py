@@ -102,8 +102,12 @@ def ref_binary(name):
     return p if os.path.exists(p) else None
 
 
-def run_ref(name, state, steps, goal_time=1.0e30, threads=None, dtype=np.float32):
-    """Run the reference binary ``name`` on ``state``; returns (state, times, info)."""
+def run_ref(name, state, steps, goal_time=1.0e30, threads=None, dtype=np.float32, ckpt_dir=None,
+            load_tag=None, save_tag=None):
+    """Run the reference binary ``name`` on ``state`` until generation
+    ``steps``; returns (state, times, info).  With ``ckpt_dir``, the run starts
+    from the reference's own load_state(load_tag) (``state`` is then unused)
+    and/or ends with save_state(save_tag), under ckpt_dir/<tag>/0000."""
     from nmhd_b200.binio import read_bin, write_bin
     exe = ref_binary(name)
     if exe is None:
@@ -111,6 +115,12 @@ def run_ref(name, state, steps, goal_time=1.0e30, threads=None, dtype=np.float32
     env = dict(os.environ)
     if threads:
         env["OMP_NUM_THREADS"] = str(threads)
+    if ckpt_dir:
+        env["NMHD_REF_DIR"] = str(ckpt_dir)
+        if load_tag:
+            env["NMHD_REF_LOAD"] = load_tag
+        if save_tag:
+            env["NMHD_REF_SAVE"] = save_tag
     with tempfile.TemporaryDirectory() as d:
         fin, fout, ftimes = (os.path.join(d, x) for x in ("in.bin", "out.bin", "t.txt"))
         write_bin(fin, state, dtype=dtype)

@@ -3,12 +3,17 @@
 //
 //   <binary> IN.bin OUT.bin NSTEPS [GOAL_TIME] [TIMES.txt]
 //
-// Reads the initial primitive state with MHDSolver::read, advances exactly
-// NSTEPS steps with MHDSolver::proceed (monitor() stops the loop, as in
+// Reads the initial primitive state with MHDSolver::read, advances until
+// generation NSTEPS with MHDSolver::proceed (monitor() stops the loop, as in
 // src/library/mhd_solver.inlrb:859-860), writes the state with
 // MHDSolver::write, and prints one JSON line with the wallclock of the proceed()
 // call.  TIMES.txt receives current_time() before every step and after the
 // last, as %.17g.
+//
+// Checkpoints (MHDSolver::save_state/load_state, mhd_solver.inlrb:1023-1050):
+// with NMHD_REF_DIR set, the solver's LocalSetup is that of rank 0 writing
+// under NMHD_REF_DIR; NMHD_REF_LOAD=tag starts from load_state(tag) instead of
+// IN.bin, NMHD_REF_SAVE=tag calls save_state(tag) after the run.
 #include <sys/time.h>
 #include <omp.h>
 
@@ -36,8 +41,15 @@ int main(int argc, char **argv) {
   }
   g_max_steps = std::atoi(argv[3]);
   double goal = argc > 4 ? std::atof(argv[4]) : 1.0e30;
-  MHDSolver solver;
-  if (!solver.read(argv[1])) {
+  const char *dir = std::getenv("NMHD_REF_DIR");
+  const char *load_tag = std::getenv("NMHD_REF_LOAD");
+  const char *save_tag = std::getenv("NMHD_REF_SAVE");
+  // LocalSetup(rank, dir) opens its log files under dir: only when asked
+  LocalSetup *setup = dir ? new LocalSetup(0, dir) : &blancLocalSetup;
+  MHDSolver solver(*setup);
+  if (dir && load_tag) {
+    solver.load_state(load_tag);
+  } else if (!solver.read(argv[1])) {
     std::fprintf(stderr, "cannot read %s (missing or size mismatch)\n", argv[1]);
     return 1;
   }
@@ -51,6 +63,7 @@ int main(int argc, char **argv) {
     std::fprintf(stderr, "cannot write %s\n", argv[2]);
     return 1;
   }
+  if (dir && save_tag) solver.save_state(save_tag);
   if (argc > 5) {
     FILE *fp = std::fopen(argv[5], "w");
     for (size_t i = 0; i < g_times.size(); ++i) std::fprintf(fp, "%.17g\n", g_times[i]);
