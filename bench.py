@@ -41,7 +41,10 @@ WORKLOADS = {
                                           l_radial=1.0, l_azimuthal=4.0, l_vertical=1.0, seed=3),
 }
 REF_BINARY = {"mri_shearing_box_128x256x64": "shear256x128x64"}
-ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0)}
+ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0),
+             # many small boxes (sides 8..16 radial/vertical, 2-4x azimuthal):
+             # the regime where per-box launches are latency-bound
+             "mri_ensemble_small_512": dict(n_boxes=512, seed=0, sides=(8, 12, 16))}
 # Differentiation: 64^3 shearing box of the MRI physics (Lx = Ly = Lz = 1,
 # seed 2), 200 FP32 steps, loss = Maxwell stress averaged over states 151..200,
 # checkpoints every 20 steps; 16 central-difference directions (seeds
