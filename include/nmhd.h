@@ -139,8 +139,11 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * variant 0: z-marching tiled kernels (32 x tile_rows cells per CTA,
  * tile_rows in {4, 8, 16}, z_chunk planes per CTA, 0 = whole height);
  * variant 1: per-cell flux and update kernels on 1-D blocks; variant 2 (the
- * default): per-cell kernels on 32x4x2 blocks.  tile_rows and z_chunk are
- * used by variant 0 only.  Every variant gives bitwise identical results. */
+ * default): per-cell kernels on 32x4x2 blocks; variant 3: the variant-2
+ * kernels as a pipeline over chunks of z_chunk planes, so each chunk's face
+ * fluxes are read back from L2 (nmhd_profile then times each whole stage as
+ * its flux class).  tile_rows is used by variant 0 only, z_chunk by variants
+ * 0 and 3.  Every variant gives bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
 /* Autotuner (replaces the reference's Ruby GA/parallel-tempering tuner of
  * launch dimensions, src/nushio_script/optimization.rb:33-140,

@@ -19,14 +19,17 @@ namespace {
 
 using namespace cell;
 
+// Every kernel covers the z planes [z0, z1) (the whole box, or one chunk of
+// the chunked pipeline).
 __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const StepCtl *ctl, const float *w0,
                                                            const float *w1, const float *wp,
-                                                           float *__restrict__ flux, int in_sel, int half) {
+                                                           float *__restrict__ flux, int in_sel, int half, int z0,
+                                                           int z1) {
   if (ctl->done) return;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
-  const int z = blockIdx.z * BZ + threadIdx.z;
-  if (x >= g.sx || y >= g.sy || z >= g.sz) return;
+  const int z = z0 + blockIdx.z * BZ + threadIdx.z;
+  if (x >= g.sx || y >= g.sy || z >= z1) return;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
   flux_cell(g, pick(ctl, in_sel, w0, w1, wp), flux, x, y, z, dt);
@@ -36,12 +39,12 @@ template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
                                                          float *w1, float *wp,
                                                          const float *__restrict__ flux, int in_sel,
-                                                         int out_sel, int half) {
+                                                         int out_sel, int half, int z0, int z1) {
   if (ctl->done) return;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
-  const int z = blockIdx.z * BZ + threadIdx.z;
-  if (x >= g.sx || y >= g.sy || z >= g.sz) return;
+  const int z = z0 + blockIdx.z * BZ + threadIdx.z;
+  if (x >= g.sx || y >= g.sy || z >= z1) return;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
   ct_cell<kPow2>(g, pick(ctl, in_sel, w0, w1, wp), pick(ctl, 0, w0, w1, wp),
@@ -52,44 +55,100 @@ template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, 3) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
                                                            float *w1, float *wp,
                                                            const float *__restrict__ flux, float *dt_hist,
-                                                           int out_sel, int half, int final_stage) {
+                                                           int out_sel, int half, int final_stage, int z0,
+                                                           int z1, unsigned ntiles) {
   __shared__ float red[kThreads / 32];
   if (ctl->done) return;
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
-  const int z = blockIdx.z * BZ + threadIdx.z;
+  const int z = z0 + blockIdx.z * BZ + threadIdx.z;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
   float tcfl = __uint_as_float(0x7f800000u);
   int bad = 0;
-  if (x < g.sx && y < g.sy && z < g.sz)
+  if (x < g.sx && y < g.sy && z < z1)
     tcfl = prim_cell<kPow2>(g, pick(ctl, 0, w0, w1, wp), const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)),
                             flux, x, y, z, dt, final_stage != 0, &bad);
-  if (final_stage) finish_tile(ctl, gridDim.x * gridDim.y * gridDim.z, tcfl, bad, dt_hist, red);
+  // ntiles: the CTAs of all this stage's k_cell_prim launches (the last one
+  // to finish advances the clock)
+  if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, red);
 }
 
-dim3 cell_grid(const GridParams &g) {
-  return dim3((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (g.sz + BZ - 1) / BZ);
+dim3 cell_grid(const GridParams &g, int nz) {
+  return dim3((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (nz + BZ - 1) / BZ);
+}
+
+template <bool kPow2>
+void update_range(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux, float *dt_hist,
+                  int in_sel, int out_sel, int half, int final_stage, int z0, int z1, unsigned ntiles, bool ct,
+                  bool prim, cudaStream_t st) {
+  const dim3 grid = cell_grid(g, z1 - z0), blk(BX, BY, BZ);
+  if (ct) k_cell_ct<kPow2><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half, z0, z1);
+  if (prim)
+    k_cell_prim<kPow2><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel, half, final_stage, z0,
+                                             z1, ntiles);
 }
 
 }  // namespace
 
 void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                       int in_sel, int half, cudaStream_t st) {
-  k_cell_flux<<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, half);
+  k_cell_flux<<<cell_grid(g, g.sz), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, half, 0, g.sz);
 }
 
 void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                         float *dt_hist, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
-  if (g.pow2_spacing) {
-    k_cell_ct<true><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
-    k_cell_prim<true><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel,
-                                                               half, final_stage);
-  } else {
-    k_cell_ct<false><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, out_sel, half);
-    k_cell_prim<false><<<cell_grid(g), dim3(BX, BY, BZ), 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, out_sel,
-                                                                half, final_stage);
+  const dim3 grid = cell_grid(g, g.sz);
+  const unsigned ntiles = grid.x * grid.y * grid.z;
+  if (g.pow2_spacing)
+    update_range<true>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, 0, g.sz, ntiles,
+                       true, true, st);
+  else
+    update_range<false>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, 0, g.sz, ntiles,
+                        true, true, st);
+}
+
+// One RK stage as a z-chunked pipeline (variant 3): chunk c of zc planes is
+// reconstructed/solved (F), its face B updated (C) and its cells finished (P)
+// so that a chunk's face fluxes are read back while still in L2.  C(c) needs
+// F(c-1), F(c), F(c+1) (corner EMFs one plane below and above); P(c) needs
+// C(c) and C(c+1) (the new B of the plane above) and F(c), F(c+1).  With the
+// periodic wrap the order is F(N-1), F(0), then F(c), C(c-1), P(c-2) for c
+// = 1..N-1, then C(N-1), P(N-2), P(N-1).
+void launch_cell_stage_chunked(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                               float *dt_hist, int in_sel, int out_sel, int half, int final_stage, int zc,
+                               cudaStream_t st) {
+  if (zc < 1) zc = g.sz;
+  const int nch = (g.sz + zc - 1) / zc;
+  auto lo = [&](int c) { return c * zc; };
+  auto hi = [&](int c) { return c == nch - 1 ? g.sz : (c + 1) * zc; };
+  unsigned ntiles = 0;
+  for (int c = 0; c < nch; ++c) {
+    const dim3 gr = cell_grid(g, hi(c) - lo(c));
+    ntiles += gr.x * gr.y * gr.z;
   }
+  const dim3 blk(BX, BY, BZ);
+  auto F = [&](int c) {
+    k_cell_flux<<<cell_grid(g, hi(c) - lo(c)), blk, 0, st>>>(g, ctl, w0, w1, wp, flux, in_sel, half, lo(c), hi(c));
+  };
+  auto U = [&](int c, bool ct, bool prim) {
+    if (g.pow2_spacing)
+      update_range<true>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, lo(c), hi(c),
+                         ntiles, ct, prim, st);
+    else
+      update_range<false>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, lo(c), hi(c),
+                          ntiles, ct, prim, st);
+  };
+  if (nch > 1) F(nch - 1);
+  F(0);
+  for (int c = 1; c < nch; ++c) {
+    if (c < nch - 1) F(c);
+    U(c - 1, true, false);
+    if (c >= 2) U(c - 2, false, true);
+  }
+  U(nch - 1, true, false);
+  if (nch >= 2) U(nch - 2, false, true);
+  U(nch - 1, false, true);
 }
 
 }  // namespace nmhd

@@ -141,6 +141,9 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
     nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
     nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                              final_stage, st);
+  } else if (s->variant == 3) {
+    nmhd::launch_cell_stage_chunked(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
+                                    final_stage, s->shape.zc, st);
   } else {
     nmhd::launch_stage(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                        final_stage, st);
@@ -499,7 +502,10 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
     NMHD_CUDA(s, cudaEventRecord(ev[2], q));
     float *unew = s->flux, *bflux = s->flux + (size_t)5 * g.n;
     // each stage as its two kernels (flux, then update / CT), separately timed
+    // variant 3 interleaves the two kernels by chunk: its whole stage is
+    // timed in the flux class and the update class reads 0
     auto flux_k = [&](int in_sel, int half) {
+      if (s->variant == 3) return;
       if (s->variant == 0)
         nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
       else if (s->variant == 2)
@@ -508,6 +514,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
         nmhd::launch_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
     };
     auto upd_k = [&](int in_sel, int out_sel, int half, int fin) {
+      if (s->variant == 3) return;
       if (s->variant == 0)
         nmhd::launch_tile_ct(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
                              half, fin, s->shape, q);
@@ -518,18 +525,26 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
         nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                             fin, q);
     };
+    auto whole = [&](int in_sel, int out_sel, int half, int fin) {
+      if (s->variant == 3)
+        nmhd::launch_cell_stage_chunked(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel,
+                                        half, fin, s->shape.zc, q);
+    };
     if (midpoint) {
       flux_k(0, 1);
+      whole(0, 2, 1, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[3], q));
       upd_k(0, 2, 1, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[4], q));
       flux_k(2, 0);
+      whole(2, 1, 0, 1);
       NMHD_CUDA(s, cudaEventRecord(ev[5], q));
       upd_k(2, 1, 0, 1);
     } else {
       NMHD_CUDA(s, cudaEventRecord(ev[3], q));
       NMHD_CUDA(s, cudaEventRecord(ev[4], q));
       flux_k(0, 0);
+      whole(0, 1, 0, 1);
       NMHD_CUDA(s, cudaEventRecord(ev[5], q));
       upd_k(0, 1, 0, 1);
     }
@@ -562,7 +577,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
 
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk) {
   if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
-  if (variant < 0 || variant > 2) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0, 1 or 2");
+  if (variant < 0 || variant > 3) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0, 1, 2 or 3");
   if (variant == 0 && tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
     return fail(s, NMHD_ERR_INVALID_ARGUMENT, "tile_rows must be 4, 8 or 16");
   if (z_chunk < 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "z_chunk must be >= 0");
@@ -570,6 +585,7 @@ nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_ch
   drop_graphs(s);
   s->variant = variant;
   if (variant == 0) s->shape = nmhd::TileShape{tile_rows, z_chunk};
+  if (variant == 3) s->shape = nmhd::TileShape{8, z_chunk};
   return NMHD_OK;
 }
 
@@ -594,6 +610,8 @@ int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials)
   std::vector<TuneChoice> cands;
   cands.push_back({2, 8, 0});
   cands.push_back({1, 8, 0});
+  for (int zc : {4, 8, 16})
+    if (zc < g.sz) cands.push_back({3, 8, zc});
   for (int rows : {4, 8, 16})
     for (int zc : {0, 8, 16, 32})
       if (zc == 0 || zc < g.sz) cands.push_back({0, rows, zc});

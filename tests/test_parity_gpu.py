@@ -166,7 +166,8 @@ def test_goal_time_semantics(gpu):
 
 
 @pytest.mark.parametrize("variant,rows,zc", [(2, 8, 0), (1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5),
-                                             (0, 8, 3)])
+                                             (0, 8, 3), (3, 8, 1), (3, 8, 2), (3, 8, 3), (3, 8, 4),
+                                             (3, 8, 64)])
 @pytest.mark.parametrize("case", ["ot_ragged", "shear_ragged", "shear_mz"])
 def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
     """Every kernel variant and tile shape, on boxes whose sizes are not
@@ -204,5 +205,27 @@ def test_autotune_restores_state_and_keeps_results_bitwise(gpu):
         assert sol.generation() == 2 and sol.current_time() == t_mid
         assert_same(sol.get_state(), mid)
         sol.step(4)
+        assert sol.current_time() == o["time"]
+        assert_same(sol.get_state(), o["state"])
+
+
+@pytest.mark.parametrize("zc", [1, 2, 5])
+@pytest.mark.parametrize("case", ["ot_2d", "euler", "order1"])
+def test_chunked_pipeline_variant_bitwise(gpu, zc, case):
+    """Variant 3 (z-chunked pipeline): single-plane boxes, Euler stepping and
+    first-order reconstruction, chunks of 1, 2 and 5 planes."""
+    if case == "ot_2d":
+        cfg, s = orszag_tang_3d(40, ny=24, nz=1)
+    elif case == "euler":
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=9, l_azimuthal=4.0, seed=4)
+        cfg.time_order = 1
+    else:
+        cfg, s = orszag_tang_3d(24, ny=20, nz=11)
+        cfg.space_order = 1
+    o = oracle.proceed(cfg, s, 10)
+    with MHDSolver(cfg) as sol:
+        sol.set_kernel(3, 8, zc)
+        sol.set_state(s)
+        sol.step(10)
         assert sol.current_time() == o["time"]
         assert_same(sol.get_state(), o["state"])
