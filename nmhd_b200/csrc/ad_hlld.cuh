@@ -333,164 +333,174 @@ NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R igm1, c
 
 
 // Reverse of the region flux (hlld_flux_side) and of the double-star states.
-template <bool kLeft, class R>
+// The fan side (left for regions 0-2, right for 3-5) is data, not control
+// flow: the side's quantities are selected, the adjoints accumulated in aX and
+// handed to its side at the end, and the sign sx = -1 (left) / +1 (right)
+// carries the two sides' mirror formulas (S_L* = S_M - |Bx|/sdL vs S_R* = S_M
+// + |Bx|/sdR, eL** = eL* - sdL(...) vs eR** = eR* + sdR(...)).  Faces of one
+// warp with fan regions on both sides then take one path.
+template <class R>
 NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj<R> &aR, R &aBx, R &aB2x,
                              R &aSM, R &aSL, R &aSR, R &aabs) {
   const int rg = t.region;
-  const HSide<R> &s = kLeft ? t.L : t.R;
-  HAdj<R> &aX = kLeft ? aL : aR;
+  const bool left = rg <= 2;
+  const R sx = left ? R(-1) : R(1);
+  // the side's forward quantities
+  const R d = left ? t.L.d : t.R.d, u = left ? t.L.u : t.R.u, v = left ? t.L.v : t.R.v;
+  const R w = left ? t.L.w : t.R.w, by = left ? t.L.by : t.R.by, bz = left ? t.L.bz : t.R.bz;
+  const R mx = left ? t.L.mx : t.R.mx, my = left ? t.L.my : t.R.my, mz = left ? t.L.mz : t.R.mz;
+  const R e = left ? t.L.e : t.R.e, pT = left ? t.L.pT : t.R.pT, vB = left ? t.L.vB : t.R.vB;
   const R Bx = t.Bx, sgn = t.sgn;
-  R aSss = R(0), aess = R(0), avss = R(0), awss = R(0), aByss = R(0), aBzss = R(0);
+  HAdj<R> aX;
+  hadj_zero(aX);
+  R aSX = R(0);
   // F = F(U) of side X
-  aX.d += lf[0] * s.u;
-  aX.u += lf[0] * s.d + lf[1] * s.mx + lf[2] * s.my + lf[3] * s.mz + lf[4] * (s.e + s.pT) + lf[5] * s.by +
-          lf[6] * s.bz;
-  aX.mx += lf[1] * s.u;
-  aX.pT += lf[1] + lf[4] * s.u;
+  aX.d += lf[0] * u;
+  aX.u += lf[0] * d + lf[1] * mx + lf[2] * my + lf[3] * mz + lf[4] * (e + pT) + lf[5] * by + lf[6] * bz;
+  aX.mx += lf[1] * u;
+  aX.pT += lf[1] + lf[4] * u;
   aB2x -= lf[1];
-  aX.my += lf[2] * s.u;
-  aX.mz += lf[3] * s.u;
-  aBx -= lf[2] * s.by + lf[3] * s.bz + lf[4] * s.vB + lf[5] * s.v + lf[6] * s.w;
-  aX.by += lf[5] * s.u - lf[2] * Bx;
-  aX.bz += lf[6] * s.u - lf[3] * Bx;
-  aX.e += lf[4] * s.u;
+  aX.my += lf[2] * u;
+  aX.mz += lf[3] * u;
+  aBx -= lf[2] * by + lf[3] * bz + lf[4] * vB + lf[5] * v + lf[6] * w;
+  aX.by += lf[5] * u - lf[2] * Bx;
+  aX.bz += lf[6] * u - lf[3] * Bx;
+  aX.e += lf[4] * u;
   aX.vB -= lf[4] * Bx;
   aX.v -= lf[5] * Bx;
   aX.w -= lf[6] * Bx;
-  if (rg == 0 || rg == 5) return;
-  const R S = kLeft ? t.S_L : t.S_R;
-  const R Us1 = s.ds * t.S_M, Us2 = s.ds * s.vs, Us3 = s.ds * s.ws;
-  // -S*U
-  aX.d -= S * lf[0];
-  aX.mx -= S * lf[1];
-  aX.my -= S * lf[2];
-  aX.mz -= S * lf[3];
-  aX.e -= S * lf[4];
-  aX.by -= S * lf[5];
-  aX.bz -= S * lf[6];
-  // d/dS of S*(U* - U) (regions 1, 4) and of -(Sss - S)*U* - S*U (regions 2, 3)
-  const R aS = lf[0] * (s.ds - s.d) + lf[1] * (Us1 - s.mx) + lf[2] * (Us2 - s.my) + lf[3] * (Us3 - s.mz) +
-               lf[4] * (s.es - s.e) + lf[5] * (s.bys - s.by) + lf[6] * (s.bzs - s.bz);
-  if (kLeft) aSL += aS; else aSR += aS;
-  R cs = S;  // coefficient of U*
-  const bool dstar = rg == 2 || rg == 3;
-  if (dstar) {
-    const R Sss = s.Ss;
-    const R ess = kLeft ? t.eLss : t.eRss;
-    cs = -(Sss - S);
-    aSss = lf[2] * (s.ds * t.vss - Us2) + lf[3] * (s.ds * t.wss - Us3) + lf[4] * (ess - s.es) +
-           lf[5] * (t.Byss - s.bys) + lf[6] * (t.Bzss - s.bzs);
-    // Sss * U**
-    aX.ds += Sss * (lf[0] + lf[1] * t.S_M + lf[2] * t.vss + lf[3] * t.wss);
-    aSM += Sss * lf[1] * s.ds;
-    avss = Sss * lf[2] * s.ds;
-    awss = Sss * lf[3] * s.ds;
-    aess = Sss * lf[4];
-    aByss = Sss * lf[5];
-    aBzss = Sss * lf[6];
-  }
-  aX.ds += cs * (lf[0] + lf[1] * t.S_M + lf[2] * s.vs + lf[3] * s.ws);
-  aSM += cs * lf[1] * s.ds;
-  aX.vs += cs * lf[2] * s.ds;
-  aX.ws += cs * lf[3] * s.ds;
-  aX.es += cs * lf[4];
-  aX.bys += cs * lf[5];
-  aX.bzs += cs * lf[6];
-  if (!dstar) return;
-
-  R avBss = R(0), afr = R(0), asdLR = R(0);
-  // ess = eLs - sdL*(vBLs - vBss)*sgn (left), eRs + sdR*(vBRs - vBss)*sgn (right)
-  aX.es += aess;
-  if (kLeft) {
-    aX.sd -= aess * (s.vBs - t.vBss) * sgn;
-    aX.vBs -= aess * s.sd * sgn;
-    avBss += aess * s.sd * sgn;
-  } else {
-    aX.sd += aess * (s.vBs - t.vBss) * sgn;
-    aX.vBs += aess * s.sd * sgn;
-    avBss -= aess * s.sd * sgn;
-  }
-  // vBss = S_M*Bx + vss*Byss + wss*Bzss
-  aSM += avBss * Bx;
-  aBx += avBss * t.S_M;
-  avss += avBss * t.Byss;
-  aByss += avBss * t.vss;
-  awss += avBss * t.Bzss;
-  aBzss += avBss * t.wss;
-  // Bzss = fr*(sdL*bzRs + sdR*bzLs + sdLR*(wRs - wLs)*sgn)
-  {
-    const R n = t.L.sd * t.R.bzs + t.R.sd * t.L.bzs + t.sdLR * (t.R.ws - t.L.ws) * sgn;
-    afr += aBzss * n;
-    const R c = aBzss * t.fr;
-    aL.sd += c * t.R.bzs;
-    aR.bzs += c * t.L.sd;
-    aR.sd += c * t.L.bzs;
-    aL.bzs += c * t.R.sd;
-    asdLR += c * (t.R.ws - t.L.ws) * sgn;
-    aR.ws += c * t.sdLR * sgn;
-    aL.ws -= c * t.sdLR * sgn;
-  }
-  // Byss = fr*(sdL*byRs + sdR*byLs + sdLR*(vRs - vLs)*sgn)
-  {
-    const R n = t.L.sd * t.R.bys + t.R.sd * t.L.bys + t.sdLR * (t.R.vs - t.L.vs) * sgn;
-    afr += aByss * n;
-    const R c = aByss * t.fr;
-    aL.sd += c * t.R.bys;
-    aR.bys += c * t.L.sd;
-    aR.sd += c * t.L.bys;
-    aL.bys += c * t.R.sd;
-    asdLR += c * (t.R.vs - t.L.vs) * sgn;
-    aR.vs += c * t.sdLR * sgn;
-    aL.vs -= c * t.sdLR * sgn;
-  }
-  // wss = fr*(sdL*wLs + sdR*wRs + (bzRs - bzLs)*sgn)
-  {
-    const R n = t.L.sd * t.L.ws + t.R.sd * t.R.ws + (t.R.bzs - t.L.bzs) * sgn;
-    afr += awss * n;
-    const R c = awss * t.fr;
-    aL.sd += c * t.L.ws;
-    aL.ws += c * t.L.sd;
-    aR.sd += c * t.R.ws;
-    aR.ws += c * t.R.sd;
-    aR.bzs += c * sgn;
-    aL.bzs -= c * sgn;
-  }
-  // vss = fr*(sdL*vLs + sdR*vRs + (byRs - byLs)*sgn)
-  {
-    const R n = t.L.sd * t.L.vs + t.R.sd * t.R.vs + (t.R.bys - t.L.bys) * sgn;
-    afr += avss * n;
-    const R c = avss * t.fr;
-    aL.sd += c * t.L.vs;
-    aL.vs += c * t.L.sd;
-    aR.sd += c * t.R.vs;
-    aR.vs += c * t.R.sd;
-    aR.bys += c * sgn;
-    aL.bys -= c * sgn;
-  }
-  // sdLR = sqrt(dLs*dRs)
-  if (t.sdLR > R(0)) {
-    const R c = asdLR * (R(0.5) / t.sdLR);
-    aL.ds += c * t.R.ds;
-    aR.ds += c * t.L.ds;
-  }
-  // fr = 1/(sdL + sdR)
-  {
-    const R c = -afr * t.fr * t.fr;
-    aL.sd += c;
-    aR.sd += c;
-  }
-  // Sss = S_L* = S_M - |Bx|/sdL (left) or S_R* = S_M + |Bx|/sdR (right)
-  aSM += aSss;
-  {
-    const R isd = R(1) / s.sd;
-    if (kLeft) {
-      aabs -= aSss * isd;
-      aX.sd += aSss * t.absBx * isd * isd;
-    } else {
-      aabs += aSss * isd;
-      aX.sd -= aSss * t.absBx * isd * isd;
+  if (rg != 0 && rg != 5) {
+    const R S = left ? t.S_L : t.S_R;
+    const R ds = left ? t.L.ds : t.R.ds, vs = left ? t.L.vs : t.R.vs, ws = left ? t.L.ws : t.R.ws;
+    const R es = left ? t.L.es : t.R.es, bys = left ? t.L.bys : t.R.bys, bzs = left ? t.L.bzs : t.R.bzs;
+    const R Us1 = ds * t.S_M, Us2 = ds * vs, Us3 = ds * ws;
+    // -S*U
+    aX.d -= S * lf[0];
+    aX.mx -= S * lf[1];
+    aX.my -= S * lf[2];
+    aX.mz -= S * lf[3];
+    aX.e -= S * lf[4];
+    aX.by -= S * lf[5];
+    aX.bz -= S * lf[6];
+    // d/dS of S*(U* - U) (regions 1, 4) and of -(Sss - S)*U* - S*U (regions 2, 3)
+    aSX += lf[0] * (ds - d) + lf[1] * (Us1 - mx) + lf[2] * (Us2 - my) + lf[3] * (Us3 - mz) +
+           lf[4] * (es - e) + lf[5] * (bys - by) + lf[6] * (bzs - bz);
+    R cs = S;  // coefficient of U*
+    const bool dstar = rg == 2 || rg == 3;
+    if (dstar) {
+      const R sd = left ? t.L.sd : t.R.sd, vBs = left ? t.L.vBs : t.R.vBs;
+      const R Sss = left ? t.L.Ss : t.R.Ss;
+      const R ess = left ? t.eLss : t.eRss;
+      cs = -(Sss - S);
+      const R aSss = lf[2] * (ds * t.vss - Us2) + lf[3] * (ds * t.wss - Us3) + lf[4] * (ess - es) +
+                     lf[5] * (t.Byss - bys) + lf[6] * (t.Bzss - bzs);
+      // Sss * U**
+      aX.ds += Sss * (lf[0] + lf[1] * t.S_M + lf[2] * t.vss + lf[3] * t.wss);
+      aSM += Sss * lf[1] * ds;
+      R avss = Sss * lf[2] * ds, awss = Sss * lf[3] * ds;
+      const R aess = Sss * lf[4];
+      R aByss = Sss * lf[5], aBzss = Sss * lf[6];
+      // ess = eX* + sx * sdX * (vBX* - vBss) * sgn
+      R avBss = R(0), afr = R(0), asdLR = R(0);
+      aX.es += aess;
+      aX.sd += sx * aess * (vBs - t.vBss) * sgn;
+      aX.vBs += sx * aess * sd * sgn;
+      avBss -= sx * aess * sd * sgn;
+      // vBss = S_M*Bx + vss*Byss + wss*Bzss
+      aSM += avBss * Bx;
+      aBx += avBss * t.S_M;
+      avss += avBss * t.Byss;
+      aByss += avBss * t.vss;
+      awss += avBss * t.Bzss;
+      aBzss += avBss * t.wss;
+      // Bzss = fr*(sdL*bzRs + sdR*bzLs + sdLR*(wRs - wLs)*sgn)
+      {
+        const R n = t.L.sd * t.R.bzs + t.R.sd * t.L.bzs + t.sdLR * (t.R.ws - t.L.ws) * sgn;
+        afr += aBzss * n;
+        const R c = aBzss * t.fr;
+        aL.sd += c * t.R.bzs;
+        aR.bzs += c * t.L.sd;
+        aR.sd += c * t.L.bzs;
+        aL.bzs += c * t.R.sd;
+        asdLR += c * (t.R.ws - t.L.ws) * sgn;
+        aR.ws += c * t.sdLR * sgn;
+        aL.ws -= c * t.sdLR * sgn;
+      }
+      // Byss = fr*(sdL*byRs + sdR*byLs + sdLR*(vRs - vLs)*sgn)
+      {
+        const R n = t.L.sd * t.R.bys + t.R.sd * t.L.bys + t.sdLR * (t.R.vs - t.L.vs) * sgn;
+        afr += aByss * n;
+        const R c = aByss * t.fr;
+        aL.sd += c * t.R.bys;
+        aR.bys += c * t.L.sd;
+        aR.sd += c * t.L.bys;
+        aL.bys += c * t.R.sd;
+        asdLR += c * (t.R.vs - t.L.vs) * sgn;
+        aR.vs += c * t.sdLR * sgn;
+        aL.vs -= c * t.sdLR * sgn;
+      }
+      // wss = fr*(sdL*wLs + sdR*wRs + (bzRs - bzLs)*sgn)
+      {
+        const R n = t.L.sd * t.L.ws + t.R.sd * t.R.ws + (t.R.bzs - t.L.bzs) * sgn;
+        afr += awss * n;
+        const R c = awss * t.fr;
+        aL.sd += c * t.L.ws;
+        aL.ws += c * t.L.sd;
+        aR.sd += c * t.R.ws;
+        aR.ws += c * t.R.sd;
+        aR.bzs += c * sgn;
+        aL.bzs -= c * sgn;
+      }
+      // vss = fr*(sdL*vLs + sdR*vRs + (byRs - byLs)*sgn)
+      {
+        const R n = t.L.sd * t.L.vs + t.R.sd * t.R.vs + (t.R.bys - t.L.bys) * sgn;
+        afr += avss * n;
+        const R c = avss * t.fr;
+        aL.sd += c * t.L.vs;
+        aL.vs += c * t.L.sd;
+        aR.sd += c * t.R.vs;
+        aR.vs += c * t.R.sd;
+        aR.bys += c * sgn;
+        aL.bys -= c * sgn;
+      }
+      // sdLR = sqrt(dLs*dRs)
+      if (t.sdLR > R(0)) {
+        const R c = asdLR * (R(0.5) / t.sdLR);
+        aL.ds += c * t.R.ds;
+        aR.ds += c * t.L.ds;
+      }
+      // fr = 1/(sdL + sdR)
+      {
+        const R c = -afr * t.fr * t.fr;
+        aL.sd += c;
+        aR.sd += c;
+      }
+      // Sss = S_M + sx*|Bx|/sdX
+      aSM += aSss;
+      {
+        const R isd = R(1) / sd;
+        aabs += sx * aSss * isd;
+        aX.sd -= sx * aSss * t.absBx * isd * isd;
+      }
     }
+    aX.ds += cs * (lf[0] + lf[1] * t.S_M + lf[2] * vs + lf[3] * ws);
+    aSM += cs * lf[1] * ds;
+    aX.vs += cs * lf[2] * ds;
+    aX.ws += cs * lf[3] * ds;
+    aX.es += cs * lf[4];
+    aX.bys += cs * lf[5];
+    aX.bzs += cs * lf[6];
   }
+  // hand the side-X adjoints to their side
+  const R kl = left ? R(1) : R(0), kr = R(1) - kl;
+#define NMHD_HAND(f) aL.f += kl * aX.f; aR.f += kr * aX.f;
+  NMHD_HAND(d) NMHD_HAND(u) NMHD_HAND(v) NMHD_HAND(w) NMHD_HAND(by) NMHD_HAND(bz)
+  NMHD_HAND(mx) NMHD_HAND(my) NMHD_HAND(mz) NMHD_HAND(e) NMHD_HAND(pT) NMHD_HAND(vB)
+  NMHD_HAND(ds) NMHD_HAND(vs) NMHD_HAND(ws) NMHD_HAND(es) NMHD_HAND(bys) NMHD_HAND(bzs)
+  NMHD_HAND(sd) NMHD_HAND(vBs)
+#undef NMHD_HAND
+  aSL += kl * aSX;
+  aSR += kr * aSX;
 }
 
 // Adjoint of hlld_g: ls and lBx receive d<lf, f>/d(state) and d<lf, f>/dBx.
@@ -506,8 +516,7 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
   hadj_zero(aR);
   R aBx = R(0), aB2x = R(0), aSM = R(0), apTs = R(0), aSL = R(0), aSR = R(0), aabs = R(0);
   const R sgn = t.sgn;
-  if (left) hlld_region_rev<true>(t, lf, aL, aR, aBx, aB2x, aSM, aSL, aSR, aabs);
-  else hlld_region_rev<false>(t, lf, aL, aR, aBx, aB2x, aSM, aSL, aSR, aabs);
+  hlld_region_rev(t, lf, aL, aR, aBx, aB2x, aSM, aSL, aSR, aabs);
   if (rg != 0 && rg != 5) {  // regions 0 and 5 use no wave speed or star state
     // --- star states of both sides ---------------------------------------------
     hlld_side_star_rev(t.L, Bx, t.S_M, t.pT_s, aL, aSM, apTs, aBx, aB2x, aSL);
