@@ -60,6 +60,11 @@ typedef struct nmhd_config {
   int32_t space_order;            /* 2: minbee (reference default), 1: piecewise constant */
   int32_t time_order;             /* 2: midpoint RK2 (reference default), 1: Euler */
   int32_t flags;                  /* reserved, 0 */
+  /* kParallelSizeY: 0 or 1 for a whole box; P > 1 makes this solver one
+   * radial slab of a box split over P ranks along Y (size_y counts the slab's
+   * rows and margins, extent_y is the whole box's).  Its Y margins then come
+   * from the neighbouring slabs through nmhd_halo_pack/nmhd_halo_unpack. */
+  int32_t parallel_size_y;
 } nmhd_config;
 
 /* Conservation and field diagnostics, accumulated in FP64 over the interior
@@ -263,6 +268,39 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
  * [0] forward run with checkpoints, [1] segment recomputation, [2] adjoint
  * kernels, [3] the whole run. */
 nmhd_status nmhd_adjoint_timing(const nmhd_solver *s, double ms_out[4]);
+
+/* ---- Radial slab decomposition (kParallelSizeY = P ranks along Y) ----
+ * Replaces the reference's host-staged MPI halo exchange, MHDSolver::
+ * communicate (src/library/mhd_solver.inlrb:283-493), and the dt reduction of
+ * proceed (:870-893, MPI_Allreduce MIN), for a solver created with
+ * parallel_size_y = P: one step of rank r is
+ *   nmhd_halo_pack(s, send_inc, send_dec)   gather the shear-shifted boundary rows
+ *   transport: send_inc to rank (r+1)%P and send_dec to rank (r-1+P)%P;
+ *              receive recv_inc from (r-1+P)%P and recv_dec from (r+1)%P
+ *   nmhd_halo_unpack(s, recv_inc, recv_dec) fill the Y (and Z) margins, CFL time of the slab
+ *   reduce:    the float at nmhd_cfl_slot(s) := its minimum over the P ranks
+ *   nmhd_step_stages(s)                     the RK stages with the common dt
+ * These enqueue on the solver's stream and return at once; the caller's
+ * transport (NCCL send/recv and all-reduce on the same stream, or device
+ * copies between slabs of one process) runs between them.  Halo buffers are
+ * device memory of nmhd_halo_count(s) floats (8 fields x Sx x margin_y x Sz,
+ * the reference's mpi_buffer_y_* layout).  With P = 1 and each message
+ * delivered to itself this is exactly nmhd_proceed's step.
+ * nmhd_slab_begin prepares a run toward goal_time (proceed()'s goal);
+ * nmhd_slab_poll waits for the stream and returns NMHD_GOAL_REACHED once the
+ * goal step is done, NMHD_ERR_NUMERICAL on a bad state, else NMHD_OK; steps
+ * after the goal step are no-ops.  nmhd_proceed, nmhd_profile and
+ * nmhd_autotune refuse a slab (P > 1) with NMHD_ERR_NOT_SUPPORTED. */
+int64_t nmhd_halo_count(const nmhd_solver *s);
+nmhd_status nmhd_slab_begin(nmhd_solver *s, double goal_time);
+nmhd_status nmhd_halo_pack(nmhd_solver *s, float *send_inc, float *send_dec);
+nmhd_status nmhd_halo_unpack(nmhd_solver *s, const float *recv_inc, const float *recv_dec);
+float *nmhd_cfl_slot(nmhd_solver *s);
+/* The reduce step for n slabs of one process that share one device and one
+ * stream (nmhd_set_stream): one kernel on that stream. */
+nmhd_status nmhd_cfl_min(nmhd_solver *const *slabs, int n);
+nmhd_status nmhd_step_stages(nmhd_solver *s);
+nmhd_status nmhd_slab_poll(nmhd_solver *s, int64_t *generation, double *time);
 
 /* Library version string. */
 const char *nmhd_version(void);

@@ -47,13 +47,15 @@ struct Derived {
 
 inline Derived derive(const nmhd_config &c) {
   Derived r;
+  const int py = c.parallel_size_y > 1 ? c.parallel_size_y : 1;
   const int s[3] = {c.size_x, c.size_y, c.size_z};
-  const int gi[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int li[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int gi[3] = {li[0], py * li[1], li[2]};
   const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
   for (int i = 0; i < 3; ++i) {
     volatile float per = L[i] / (float)gi[i];
     volatile float comp = per * (float)s[i];
-    volatile float local = per * (float)gi[i];
+    volatile float local = per * (float)li[i];
     volatile float d = comp / (float)s[i];
     r.extent[i] = comp;
     r.local[i] = local;
@@ -65,8 +67,8 @@ inline Derived derive(const nmhd_config &c) {
   return r;
 }
 
-// relative_displacement()'s normalized displacement of rank 0
-// (mhd_solver.inlrb:244-259), as the reference's float.
+// relative_displacement()'s normalized displacement (mhd_solver.inlrb:244-259),
+// as the reference's float; the same for every radial rank.
 inline float shear_displacement(const nmhd_config &c, double t) {
   if (c.problem != NMHD_PROBLEM_SHEARING_BOX) return 0.0f;
   const Derived d = derive(c);
@@ -91,9 +93,14 @@ inline std::string encode(const std::string &s) {
   return out;
 }
 
-inline std::string setup_text(const nmhd_config &c, int generation, double time, const std::string &dir) {
+// `rank`: the radial slab's rank when c.parallel_size_y > 1, else 0.
+inline std::string setup_text(const nmhd_config &c, int generation, double time, const std::string &dir,
+                              int rank = 0) {
   const Derived d = derive(c);
-  const int gs[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int py = c.parallel_size_y > 1 ? c.parallel_size_y : 1;
+  const int li[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int gs[3] = {li[0], py * li[1], li[2]};
+  const int ps[3] = {1, py, 1}, r3[3] = {0, rank, 0};
   const int sz[3] = {c.size_x, c.size_y, c.size_z};
   const int mg[3] = {0, c.margin_y, c.margin_z};
   const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
@@ -104,10 +111,10 @@ inline std::string setup_text(const nmhd_config &c, int generation, double time,
   o << "real_size " << 4 << std::endl;
   o << "real_precision float" << std::endl;
   o << "current_time " << time << std::endl;
-  o << "parallel_size " << 1 << std::endl;
+  o << "parallel_size " << py << std::endl;
   for (int k = 0; k < 3; ++k) {
     o << "global_size_" << ax[k] << " " << gs[k] << std::endl;
-    o << "parallel_size_" << ax[k] << " " << 1 << std::endl;
+    o << "parallel_size_" << ax[k] << " " << ps[k] << std::endl;
     o << "global_extent_" << ax[k] << " " << L[k] << std::endl;
     o << "global_corner_" << ax[k] << " " << 0.0f << std::endl;
     o << "d" << AX[k] << " " << d.d[k] << std::endl;
@@ -115,14 +122,17 @@ inline std::string setup_text(const nmhd_config &c, int generation, double time,
   o << "current_time_exact " << std::setprecision(17) << time << std::setprecision(6) << std::endl;
   o << std::endl << "################" << std::endl;
   o << 21 << std::endl;
-  o << "mpi_rank " << 0 << std::endl;
+  char prefix[16];
+  std::snprintf(prefix, sizeof prefix, "%04d", rank);
+  o << "mpi_rank " << rank << std::endl;
   o << "output_directory " << encode(dir) << std::endl;
-  o << "mpi_prefix " << encode("0000") << std::endl;
+  o << "mpi_prefix " << encode(prefix) << std::endl;
   o << "relative_displacement " << (double)shear_displacement(c, time) << std::endl;
   o << "relative_velocity " << d.rel_vel << std::endl;
   o << "computational_size " << (size_t)c.size_x * c.size_y * c.size_z << std::endl;
   for (int k = 0; k < 3; ++k) {
-    volatile float corner = (float)(-mg[k]) * d.d[k];
+    // kGlobalCorner + (kLocalSize * rank - kMarginSize) * kD (LocalSetup, mhd_solver.h:311-317)
+    volatile float corner = (float)(li[k] * r3[k] - mg[k]) * d.d[k];
     o << "computational_size_" << ax[k] << " " << sz[k] << std::endl;
     o << "margin_" << ax[k] << " " << mg[k] << std::endl;
     o << "computational_corner_" << ax[k] << " " << (float)corner << std::endl;
@@ -209,14 +219,14 @@ class MHDSolver {
   long long last_steps() const { return last_steps_; }
 
   // save_state/load_state (mhd_solver.inlrb:1023-1050): the .bin dump plus
-  // the reference's setup text (nmhd::checkpoint).
-  bool save_state(const std::string &prefix) {
+  // the reference's setup text (nmhd::checkpoint); `rank` of a radial slab.
+  bool save_state(const std::string &prefix, int rank = 0) {
     if (!write(prefix + ".bin")) return false;
     std::ofstream ofs((prefix + "_setup.txt").c_str());
     if (!ofs) return false;
     const std::string::size_type slash = prefix.rfind('/');
     const std::string dir = slash == std::string::npos ? "." : prefix.substr(0, slash);
-    ofs << checkpoint::setup_text(cfg_, generation(), current_time(), dir);
+    ofs << checkpoint::setup_text(cfg_, generation(), current_time(), dir, rank);
     return (bool)ofs;
   }
   bool load_state(const std::string &prefix) {

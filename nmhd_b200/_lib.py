@@ -80,6 +80,14 @@ _SIGS = [
     ("nmhd_batch_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_last_error", ctypes.c_char_p, [_P]),
+    ("nmhd_halo_count", ctypes.c_int64, [_P]),
+    ("nmhd_slab_begin", ctypes.c_int, [_P, ctypes.c_double]),
+    ("nmhd_halo_pack", ctypes.c_int, [_P, _P, _P]),
+    ("nmhd_halo_unpack", ctypes.c_int, [_P, _P, _P]),
+    ("nmhd_cfl_slot", _P, [_P]),
+    ("nmhd_cfl_min", ctypes.c_int, [ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_step_stages", ctypes.c_int, [_P]),
+    ("nmhd_slab_poll", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int64), ctypes.POINTER(ctypes.c_double)]),
 ]
 EXPORTS = [s[0] for s in _SIGS]
 

@@ -54,9 +54,10 @@ def _dec(s: str) -> str:
 
 
 def shear_displacement(cfg, time: float) -> float:
-    """relative_displacement()'s normalized displacement (mhd_solver.inlrb:244-259)
-    of rank 0: the azimuthal offset of the shearing boundary, folded into the
-    box, as the reference's float."""
+    """relative_displacement()'s normalized displacement (mhd_solver.inlrb:244-259):
+    the azimuthal offset of a rank's upper shearing boundary, folded into the
+    box, as the reference's float (the same for every radial rank, whose
+    relative velocity is that of its own slab)."""
     if cfg.problem != "shearing_box":
         return 0.0
     d = cfg.derived()
@@ -66,26 +67,36 @@ def shear_displacement(cfg, time: float) -> float:
 
 
 def setup_text(cfg, generation: int, time: float, output_directory: str = ".",
-               mpi_prefix: str = "0000") -> str:
+               mpi_prefix: str = None, rank: int = 0) -> str:
     """The ``_setup.txt`` that the reference's save_state writes for this box
-    and clock (rank 0 of one), plus the ``current_time_exact`` member."""
+    and clock, plus the ``current_time_exact`` member.  ``rank`` is the radial
+    slab's rank when ``cfg.parallel_size_y`` > 1 (ranks along Y only), else 0."""
     d = cfg.derived()
-    gsize = (cfg.size_x, cfg.size_y - 2 * cfg.margin_y, cfg.size_z - 2 * cfg.margin_z)
+    py = max(1, cfg.parallel_size_y)
+    if not 0 <= rank < py:
+        raise ValueError("rank must be in [0, parallel_size_y)")
+    if mpi_prefix is None:
+        mpi_prefix = "%04d" % rank
+    local = (cfg.size_x, cfg.size_y - 2 * cfg.margin_y, cfg.size_z - 2 * cfg.margin_z)
+    gsize = (local[0], py * local[1], local[2])
+    psize = (1, py, 1)
+    rank3 = (0, rank, 0)
     gext = (np.float32(cfg.extent_x), np.float32(cfg.extent_y), np.float32(cfg.extent_z))
     sizes = (cfg.size_x, cfg.size_y, cfg.size_z)
     margins = (0, cfg.margin_y, cfg.margin_z)
     dd = (d["dx"], d["dy"], d["dz"])
     g = [("generation", generation), ("real_size", 4), ("real_precision", "float"),
-         ("current_time", float(time)), ("parallel_size", 1)]
+         ("current_time", float(time)), ("parallel_size", py)]
     for k, ax in enumerate("xyz"):
-        g += [("global_size_" + ax, gsize[k]), ("parallel_size_" + ax, 1),
+        g += [("global_size_" + ax, gsize[k]), ("parallel_size_" + ax, psize[k]),
               ("global_extent_" + ax, gext[k]), ("global_corner_" + ax, 0.0), ("d" + ax.upper(), dd[k])]
     rel_vel = d["relative_velocity"] if cfg.problem == "shearing_box" else 0.0
-    loc = [("mpi_rank", 0), ("output_directory", output_directory), ("mpi_prefix", mpi_prefix),
+    loc = [("mpi_rank", rank), ("output_directory", output_directory), ("mpi_prefix", mpi_prefix),
            ("relative_displacement", shear_displacement(cfg, time)), ("relative_velocity", rel_vel),
            ("computational_size", cfg.cells)]
     for k, ax in enumerate("xyz"):
-        corner = np.float32(np.float32(-margins[k]) * dd[k])  # (local size * rank - margin) * d
+        # LocalSetup: kGlobalCorner + (kLocalSize * rank - kMarginSize) * kD (mhd_solver.h:311-317)
+        corner = np.float32(np.float32(local[k] * rank3[k] - margins[k]) * dd[k])
         loc += [("computational_size_" + ax, sizes[k]), ("margin_" + ax, margins[k]),
                 ("computational_corner_" + ax, corner), ("computational_extent_" + ax, d["extent_" + ax]),
                 ("d" + ax.upper(), dd[k])]

@@ -29,7 +29,7 @@ class NmhdConfig(ctypes.Structure):
         ("gamma", ctypes.c_float), ("cfl", ctypes.c_float),
         ("problem", ctypes.c_int32), ("q", ctypes.c_float), ("omega", ctypes.c_float),
         ("space_order", ctypes.c_int32), ("time_order", ctypes.c_int32),
-        ("flags", ctypes.c_int32),
+        ("flags", ctypes.c_int32), ("parallel_size_y", ctypes.c_int32),
     ]
 
 
@@ -55,6 +55,9 @@ class SolverConfig:
     space_order: int = 2
     time_order: int = 2
     flags: int = 0
+    # kParallelSizeY: > 1 makes this one radial slab of a box split over that
+    # many ranks (size_y: the slab's rows and margins; extent_y: the box's)
+    parallel_size_y: int = 1
 
     @property
     def shape(self):
@@ -77,13 +80,14 @@ class SolverConfig:
     def derived(self):
         """Spacings and extents exactly as the reference's float32 chains give them."""
         f = np.float32
-        g = (self.size_x, self.size_y - 2 * self.margin_y, self.size_z - 2 * self.margin_z)
+        loc = (self.size_x, self.size_y - 2 * self.margin_y, self.size_z - 2 * self.margin_z)
+        g = (loc[0], max(1, self.parallel_size_y) * loc[1], loc[2])
         s = (self.size_x, self.size_y, self.size_z)
         ext = (self.extent_x, self.extent_y, self.extent_z)
         out = {}
-        for name, gi, si, li in zip("xyz", g, s, ext):
+        for name, gi, si, li, ni in zip("xyz", g, s, ext, loc):
             comp_ext = f(f(f(li) / f(gi)) * f(si))          # kExtent
-            local_ext = f(f(f(li) / f(gi)) * f(gi))         # kLocalExtent
+            local_ext = f(f(f(li) / f(gi)) * f(ni))         # kLocalExtent
             out["extent_" + name] = comp_ext
             out["local_extent_" + name] = local_ext
             out["d" + name] = f(comp_ext / f(si))           # kD

@@ -209,6 +209,8 @@ nmhd_status validate(nmhd_solver *s, int nsteps, int ckpt, const nmhd_loss_spec 
     return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "loss window must satisfy 0 <= first <= last <= nsteps");
   if (s->cfg.size_y - 2 * s->cfg.margin_y < 1 || s->cfg.size_z - 2 * s->cfg.margin_z < 1)
     return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "no interior cells");
+  if (s->cfg.parallel_size_y > 1)
+    return set_err(s, NMHD_ERR_NOT_SUPPORTED, "the differentiated step covers a whole box, not a radial slab");
   return NMHD_OK;
 }
 

@@ -57,47 +57,85 @@ __device__ __forceinline__ void margin_cfl_cell(const GridParams &g, int idx, in
   }
 }
 
-// One item (sx, sy, sz), sy < M, of the shearing-periodic Y-margin fill
-// (communicate_gather/scatter_kernel_y, mhd_solver.inlrb:184-242, with
-// relative_displacement :244-259) for one rank: the bottom margin row sy takes
-// the top interior row Sy-2M+sy shifted by +d_int in x with vx - rel_vel; the
-// top margin row Sy-M+sy takes the bottom interior row M+sy shifted by
-// -d_int-1 with vx + rel_vel; By of row Sy-M is kept.  The reference's
-// two-point interpolation weights both multiply the same sample; that
-// arithmetic is kept.
-__device__ __forceinline__ void fill_y_item(const GridParams &g, double time, float *w, int idx) {
+// Integer and fractional shear displacement of the Y-margin exchange at time t
+// (relative_displacement, src/library/mhd_solver.inlrb:244-259): all double
+// except the float product fold * kExtentX.
+struct ShearShift {
+  int dint;
+  float f;
+};
+__device__ __forceinline__ ShearShift shear_shift(const GridParams &g, double time) {
+  const double d0 = 0.0 + time * g.rel_vel;
+  const int fold = (int)floor(d0 / (double)g.extent_x);
+  const double d1 = d0 - (double)((float)fold * g.extent_x);
+  ShearShift s;
+  s.dint = (int)floor(d1 / (double)g.dx);
+  s.f = (float)(d1 / (double)g.dx - s.dint);
+  return s;
+}
+
+// Gather half of the Y-margin exchange for item idx = (sz*M + sy)*Sx + sx,
+// sy < M (communicate_gather_kernel_y, mhd_solver.inlrb:184-222): field v of
+// the top interior row Sy-2M+sy shifted by +d_int in x with vx -
+// relative_velocity (`inc`, sent to the rank above) and of the bottom interior
+// row M+sy shifted by -d_int-1 with vx + relative_velocity (`dec`, sent to the
+// rank below).  The reference's two-point interpolation weights both multiply
+// the same sample; that arithmetic is kept.
+__device__ __forceinline__ void gather_y_item(const GridParams &g, const ShearShift &sh, const float *w,
+                                              int idx, float inc[8], float dec[8]) {
   const int M = g.my;
   const int sx = idx % g.sx;
   const int sy = (idx / g.sx) % M;
   const int sz = idx / (g.sx * M);
-  // relative_displacement(t): all double except the float product fold*kExtentX
-  const double d0 = 0.0 + time * g.rel_vel;
-  const int fold = (int)floor(d0 / (double)g.extent_x);
-  const double d1 = d0 - (double)((float)fold * g.extent_x);
-  const int dint = (int)floor(d1 / (double)g.dx);
-  const float f = (float)(d1 / (double)g.dx - dint);
   const float rv = (float)g.rel_vel;
-  const int inc_x = wrap((sx + dint) % g.sx, g.sx);
-  const int dec_x = wrap((sx - dint - 1) % g.sx, g.sx);
+  const int inc_x = wrap((sx + sh.dint) % g.sx, g.sx);
+  const int dec_x = wrap((sx - sh.dint - 1) % g.sx, g.sx);
   const size_t N = (size_t)g.n;
   const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + inc_x;
   const int src_dec = (sz * g.sy + (M + sy)) * g.sx + dec_x;
-  const int dst_lo = (sz * g.sy + sy) * g.sx + sx;
-  const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx;
-  const float omf = 1.0f - f;
+  const float omf = 1.0f - sh.f;
 #pragma unroll
   for (int v = 0; v < 8; ++v) {
     const float vi = w[v * N + src_inc];
     const float vd = w[v * N + src_dec];
-    float bi = omf * vi + f * vi;
-    float bd = f * vd + omf * vd;
+    float bi = omf * vi + sh.f * vi;
+    float bd = sh.f * vd + omf * vd;
     if (v == 1) {
       bi = bi - rv;
       bd = bd + rv;
     }
-    w[v * N + dst_lo] = bi;
-    if (!(v == 6 && sy == 0)) w[v * N + dst_hi] = bd;
+    inc[v] = bi;
+    dec[v] = bd;
   }
+}
+
+// Scatter half (communicate_scatter_kernel_y, mhd_solver.inlrb:224-242): the
+// bottom margin row sy takes `inc` (from the rank below), the top margin row
+// Sy-M+sy takes `dec` (from the rank above); By of row Sy-M (the interior's
+// upper face) is kept.
+__device__ __forceinline__ void scatter_y_item(const GridParams &g, float *w, int idx, const float inc[8],
+                                               const float dec[8]) {
+  const int M = g.my;
+  const int sx = idx % g.sx;
+  const int sy = (idx / g.sx) % M;
+  const int sz = idx / (g.sx * M);
+  const size_t N = (size_t)g.n;
+  const int dst_lo = (sz * g.sy + sy) * g.sx + sx;
+  const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    w[v * N + dst_lo] = inc[v];
+    if (!(v == 6 && sy == 0)) w[v * N + dst_hi] = dec[v];
+  }
+}
+
+// One item of the shearing-periodic Y-margin fill of a single box (one rank:
+// every message of the exchange goes to itself).  Reads only interior rows and
+// writes only margin rows, so it runs in place.
+__device__ __forceinline__ void fill_y_item(const GridParams &g, double time, float *w, int idx) {
+  float inc[8], dec[8];
+  gather_y_item(g, shear_shift(g, time), w, idx, inc, dec);
+  scatter_y_item(g, w, idx, inc, dec);
 }
 
 }  // namespace margin

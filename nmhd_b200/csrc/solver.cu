@@ -59,14 +59,18 @@ GridParams nmhd::derive_grid(const nmhd_config &c) {
   g.n = c.size_x * c.size_y * c.size_z;
   g.my = c.margin_y;
   g.mz = c.margin_z;
+  // A radial slab of a box split over P ranks along Y: kGlobalSizeY = P * the
+  // slab's interior rows, extent_y is the whole box's (kGlobalExtentY).
+  const int py = c.parallel_size_y > 1 ? c.parallel_size_y : 1;
   const int s[3] = {c.size_x, c.size_y, c.size_z};
-  const int gi[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int li[3] = {c.size_x, c.size_y - 2 * c.margin_y, c.size_z - 2 * c.margin_z};
+  const int gi[3] = {li[0], py * li[1], li[2]};
   const float L[3] = {c.extent_x, c.extent_y, c.extent_z};
   volatile float comp[3], local[3], d[3];
   for (int i = 0; i < 3; ++i) {
     volatile float per = L[i] / (float)gi[i];
     comp[i] = per * (float)s[i];
-    local[i] = per * (float)gi[i];
+    local[i] = per * (float)li[i];
     d[i] = comp[i] / (float)s[i];
   }
   g.dx = d[0];
@@ -80,8 +84,9 @@ GridParams nmhd::derive_grid(const nmhd_config &c) {
   g.omega = c.omega;
   volatile float qo = -c.q * c.omega;
   volatile float rv = qo * local[1];
-  g.rel_vel = (double)rv;
   g.shear = c.problem == NMHD_PROBLEM_SHEARING_BOX;
+  // relative_velocity() hook: zero without a shearing box
+  g.rel_vel = g.shear ? (double)rv : 0.0;
   g.order2 = c.space_order != 1;
   auto pow2 = [](float v) {
     int e;
@@ -113,6 +118,10 @@ nmhd_status validate(const nmhd_config *c, std::string &why) {
   if (c->problem != NMHD_PROBLEM_NONE && c->problem != NMHD_PROBLEM_SHEARING_BOX) { why = "unknown problem"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->space_order != 1 && c->space_order != 2) { why = "space_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->time_order != 1 && c->time_order != 2) { why = "time_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->parallel_size_y < 0) { why = "parallel_size_y must be >= 0"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->parallel_size_y > 1 && c->margin_y < 1) {
+    why = "a radial slab (parallel_size_y > 1) needs margin_y >= 1"; return NMHD_ERR_INVALID_ARGUMENT;
+  }
   return NMHD_OK;
 }
 
@@ -341,6 +350,8 @@ nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limi
                          int64_t *steps_done) {
   if (steps_done) *steps_done = 0;
   if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (s->cfg.parallel_size_y > 1)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
   const auto t0 = std::chrono::steady_clock::now();
   StepCtl h;
   nmhd_status st = read_ctl(s, h);
@@ -473,6 +484,8 @@ const char *nmhd_kernel_name(int i) {
 
 int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max) {
   if (!s || !ms_out || steps <= 0 || max <= 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  if (s->cfg.parallel_size_y > 1)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
   StepCtl h;
   nmhd_status st = read_ctl(s, h);
   if (st != NMHD_OK) return st;
@@ -605,6 +618,8 @@ std::map<TuneKey, TuneChoice> g_tune_cache;
 
 int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials) {
   if (!s || steps <= 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  if (s->cfg.parallel_size_y > 1)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
   const GridParams &g = s->g;
   const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order, s->cfg.time_order};
   std::vector<TuneChoice> cands;
@@ -704,6 +719,95 @@ nmhd_status nmhd_set_stream(nmhd_solver *s, void *cuda_stream) {
     s->stream = (cudaStream_t)cuda_stream;
   }
   return NMHD_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Split-phase step of a radial slab (MHDSolver::proceed with kParallelSizeY
+// ranks, mhd_solver.inlrb:850-993, communicate() :283-493).
+
+int64_t nmhd_halo_count(const nmhd_solver *s) {
+  return s ? (int64_t)8 * s->g.sx * s->g.my * s->g.sz : -1;
+}
+
+nmhd_status nmhd_slab_begin(nmhd_solver *s, double goal_time) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (h.status) return fail(s, NMHD_ERR_NUMERICAL, "state is not valid (set a new state)");
+  h.goal = (float)goal_time;
+  h.done = 0;
+  if (!s->cfl_ready) {
+    h.cfl_cur = h.cfl_next = 0x7f800000u;
+    h.blocks_done = 0;
+  }
+  return write_ctl(s, h);
+}
+
+nmhd_status nmhd_halo_pack(nmhd_solver *s, float *send_inc, float *send_dec) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (s->g.my > 0 && (!send_inc || !send_dec)) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL halo buffer");
+  nmhd::launch_halo_pack(s->g, s->ctl, s->w0, s->w1, send_inc, send_dec, s->stream);
+  NMHD_CUDA(s, cudaGetLastError());
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_halo_unpack(nmhd_solver *s, const float *recv_inc, const float *recv_dec) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (s->g.my > 0 && (!recv_inc || !recv_dec)) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL halo buffer");
+  nmhd::launch_halo_unpack(s->g, s->ctl, s->w0, s->w1, recv_inc, recv_dec, s->stream);
+  // the CFL time of this slab: every cell after a state change, else the
+  // margin set (the interior was reduced by the previous step's final stage)
+  if (!s->cfl_ready) {
+    nmhd::launch_cfl_all(s->g, s->ctl, s->w0, s->w1, s->stream);
+    s->cfl_ready = true;
+  } else {
+    nmhd::launch_cfl_margin(s->g, s->ctl, s->w0, s->w1, s->stream);
+  }
+  NMHD_CUDA(s, cudaGetLastError());
+  return NMHD_OK;
+}
+
+float *nmhd_cfl_slot(nmhd_solver *s) { return s ? reinterpret_cast<float *>(&s->ctl->cfl_cur) : nullptr; }
+
+nmhd_status nmhd_cfl_min(nmhd_solver *const *slabs, int n) {
+  if (!slabs || n < 1 || n > nmhd::kMaxSlots) return fail(nullptr, NMHD_ERR_INVALID_ARGUMENT, "bad slab list");
+  nmhd::CflSlots slots;
+  slots.n = n;
+  for (int i = 0; i < n; ++i) {
+    if (!slabs[i] || slabs[i]->device != slabs[0]->device || slabs[i]->stream != slabs[0]->stream)
+      return fail(slabs[0], NMHD_ERR_INVALID_ARGUMENT, "slabs must share one device and one stream");
+    slots.p[i] = nmhd_cfl_slot(slabs[i]);
+  }
+  nmhd::launch_cfl_min(slots, slabs[0]->stream);
+  NMHD_CUDA(slabs[0], cudaGetLastError());
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_step_stages(nmhd_solver *s) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (s->cfg.time_order == 1) {
+    enqueue_stage(s, 0, 1, 0, 1, s->stream);
+  } else {
+    enqueue_stage(s, 0, 2, 1, 0, s->stream);
+    enqueue_stage(s, 2, 1, 0, 1, s->stream);
+  }
+  NMHD_CUDA(s, cudaGetLastError());
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_slab_poll(nmhd_solver *s, int64_t *generation, double *time) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  StepCtl h;
+  nmhd_status st = read_ctl(s, h);
+  if (st != NMHD_OK) return st;
+  if (generation) *generation = h.generation;
+  if (time) *time = h.time;
+  if (h.status)
+    return fail(s, NMHD_ERR_NUMERICAL,
+                (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
+                                                : "non-finite state, density <= 0 or pressure <= 0");
+  return h.done ? NMHD_GOAL_REACHED : NMHD_OK;
 }
 
 const char *nmhd_last_error(const nmhd_solver *s) {

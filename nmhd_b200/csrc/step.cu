@@ -150,6 +150,52 @@ __global__ void __launch_bounds__(kBlock) k_fill_y(GridParams g, StepCtl *ctl, f
   margin::fill_y_item(g, ctl->time, w, idx);
 }
 
+// Halo exchange of a radial slab (kParallelSizeY > 1), split around the
+// caller's transport: k_halo_pack gathers this slab's shear-shifted boundary
+// rows into the two outgoing messages, k_halo_unpack scatters the two
+// incoming messages into the Y margins.  Message layout (the reference's
+// mpi_buffer_y_*): field v of item (sz*M + sy)*Sx + sx at v*Sx*M*Sz + item.
+__global__ void __launch_bounds__(kBlock) k_halo_pack(GridParams g, StepCtl *ctl, const float *w0,
+                                                      const float *w1, float *send_inc, float *send_dec) {
+  if (ctl->done) return;
+  const float *w = ctl->parity ? w1 : w0;
+  const int unit = g.sx * g.my * g.sz;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= unit) return;
+  float inc[8], dec[8];
+  margin::gather_y_item(g, margin::shear_shift(g, ctl->time), w, idx, inc, dec);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    send_inc[(size_t)v * unit + idx] = inc[v];
+    send_dec[(size_t)v * unit + idx] = dec[v];
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) k_halo_unpack(GridParams g, StepCtl *ctl, float *w0, float *w1,
+                                                        const float *recv_inc, const float *recv_dec) {
+  if (ctl->done) return;
+  float *w = ctl->parity ? w1 : w0;
+  const int unit = g.sx * g.my * g.sz;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= unit) return;
+  float inc[8], dec[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    inc[v] = recv_inc[(size_t)v * unit + idx];
+    dec[v] = recv_dec[(size_t)v * unit + idx];
+  }
+  margin::scatter_y_item(g, w, idx, inc, dec);
+}
+
+// Minimum of the CFL times of n slabs of one process (the MPI_Allreduce MIN of
+// proceed(), mhd_solver.inlrb:870-893), written back to every slab.
+__global__ void k_cfl_min(CflSlots slots) {
+  if (threadIdx.x != 0) return;
+  float m = *slots.p[0];
+  for (int i = 1; i < slots.n; ++i) m = fminf(m, *slots.p[i]);
+  for (int i = 0; i < slots.n; ++i) *slots.p[i] = m;
+}
+
 // Plain periodic Z-margin copy (the Z part of communicate(), mhd_solver.inlrb:384-402, 463-480).
 __global__ void __launch_bounds__(kBlock) k_fill_z(GridParams g, StepCtl *ctl, float *w0, float *w1) {
   if (ctl->done) return;
@@ -532,6 +578,22 @@ void launch_fill(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaSt
   if (g.my > 0) k_fill_y<<<blocks_for((long long)g.sx * g.my * g.sz), kBlock, 0, st>>>(g, ctl, w0, w1);
   if (g.mz > 0) k_fill_z<<<blocks_for((long long)g.sx * g.sy * g.mz), kBlock, 0, st>>>(g, ctl, w0, w1);
 }
+
+void launch_halo_pack(const GridParams &g, StepCtl *ctl, const float *w0, const float *w1, float *send_inc,
+                      float *send_dec, cudaStream_t st) {
+  if (g.my > 0)
+    k_halo_pack<<<blocks_for((long long)g.sx * g.my * g.sz), kBlock, 0, st>>>(g, ctl, w0, w1, send_inc, send_dec);
+}
+
+void launch_halo_unpack(const GridParams &g, StepCtl *ctl, float *w0, float *w1, const float *recv_inc,
+                        const float *recv_dec, cudaStream_t st) {
+  if (g.my > 0)
+    k_halo_unpack<<<blocks_for((long long)g.sx * g.my * g.sz), kBlock, 0, st>>>(g, ctl, w0, w1, recv_inc,
+                                                                              recv_dec);
+  if (g.mz > 0) k_fill_z<<<blocks_for((long long)g.sx * g.sy * g.mz), kBlock, 0, st>>>(g, ctl, w0, w1);
+}
+
+void launch_cfl_min(const CflSlots &slots, cudaStream_t st) { k_cfl_min<<<1, 32, 0, st>>>(slots); }
 
 void launch_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                  int in_sel, int half, cudaStream_t st) {

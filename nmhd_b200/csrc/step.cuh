@@ -57,6 +57,19 @@ constexpr int kFluxFields = 21;  // 3 face directions x 7 flux components
 void launch_cfl_all(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
 void launch_cfl_margin(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
 void launch_fill(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
+// Radial slab halo: gather the outgoing Y-boundary messages / scatter the
+// incoming ones into the Y margins and copy the Z margins.
+void launch_halo_pack(const GridParams &g, StepCtl *ctl, const float *w0, const float *w1, float *send_inc,
+                      float *send_dec, cudaStream_t stream);
+void launch_halo_unpack(const GridParams &g, StepCtl *ctl, float *w0, float *w1, const float *recv_inc,
+                        const float *recv_dec, cudaStream_t stream);
+// CFL-time slots (StepCtl::cfl_cur as float) of the slabs of one process.
+constexpr int kMaxSlots = 64;
+struct CflSlots {
+  float *p[kMaxSlots];
+  int n;
+};
+void launch_cfl_min(const CflSlots &slots, cudaStream_t stream);
 // One RK stage: fluxes from buffer `in_sel`, conserved state from the current
 // buffer, result into `out_sel` (0 current, 1 next, 2 predictor); `half`
 // selects dt/2; `final_stage` reduces the next CFL time and advances the clock.

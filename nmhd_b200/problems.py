@@ -101,6 +101,41 @@ def shearing_box(n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0, l_a
     return cfg, state.astype(np.float32)
 
 
+def shearing_box_slabs(n_slabs, n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0,
+                       l_azimuthal=4.0, l_vertical=1.0, q=1.5, omega=1.0, beta=400.0, density=1.0,
+                       pressure=1.0, gamma=5.0 / 3.0, cfl=0.4, noise=0.01, seed=1, margin=4):
+    """The box of :func:`shearing_box` split into ``n_slabs`` radial slabs, as
+    the reference's ranks along Y hold it: each slab in its own frame (v_X =
+    -q Omega y with y measured from the slab's own margin-inclusive centre),
+    the noise of the whole box (same seed and draw) cut into the slabs' rows.
+    Returns (one slab's config, [state of rank 0, ..., rank n_slabs - 1])."""
+    from .slab import slab_config
+    whole, _ = shearing_box(n_radial=n_radial, n_azimuthal=n_azimuthal, n_vertical=n_vertical,
+                            l_radial=l_radial, l_azimuthal=l_azimuthal, l_vertical=l_vertical, q=q,
+                            omega=omega, beta=beta, density=density, pressure=pressure, gamma=gamma,
+                            cfl=cfl, noise=0.0, seed=seed, margin=margin)
+    cfg = slab_config(whole, n_slabs)
+    d = cfg.derived()
+    rows = n_radial // n_slabs
+    sx, sy, sz = cfg.size_x, cfg.size_y, cfg.size_z
+    y_idx = np.arange(sy, dtype=np.float32)
+    y_loc = np.float32(d["corner_y"]) + np.float32(d["dy"]) * (y_idx + np.float32(0.5))
+    v_shear = (np.float32(-q) * np.float32(omega)) * y_loc
+    cs = math.sqrt(gamma * pressure / density)
+    rng = np.random.Generator(np.random.PCG64(seed))
+    pert = rng.uniform(-noise, noise, size=(3, sz, n_radial, sx)) * cs
+    states = []
+    for r in range(n_slabs):
+        state = np.zeros((8, sz, sy, sx), dtype=np.float64)
+        state[0] = density
+        state[4] = pressure
+        state[1] = v_shear.astype(np.float64)[None, :, None]
+        state[7] = math.sqrt(2.0 * pressure / beta)
+        state[1:4, :, margin:margin + rows, :] += pert[:, :, r * rows:(r + 1) * rows, :]
+        states.append(state.astype(np.float32))
+    return cfg, states
+
+
 def mri_ensemble(n_boxes=64, seed=0, sides=(32, 48, 64, 96), ratios=(2, 3, 4), beta_range=(1e2, 1e4),
                  q_range=(1.2, 1.8), noise=0.01, margin=4):
     """Ensemble of independent MRI shearing boxes of uneven sizes.

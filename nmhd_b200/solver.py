@@ -164,16 +164,16 @@ class MHDSolver:
         }
 
     # -- checkpoint ------------------------------------------------------
-    def save_state(self, prefix) -> bool:
+    def save_state(self, prefix, rank=0) -> bool:
         """MHDSolver::save_state (src/library/mhd_solver.inlrb:1023-1036):
         ``prefix.bin`` plus ``prefix_setup.txt`` in the reference's pod text
         (see :mod:`nmhd_b200.checkpoint`); the reference's load_state reads
-        both."""
+        both.  ``rank``: this solver's rank when it is a radial slab."""
         prefix = str(prefix)
         if not self.write(prefix + ".bin"):
             return False
         text = checkpoint.setup_text(self.config, self.generation(), self.current_time(),
-                                     output_directory=os.path.dirname(os.path.abspath(prefix)))
+                                     output_directory=os.path.dirname(os.path.abspath(prefix)), rank=rank)
         try:
             with open(prefix + "_setup.txt", "w") as fp:
                 fp.write(text)

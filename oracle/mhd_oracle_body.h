@@ -58,7 +58,9 @@ static void FN(derive)(const oracle_config *c, FN(consts) *k) {
   k->cfl = (real)c->cfl;
   k->q = (real)c->q;
   k->omega = (real)c->omega;
-  k->rel_vel = (double)((real)(-k->q * k->omega) * local_ext[1]);
+  /* relative_velocity() hook: the Kepler app's (kepler_disk_demo/mhd_solver.curb:50-52),
+     zero without a shearing box */
+  k->rel_vel = c->problem == 1 ? (double)((real)(-k->q * k->omega) * local_ext[1]) : 0.0;
 }
 
 /* ---- minbee reconstruction (src/library/mhd_solver.inlrb:140-155) -------- */

@@ -130,3 +130,52 @@ def run_ref(name, state, steps, goal_time=1.0e30, threads=None, dtype=np.float32
         out = read_bin(fout, dtype=dtype)
         times = np.loadtxt(ftimes, ndmin=1)
     return out, times, info
+
+
+def run_ref_slabs(name, states, steps, goal_time=1.0e30, threads=1, dtype=np.float32, timeout=600,
+                  ckpt_dir=None, save_tag=None):
+    """Run the reference binary ``name`` (built with NMHD_REF_PY = len(states)
+    ranks along Y) as one process per rank, rank r starting from
+    ``states[r]`` (its radial slab, margins included), until generation
+    ``steps``.  The ranks exchange their halos and reduce dt through the
+    file mailbox of refshim/mpi.h.  With ``ckpt_dir`` and ``save_tag`` every
+    rank ends with save_state(save_tag) under ckpt_dir/<tag>/.  Returns
+    (per-rank states, times of rank 0, per-rank infos)."""
+    from nmhd_b200.binio import read_bin, write_bin
+    exe = ref_binary(name)
+    if exe is None:
+        raise FileNotFoundError(f"reference binary ref_{name} is not built")
+    n = len(states)
+    with tempfile.TemporaryDirectory() as d:
+        box = os.path.join(d, "mailbox")
+        logs = str(ckpt_dir) if ckpt_dir else os.path.join(d, "logs")
+        os.makedirs(box)
+        os.makedirs(logs, exist_ok=True)
+        for r, s in enumerate(states):
+            write_bin(os.path.join(d, "in%04d.bin" % r), s, dtype=dtype)
+        procs = []
+        for r in range(n):
+            env = dict(os.environ, NMHD_REF_RANK=str(r), NMHD_REF_NRANKS=str(n), NMHD_REF_MAILBOX=box,
+                       NMHD_REF_DIR=logs, NMHD_REF_MPI_TIMEOUT=str(timeout), OMP_NUM_THREADS=str(threads))
+            if save_tag:
+                env["NMHD_REF_SAVE"] = save_tag
+            procs.append(subprocess.Popen(
+                [exe, os.path.join(d, "in%04d.bin"), os.path.join(d, "out%04d.bin"), str(steps),
+                 repr(float(goal_time)), os.path.join(d, "t%04d.txt")],
+                stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True, env=env))
+        outs = []
+        for p in procs:
+            try:
+                o, e = p.communicate(timeout=timeout + 60)
+            except subprocess.TimeoutExpired:
+                for q in procs:
+                    q.kill()
+                raise
+            outs.append((p.returncode, o, e))
+        for r, (rc, o, e) in enumerate(outs):
+            if rc != 0:
+                raise RuntimeError(f"reference rank {r} exited {rc}: {e.strip()[-400:]}")
+        infos = [json.loads(o.strip().splitlines()[-1]) for _, o, _ in outs]
+        res = [read_bin(os.path.join(d, "out%04d.bin" % r), dtype=dtype) for r in range(n)]
+        times = np.loadtxt(os.path.join(d, "t0000.txt"), ndmin=1)
+    return res, times, infos

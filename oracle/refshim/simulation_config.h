@@ -5,11 +5,13 @@
 // simulation_config.h (defaults: src/library/simulation_config_default.h;
 // per-application overrides: src/application/*/simulation_config.hrb).  This
 // file provides the same names, filled from -D macros by oracle/Makefile, for
-// one rank (kParallelSize* == 1), fully periodic addressing, and margins in Y
-// (the shearing direction) and optionally Z.
+// NMHD_REF_PY ranks along Y (default 1; kParallelSize{X,Z} == 1), fully
+// periodic addressing, and margins in Y (the shearing direction) and
+// optionally Z.
 //
 //   NMHD_REF_DOUBLE   0: Real = float (USE_SINGLE_PRECISION), 1: Real = double
-//   NMHD_REF_G{X,Y,Z} interior cell counts (kGlobalSize*)
+//   NMHD_REF_G{X,Y,Z} interior cell counts of the whole box (kGlobalSize*)
+//   NMHD_REF_PY       ranks along Y (kParallelSizeY), each a radial slab
 //   NMHD_REF_M{Y,Z}   margin widths (kMarginSize*)
 //   NMHD_REF_L{X,Y,Z} global extents (kGlobalExtent*)
 //   NMHD_REF_GAMMA    kGamma expression, e.g. (5.0f/3.0f)
@@ -47,10 +49,13 @@ const int kGlobalSizeX = NMHD_REF_GX;
 const int kGlobalSizeY = NMHD_REF_GY;
 const int kGlobalSizeZ = NMHD_REF_GZ;
 
+#ifndef NMHD_REF_PY
+#define NMHD_REF_PY 1
+#endif
 const int kParallelSizeX = 1;
-const int kParallelSizeY = 1;
+const int kParallelSizeY = NMHD_REF_PY;
 const int kParallelSizeZ = 1;
-const int kParallelSize = 1;
+const int kParallelSize = NMHD_REF_PY;
 
 const int kMarginSizeX = 0;
 const int kMarginSizeY = NMHD_REF_MY;

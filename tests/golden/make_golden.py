@@ -19,7 +19,7 @@ import numpy as np
 ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
 sys.path.insert(0, ROOT)
 
-from nmhd_b200.problems import orszag_tang_3d, shearing_box  # noqa: E402
+from nmhd_b200.problems import orszag_tang_3d, shearing_box, shearing_box_slabs  # noqa: E402
 from oracle import oracle  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -38,6 +38,32 @@ CASES = {
 }
 
 
+# Radial slab decompositions, run as one reference process per rank
+# (oracle.run_ref_slabs).  name -> (binary, slab builder, steps, store outputs)
+# Without stored outputs the fixture keeps each rank's SHA-256 (bitwise parity
+# needs no more).
+SLAB_CASES = {
+    "shear32x16x8_p2": ("shear32x16x8_p2",
+                        lambda: shearing_box_slabs(2, n_radial=16, n_azimuthal=32, n_vertical=8,
+                                                   l_azimuthal=4.0, seed=3), 10, True),
+    "shear32x16x8_p4": ("shear32x16x8_p4",
+                        lambda: shearing_box_slabs(4, n_radial=16, n_azimuthal=32, n_vertical=8,
+                                                   l_azimuthal=4.0, seed=4), 10, False),
+    "shear48x24x12_p3": ("shear48x24x12_p3",
+                         lambda: shearing_box_slabs(3, n_radial=24, n_azimuthal=48, n_vertical=12,
+                                                    l_radial=1.5, l_azimuthal=2.0, seed=5), 8, False),
+    "shear64x32x16_mz_p2": ("shear64x32x16_mz_p2", lambda: _z_margins(shearing_box_slabs(
+        2, n_radial=32, n_azimuthal=64, n_vertical=16, l_azimuthal=4.0, seed=6)), 6, False),
+}
+
+
+def _z_margins(slabs, m=4):
+    """The slabs with m periodic Z-margin planes on each side."""
+    cfg, states = slabs
+    cfg.margin_z, cfg.size_z = m, cfg.size_z + 2 * m
+    return cfg, [np.concatenate([s[:, -m:], s, s[:, :m]], axis=1) for s in states]
+
+
 def digest(a):
     return hashlib.sha256(np.ascontiguousarray(a).tobytes()).hexdigest()
 
@@ -53,6 +79,16 @@ def main():
             payload["input"] = state
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **payload)
         print(name, info)
+    for name, (binary, make, steps, keep) in SLAB_CASES.items():
+        cfg, states = make()
+        outs, times, infos = oracle.run_ref_slabs(binary, states, steps)
+        payload = {"times": times, "steps": np.int64(infos[0]["steps"]),
+                   "output_sha256": np.array([digest(o) for o in outs]),
+                   "input_sha256": np.array([digest(s) for s in states])}
+        if keep:
+            payload["output"] = np.stack(outs)
+        np.savez_compressed(os.path.join(HERE, name + ".npz"), **payload)
+        print(name, infos[0])
 
 
 if __name__ == "__main__":

@@ -45,9 +45,23 @@ def test_create_rejects_bad_config_without_touching_the_gpu():
     assert L.nmhd_create(ctypes.byref(bad), ctypes.byref(h)) == -1
 
 
-def test_config_struct_layout_matches_header():
-    # 16 four-byte fields, no padding
-    assert ctypes.sizeof(NmhdConfig) == 64
+def test_config_struct_layout_matches_header(tmp_path):
+    """Size and every field offset of nmhd_config as the C compiler lays it
+    out from include/nmhd.h, against the ctypes mirror."""
+    import subprocess
+    names = [f[0] for f in NmhdConfig._fields_]
+    src = tmp_path / "layout.c"
+    src.write_text("#include <stdio.h>\n#include <stddef.h>\n#include \"nmhd.h\"\nint main(void) {\n"
+                   '  printf("%zu\\n", sizeof(nmhd_config));\n'
+                   + "".join('  printf("%%zu\\n", offsetof(nmhd_config, %s));\n' % n for n in names)
+                   + "  return 0;\n}\n")
+    exe = tmp_path / "layout"
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    subprocess.run(["gcc", "-I" + os.path.join(root, "include"), str(src), "-o", str(exe)], check=True)
+    got = [int(v) for v in subprocess.run([str(exe)], check=True, capture_output=True,
+                                          text=True).stdout.split()]
+    assert got[0] == ctypes.sizeof(NmhdConfig)
+    assert got[1:] == [getattr(NmhdConfig, n).offset for n in names]
 
 
 def test_derived_constants_follow_reference_float_chains():
