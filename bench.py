@@ -51,6 +51,11 @@ ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0),
 # 100..115) with eps = 1e-3 relative to the velocity noise.
 ADJOINTS = {"mri_adjoint_64": dict(n=64, seed=2, steps=200, window=(151, 200), ckpt=20, fd_dirs=16,
                                    fd_eps=1e-3, tlm_dirs=4)}
+# Radial slab decomposition of one box (strong scaling): rank r of N holds
+# radial slab r of the named box, halos over NCCL point-to-point, dt by an
+# NCCL all-reduce (nmhd_b200.slab.DistributedSlab).
+SLABS = {"mri_slabs_128x256x64": "mri_shearing_box_128x256x64",
+         "mri_slabs_512x1024x256": "mri_shearing_box_512x1024x256"}
 BYTES_PER_CELL_UPDATE = 160  # 8 FP32 state words: stage 1 read+write, stage 2 2x read + write
 
 
@@ -145,9 +150,16 @@ def cpu_sample(workload, budget_s=12.0):
             "sample": f"{steps} full RK2 steps of {workload} ({secs:.1f} s, OpenMP {threads} threads)"}
 
 
-def dist_setup(n_gpus):
+def dist_setup(n_gpus, force=False):
     import torch
     import torch.distributed as dist
+    if force and "RANK" not in os.environ and n_gpus == 1:
+        # a one-rank process group (the slab arm's transport needs one)
+        os.environ.update(RANK="0", WORLD_SIZE="1", LOCAL_RANK="0", MASTER_ADDR="127.0.0.1")
+        import socket
+        with socket.socket() as so:
+            so.bind(("127.0.0.1", 0))
+            os.environ.setdefault("MASTER_PORT", str(so.getsockname()[1]))
     if n_gpus > 1 or "RANK" in os.environ:
         os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
         rank = int(os.environ.get("RANK", 0))
@@ -168,7 +180,15 @@ def run_reference_arm(args):
         if dist:
             dist.destroy_process_group()
         return
-    wl = args.workload
+    # a slab workload's reference arm is the whole box on the host cores
+    wl = SLABS.get(args.workload, args.workload)
+    if wl not in WORKLOADS:
+        why = ("the reference has no batched ensemble; its sizes are compile-time constants"
+               if wl in ENSEMBLES else "the reference has no differentiated step")
+        print(json.dumps({"impl": "reference", "unavailable": why}), flush=True)
+        if dist:
+            dist.destroy_process_group()
+        return
     cpu_reference_run(wl, max(1, min(args.warmup, 2)))
     # bounded: at most ~90 s of timed CPU work
     _, _, secs1, _, _ = cpu_reference_run(wl, 1)
@@ -384,6 +404,85 @@ def run_ensemble_arm(args):
         dist.destroy_process_group()
 
 
+def run_slab_arm(args):
+    """One box split into N radial slabs, one per GPU (strong scaling): the
+    split-phase step with NCCL halos and dt all-reduce, interior
+    cell-updates/s of the whole box."""
+    import torch
+    from nmhd_b200.problems import shearing_box_slabs
+    from nmhd_b200.slab import DistributedSlab, SolverBackend
+    from nmhd_b200.solver import MHDSolver
+
+    rank, world, local, dist = dist_setup(args.gpus, force=True)
+    dev = torch.device("cuda", local)
+    wl = SLABS[args.workload]
+    cfg, states = shearing_box_slabs(world, only=rank, **WORKLOADS[wl])
+    sol = MHDSolver(cfg)
+    backend = SolverBackend(sol, dev)
+    sol.set_state(states[0])
+    slab = DistributedSlab(backend)
+    stream = torch.cuda.current_stream(dev)
+    slab.proceed(math.inf, max_steps=args.warmup)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    with ClockSampler(dev.index) as clocks:
+        start.record(stream)
+        slab.proceed(math.inf, max_steps=args.steps)
+        end.record(stream)
+        torch.cuda.synchronize(dev)
+    dist.barrier()
+    t = torch.tensor([start.elapsed_time(end)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    ms = float(t.item())
+    cells = cfg.interior_cells * world
+    value = cells * args.steps / (ms * 1e-3) / 1e6
+    # end to end: this rank's slab in from pinned host memory, K steps, out
+    host = torch.empty((8,) + cfg.shape, dtype=torch.float32, pin_memory=True).numpy()
+    host[...] = states[0]
+    del states
+    dist.barrier()
+    torch.cuda.synchronize(dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sol.set_state(host)
+    slab.proceed(math.inf, max_steps=args.steps)
+    sol.get_state(host)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    e2e_ms = float(t.item())
+    state_bytes = 8 * 4 * cfg.cells * world
+    halo_bytes = 2 * 4 * backend.halo_count()
+    if rank == 0:
+        peak, peak_kind = load_peaks()
+        achieved = BYTES_PER_CELL_UPDATE * cells / world / (ms / args.steps * 1e-3) / 1e9
+        line = {
+            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic (seeded shearing-box noise)",
+            "config": {"workload": args.workload, "box": wl, "cells_interior": cells,
+                       "parallelism": "radial slabs over %d GPU(s)" % world,
+                       "slab": [cfg.size_x, cfg.size_y, cfg.size_z],
+                       "halo_bytes_per_rank_per_step": halo_bytes,
+                       "l2": "working set per step (state x3 + fluxes) > 126 MB L2"},
+            "e2e": {"value": cells * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+                    "h2d_bytes_per_step": state_bytes / args.steps,
+                    "d2h_bytes_per_step": state_bytes / args.steps,
+                    "note": "set_state(pinned host) + K slab steps + get_state(pinned host), per step"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
+                         "unit_of_work": "one RK2 step of one slab (whole-step time); 160 B per cell-update"},
+            "gpu_launches": 7 * args.steps,
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    sol.close()
+    dist.destroy_process_group()
+
+
 def run_adjoint_arm(args):
     """Adjoint / forward time ratio on the 64^3 shearing box, with the
     gradient's checks: central differences of the FP32 and FP64 losses along
@@ -536,7 +635,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="nmhd", choices=["nmhd", "reference"])
     ap.add_argument("--workload", default="mri_shearing_box_128x256x64",
-                    choices=sorted(WORKLOADS) + sorted(ENSEMBLES) + sorted(ADJOINTS))
+                    choices=sorted(WORKLOADS) + sorted(ENSEMBLES) + sorted(ADJOINTS) + sorted(SLABS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
@@ -549,6 +648,8 @@ def main():
         run_ensemble_arm(args)
     elif args.workload in ADJOINTS:
         run_adjoint_arm(args)
+    elif args.workload in SLABS:
+        run_slab_arm(args)
     else:
         run_gpu_arm(args)
 

@@ -103,12 +103,13 @@ def shearing_box(n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0, l_a
 
 def shearing_box_slabs(n_slabs, n_radial=128, n_azimuthal=256, n_vertical=64, l_radial=1.0,
                        l_azimuthal=4.0, l_vertical=1.0, q=1.5, omega=1.0, beta=400.0, density=1.0,
-                       pressure=1.0, gamma=5.0 / 3.0, cfl=0.4, noise=0.01, seed=1, margin=4):
+                       pressure=1.0, gamma=5.0 / 3.0, cfl=0.4, noise=0.01, seed=1, margin=4, only=None):
     """The box of :func:`shearing_box` split into ``n_slabs`` radial slabs, as
     the reference's ranks along Y hold it: each slab in its own frame (v_X =
     -q Omega y with y measured from the slab's own margin-inclusive centre),
     the noise of the whole box (same seed and draw) cut into the slabs' rows.
-    Returns (one slab's config, [state of rank 0, ..., rank n_slabs - 1])."""
+    Returns (one slab's config, [state of rank 0, ..., rank n_slabs - 1]);
+    with ``only`` = r the list holds rank r's state alone."""
     from .slab import slab_config
     whole, _ = shearing_box(n_radial=n_radial, n_azimuthal=n_azimuthal, n_vertical=n_vertical,
                             l_radial=l_radial, l_azimuthal=l_azimuthal, l_vertical=l_vertical, q=q,
@@ -125,7 +126,7 @@ def shearing_box_slabs(n_slabs, n_radial=128, n_azimuthal=256, n_vertical=64, l_
     rng = np.random.Generator(np.random.PCG64(seed))
     pert = rng.uniform(-noise, noise, size=(3, sz, n_radial, sx)) * cs
     states = []
-    for r in range(n_slabs):
+    for r in range(n_slabs) if only is None else [only]:
         state = np.zeros((8, sz, sy, sx), dtype=np.float64)
         state[0] = density
         state[4] = pressure

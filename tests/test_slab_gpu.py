@@ -124,3 +124,36 @@ def test_distributed_slab_one_rank_nccl(gpu):
         ref.set_state(s)
         ref.step(21)
         assert np.array_equal(got, ref.get_state()) and t == ref.current_time()
+
+
+def test_slab_snapshot_is_the_reference_snapshot(gpu, tmp_path):
+    """save_state of every slab writes the reference's P-rank snapshot folder:
+    the same .bin bytes as the reference's ranks after the same steps, and
+    setup texts equal to theirs plus the exact-time member; the reference's
+    to_gnuplot reads it like its own."""
+    import subprocess
+    name = "shear48x24x12_p3"
+    if oracle.ref_binary(name) is None:
+        pytest.skip(f"reference binary ref_{name} not built")
+    cfg, states = SLAB_CASES[name][0]()
+    grp = SlabGroup(cfg, states)
+    try:
+        grp.step(6)
+        assert grp.save_state(tmp_path / "ours", "c")
+    finally:
+        grp.close()
+    oracle.run_ref_slabs(name, states, 6, ckpt_dir=tmp_path / "ref", save_tag="c")
+    for r in range(3):
+        a = (tmp_path / "ours" / "c" / ("%04d.bin" % r)).read_bytes()
+        b = (tmp_path / "ref" / "c" / ("%04d.bin" % r)).read_bytes()
+        assert a == b, f"rank {r}"
+        ours = (tmp_path / "ours" / "c" / ("%04d_setup.txt" % r)).read_text().splitlines()
+        ref = (tmp_path / "ref" / "c" / ("%04d_setup.txt" % r)).read_text().splitlines()
+        keep = lambda lines: [x for x in lines if not x.startswith(("current_time_exact", "output_directory"))
+                              and x not in ("20", "21")]
+        assert keep(ours) == keep(ref), f"rank {r}"
+    tg = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "oracle", "_ref", "to_gnuplot")
+    if os.path.exists(tg):
+        a = subprocess.run([tg, str(tmp_path / "ours" / "c")], check=True, capture_output=True, text=True).stdout
+        b = subprocess.run([tg, str(tmp_path / "ref" / "c")], check=True, capture_output=True, text=True).stdout
+        assert a == b
