@@ -540,7 +540,9 @@ def run_adjoint_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing box)",
         "config": {"workload": args.workload, "cells_interior": cfg.interior_cells,
                    "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
-                   "ckpt_every": K, "parallelism": "replicas" if world > 1 else "single"},
+                   "ckpt_every": K, "segments_kept_on_tape": sol.adjoint_kept_segments(),
+                   "segments": -(-steps // K),
+                   "parallelism": "replicas" if world > 1 else "single"},
         "forward_ms": fwd_ms, "adjoint_total_ms": tot, "adjoint_reverse_ms": rev,
         "reverse_over_forward": rev / fwd_ms, "phases_ms": adj[-1], "loss": J,
         "clocks": clocks.summary(),

@@ -264,6 +264,16 @@ nmhd_status nmhd_adjoint_run_f64(nmhd_solver *s, int32_t nsteps, int32_t ckpt_ev
  * float rounding (shift is ignored when dir is NULL).  dt_seq is required. */
 nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *loss, const float *dt_seq,
                          const double *const dir[8], double shift, double *loss_out, double *dloss_out);
+/* Memory for forward tapes beyond the last segment's.  The forward run of
+ * nmhd_adjoint_run(_f64) stores a checkpoint every ckpt_every steps and keeps
+ * the tapes of the last segments; the reverse sweep recomputes only the
+ * segments whose tapes were not kept.  bytes = -1 (default): as many segments
+ * as fit in half of the device memory free at the run; 0: the last segment
+ * only (least memory); > 0: that many bytes for further segments.  The
+ * gradient does not depend on it (bitwise).  nmhd_adjoint_kept_segments: how
+ * many segments the last run kept. */
+nmhd_status nmhd_adjoint_set_tape_budget(nmhd_solver *s, int64_t bytes);
+int32_t nmhd_adjoint_kept_segments(const nmhd_solver *s);
 /* Device time of the last nmhd_adjoint_run / nmhd_adjoint_run_f64 in ms:
  * [0] forward run with checkpoints, [1] segment recomputation, [2] adjoint
  * kernels, [3] the whole run. */

@@ -70,6 +70,8 @@ _SIGS = [
     ("nmhd_tlm_run", ctypes.c_int, [_P, ctypes.c_int32, _P, _P, ctypes.POINTER(_P), ctypes.c_double,
                                     ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]),
     ("nmhd_adjoint_timing", ctypes.c_int, [_P, _P]),
+    ("nmhd_adjoint_set_tape_budget", ctypes.c_int, [_P, ctypes.c_int64]),
+    ("nmhd_adjoint_kept_segments", ctypes.c_int32, [_P]),
     ("nmhd_batch_create", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P)]),
     ("nmhd_batch_destroy", None, [_P]),
     ("nmhd_batch_size", ctypes.c_int, [_P]),

@@ -8,10 +8,13 @@
 // kernels of ad_driver.cuh over double and Dual<double>.  The adjoint kernels
 // are the transposes in ad_cell.cuh / ad_hlld.cuh, one launch per pass.
 //
-// Memory: checkpoints (8 fields) every K steps, plus one segment's tape (66
-// fields per step: filled input, predictor, raw output, both stages' fluxes),
-// plus 3 adjoint states and 42 scratch fields.  The forward run keeps the
-// last segment on the tape, so only the earlier segments are recomputed.
+// Memory: checkpoints (8 fields) every K steps, plus the tape (66 fields per
+// step: filled input, predictor, raw output, both stages' fluxes) of the last
+// segments, plus 3 adjoint states and 42 scratch fields.  The forward run
+// keeps as many trailing segments on the tape as the tape budget allows (at
+// least one; by default as many as fit in half of the free device memory),
+// and the reverse sweep recomputes only the earlier segments, from their
+// checkpoints.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -141,6 +144,8 @@ struct GpuExec {
 struct Workspace {
   void *mem = nullptr;
   size_t bytes = 0;
+  long long tape_budget = -1;  // bytes for the tapes of segments beyond the last; -1: automatic
+  int kept_segments = 0;       // of the last run
   StepCtl *ctl = nullptr;
   float *dt_dev = nullptr, *hist_dummy = nullptr;
   double ms[4] = {0, 0, 0, 0};
@@ -291,6 +296,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   const GGrid<R> gg = make_ggrid<R>(s->cfg);
   const int nseg = (nsteps + K - 1) / K;
   const int tape_steps = want_grad ? std::min(K, nsteps) : 1;
+  int kseg = 1;  // trailing segments kept on the tape by the forward run
   const bool frozen = dt_seq != nullptr;
   if (!Prec<R>::kProduction && !frozen)
     return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "dt_seq is required for FP64 runs");
@@ -301,7 +307,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   double *partial = nullptr, *acc = nullptr;
   auto carve = [&](Arena &ar) {
     ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
-    tape = ar.take<R>((size_t)tape_steps * kTapeFields * n);
+    tape = ar.take<R>((size_t)kseg * tape_steps * kTapeFields * n);
     spare = ar.take<R>(8 * n);
     lam = want_grad ? ar.take<R>(24 * n) : nullptr;
     scr = want_grad ? ar.take<R>((size_t)kAdjScratchFields * n) : nullptr;
@@ -310,6 +316,20 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   };
   Arena probe{0, 0};
   carve(probe);
+  if (want_grad && nseg > 1) {
+    // more trailing segments on the tape, within the budget
+    const size_t seg_bytes = (size_t)tape_steps * kTapeFields * n * sizeof(R);
+    long long budget = w.tape_budget;
+    if (budget < 0) {
+      size_t free_b = 0, total_b = 0;
+      AD_CUDA(cudaMemGetInfo(&free_b, &total_b));
+      budget = (long long)((free_b + w.bytes) / 2) - (long long)probe.off;
+    }
+    if (budget > 0) kseg = 1 + (int)std::min<long long>(nseg - 1, budget / (long long)seg_bytes);
+    probe = Arena{0, 0};
+    carve(probe);
+  }
+  w.kept_segments = want_grad ? kseg : 0;
   nmhd_status st = reserve(s, w, probe.off + 256);
   if (st != NMHD_OK) return st;
   Arena ar{reinterpret_cast<uintptr_t>(w.mem), 0};
@@ -349,9 +369,9 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   }
   std::vector<double> tn(nsteps + 1);
   tn[0] = t0;
-  // the last segment's steps are kept on the tape: the reverse sweep starts
-  // there without recomputing it
-  const int kept0 = want_grad ? (nseg - 1) * K : nsteps;
+  // the last kseg segments' steps are kept on the tape: the reverse sweep
+  // runs over them without recomputing them
+  const int kept0 = want_grad ? (nseg - kseg) * K : nsteps;
   for (int i = 0; i < nsteps; ++i) {
     if (want_grad && i % K == 0)
       AD_CUDA(cudaMemcpyAsync(ckpt + (size_t)(i / K) * 8 * n, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
@@ -403,28 +423,31 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   double ms_re = 0.0, ms_adj = 0.0;
   for (int seg = nseg - 1; seg >= 0; --seg) {
     const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
-    const bool kept = seg == nseg - 1;  // taped by the forward run
+    const bool kept = n0 >= kept0;  // taped by the forward run
+    // a recomputed segment reuses the first segment slot of the tape: every
+    // kept segment comes later in the run and has been swept already
+    R *segtape = kept ? tape + (size_t)(n0 - kept0) * kTapeFields * n : tape;
     if (Prec<R>::kProduction && !kept) {
       st = write_ctl(s, w, tn[n0], n0, true);
       if (st != NMHD_OK) return st;
     }
     AD_CUDA(cudaEventRecord(w.ev[2], q));
     if (!kept)
-      AD_CUDA(cudaMemcpyAsync(tape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+      AD_CUDA(cudaMemcpyAsync(segtape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     for (int i = n0; i < (kept ? n0 : n1); ++i) {
-      const StepTape<R> t = tape_at(tape + (size_t)(i - n0) * kTapeFields * n, n);
+      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n);
       if constexpr (Prec<R>::kProduction)
         prod_step(s, w, t, false);
       else
         fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
       if (i + 1 < n1) {
-        const StepTape<R> tn1 = tape_at(tape + (size_t)(i + 1 - n0) * kTapeFields * n, n);
+        const StepTape<R> tn1 = tape_at(segtape + (size_t)(i + 1 - n0) * kTapeFields * n, n);
         AD_CUDA(cudaMemcpyAsync(tn1.wf, t.wo, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
       }
     }
     AD_CUDA(cudaEventRecord(w.ev[3], q));
     for (int i = n1 - 1; i >= n0; --i) {
-      const StepTape<R> t = tape_at(tape + (size_t)(i - n0) * kTapeFields * n, n);
+      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n);
       if (in_window(L, i + 1)) ex.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
       adj_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
       std::swap(lamA, lamF);
@@ -550,6 +573,18 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
   *loss_out = h.v;
   if (dloss_out) *dloss_out = h.d;
   return NMHD_OK;
+}
+
+nmhd_status nmhd_adjoint_set_tape_budget(nmhd_solver *s, int64_t bytes) {
+  if (!s) return NMHD_ERR_INVALID_ARGUMENT;
+  if (bytes < -1) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "tape budget must be >= -1");
+  workspace(s).tape_budget = bytes;
+  return NMHD_OK;
+}
+
+int32_t nmhd_adjoint_kept_segments(const nmhd_solver *s) {
+  if (!s || !s->adjoint) return 0;
+  return static_cast<const Workspace *>(s->adjoint)->kept_segments;
 }
 
 nmhd_status nmhd_adjoint_timing(const nmhd_solver *s, double ms_out[4]) {

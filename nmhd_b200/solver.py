@@ -298,6 +298,16 @@ class MHDSolver:
             ctypes.byref(dloss)))
         return loss.value, dloss.value
 
+    def set_adjoint_tape_budget(self, nbytes=-1):
+        """Device memory for forward tapes beyond the last segment's (-1:
+        as many segments as fit in half the free memory; 0: last segment
+        only).  The gradient does not depend on it."""
+        _check(self._L, self._h, self._L.nmhd_adjoint_set_tape_budget(self._h, int(nbytes)))
+
+    def adjoint_kept_segments(self):
+        """Segments whose forward tape the last adjoint run kept (not recomputed)."""
+        return int(self._L.nmhd_adjoint_kept_segments(self._h))
+
     def adjoint_timing(self):
         """Device ms of the last adjoint run: forward, recompute, adjoint, total."""
         ms = np.zeros(4, np.float64)

@@ -81,12 +81,24 @@ def test_fp32_adjoint_matches_the_host_build(gpu, case):
 
 
 @pytest.mark.parametrize("ckpt", [1, 2, 5, 6, 20])
-def test_checkpoint_interval_does_not_change_the_gradient(gpu, ckpt):
+@pytest.mark.parametrize("budget", ["last", "two", "auto"])
+def test_checkpoint_interval_and_tape_budget_do_not_change_the_gradient(gpu, ckpt, budget):
+    """Checkpoint interval and the number of segments kept on the tape (the
+    last only: every earlier segment recomputed; two; all that fit) leave the
+    gradient bitwise unchanged."""
     cfg, s = _case("shear")
+    nseg = -(-6 // ckpt)
+    seg_bytes = min(ckpt, 6) * 66 * cfg.cells * 4
     with MHDSolver(cfg) as sol:
         sol.set_state(s)
+        sol.set_adjoint_tape_budget(0)
         J0, g0, _ = sol.adjoint(6, window=(1, 6), ckpt_every=3)
+        assert sol.adjoint_kept_segments() == 1
+        sol.set_adjoint_tape_budget({"last": 0, "two": seg_bytes, "auto": -1}[budget])
         J, g, _ = sol.adjoint(6, window=(1, 6), ckpt_every=ckpt)
+        assert sol.adjoint_kept_segments() == {"last": 1, "two": min(2, nseg), "auto": nseg}[budget]
+        if budget == "auto":
+            assert sol.adjoint_timing()["recompute"] < 0.05  # nothing to recompute
     assert J == J0
     assert np.array_equal(g.view(np.uint32), g0.view(np.uint32))
 
