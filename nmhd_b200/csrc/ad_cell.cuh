@@ -404,7 +404,7 @@ NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R 
   lamU[4 * N + o] = l_ene;
   lamE[o] = l_eint;
   // conserved state before the stage from the base primitives
-  lb[o] += l_rho + l_mx * vx0 + l_my * vy0 + l_mz * vz0 + l_ene * R(0.5f) * (vx0 * vx0 + vy0 * vy0 + vz0 * vz0);
+  lb[o] = fmaa(l_ene * R(0.5f), (vx0 * vx0 + vy0 * vy0 + vz0 * vz0), fmaa(l_mz, vz0, fmaa(l_my, vy0, fmaa(l_mx, vx0, lb[o] + l_rho))));
   lb[N + o] += (l_mx + l_ene * vx0) * rho0;
   lb[2 * N + o] += (l_my + l_ene * vy0) * rho0;
   lb[3 * N + o] += (l_mz + l_ene * vz0) * rho0;
@@ -549,7 +549,7 @@ NMHD_HD R ct_flux_adj_nb(const GGrid<R> &g, const R *win, const R *lamBn, const 
     const R wgt = db == 0 ? (wind > R(0) ? R(0) : (wind < R(0) ? R(1) : R(0.5f)))
                           : (wind > R(0) ? R(1) : (wind < R(0) ? R(0) : R(0.5f)));
     const R lam_c = ca * (lA[eb] - lA[e]) - cb * (lB[ea] - lB[e]);
-    acc += wgt * lam_c;
+    acc = fmaa(wgt, lam_c, acc);
   }
   return acc;
 }
@@ -696,11 +696,11 @@ NMHD_HD void a_fill_y_item(const GGrid<R> &g, int dint, R f, R *lam, int idx) {
   const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx_hi;
   const R llo = var[dst_lo];
   var[dst_lo] = R(0);
-  var[src_inc] += coef * llo;
+  var[src_inc] = fmaa(coef, llo, var[src_inc]);
   if (!(v == 6 && sy == 0)) {
     const R lhi = var[dst_hi];
     var[dst_hi] = R(0);
-    var[src_dec] += coef * lhi;
+    var[src_dec] = fmaa(coef, lhi, var[src_dec]);
   }
 }
 
@@ -719,13 +719,13 @@ NMHD_HD void a_stress_cell(const GGrid<R> &g, const R *w, R *lam, int x, int y, 
     const int cx = x - k;
     if (!inner(y, z)) break;
     const double byl = (double)w[6 * N + cell_at(g, cx, y, z)], byh = (double)w[6 * N + cell_at(g, cx, y + 1, z)];
-    gx += -0.25 * (byl + byh);
+    gx = fmaa(-0.25, (byl + byh), gx);
   }
   for (int k = 0; k < 2; ++k) {
     const int cy = wrapc(y - k, g.sy);
     if (!inner(cy, z)) continue;
     const double bxl = (double)w[5 * N + cell_at(g, x, cy, z)], bxh = (double)w[5 * N + cell_at(g, x + 1, cy, z)];
-    gy += -0.25 * (bxl + bxh);
+    gy = fmaa(-0.25, (bxl + bxh), gy);
   }
   lam[5 * N + o] += (R)(s * gx);
   lam[6 * N + o] += (R)(s * gy);

@@ -218,32 +218,32 @@ NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, cons
   // es = (sv*e - pT*u + pT_s*S_M + Bx*(vB - vBs)) / sm
   {
     const R t = a.es * ism;
-    a.sv += t * s.e;
-    a.e += t * s.sv;
-    a.pT -= t * s.u;
-    a.u -= t * s.pT;
-    apTs += t * S_M;
-    aSM += t * pT_s;
-    aBx += t * (s.vB - s.vBs);
-    a.vB += t * Bx;
-    a.vBs -= t * Bx;
-    a.sm -= t * s.es;
+    a.sv = fmaa(t, s.e, a.sv);
+    a.e = fmaa(t, s.sv, a.e);
+    a.pT = fmaa(-t, s.u, a.pT);
+    a.u = fmaa(-t, s.pT, a.u);
+    apTs = fmaa(t, S_M, apTs);
+    aSM = fmaa(t, pT_s, aSM);
+    aBx = fmaa(t, (s.vB - s.vBs), aBx);
+    a.vB = fmaa(t, Bx, a.vB);
+    a.vBs = fmaa(-t, Bx, a.vBs);
+    a.sm = fmaa(-t, s.es, a.sm);
   }
   // vBs = S_M*Bx + vs*bys + ws*bzs
-  aSM += a.vBs * Bx;
-  aBx += a.vBs * S_M;
-  a.vs += a.vBs * s.bys;
-  a.bys += a.vBs * s.vs;
-  a.ws += a.vBs * s.bzs;
-  a.bzs += a.vBs * s.ws;
+  aSM = fmaa(a.vBs, Bx, aSM);
+  aBx = fmaa(a.vBs, S_M, aBx);
+  a.vs = fmaa(a.vBs, s.bys, a.vs);
+  a.bys = fmaa(a.vBs, s.vs, a.bys);
+  a.ws = fmaa(a.vBs, s.bzs, a.ws);
+  a.bzs = fmaa(a.vBs, s.ws, a.bzs);
   // bys = by*q/dn, bzs = bz*q/dn
-  a.by += a.bys * s.q * idn;
-  a.bz += a.bzs * s.q * idn;
-  a.q += (a.bys * s.by + a.bzs * s.bz) * idn;
-  a.dn -= (a.bys * s.bys + a.bzs * s.bzs) * idn;
+  a.by = fmaa(a.bys * s.q, idn, a.by);
+  a.bz = fmaa(a.bzs * s.q, idn, a.bz);
+  a.q = fmaa((a.bys * s.by + a.bzs * s.bz), idn, a.q);
+  a.dn = fmaa(-(a.bys * s.bys + a.bzs * s.bzs), idn, a.dn);
   // q = d*sv^2 - B2x
-  a.d += a.q * s.sv * s.sv;
-  a.sv += a.q * R(2) * s.d * s.sv;
+  a.d = fmaa(a.q * s.sv, s.sv, a.d);
+  a.sv = fmaa(a.q * R(2) * s.d, s.sv, a.sv);
   aB2x -= a.q;
   // vs = v - Bx*by*(S_M - u)/dn, ws = w - Bx*bz*(S_M - u)/dn
   {
@@ -251,25 +251,25 @@ NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, cons
     const R tv = -a.vs, tw = -a.ws;
     a.v += a.vs;
     a.w += a.ws;
-    aBx += (tv * s.by + tw * s.bz) * g;
-    a.by += tv * Bx * g;
-    a.bz += tw * Bx * g;
+    aBx = fmaa((tv * s.by + tw * s.bz), g, aBx);
+    a.by = fmaa(tv * Bx, g, a.by);
+    a.bz = fmaa(tw * Bx, g, a.bz);
     const R c = (tv * s.by + tw * s.bz) * Bx * idn;
     aSM += c;
     a.u -= c;
-    a.dn -= c * g;
+    a.dn = fmaa(-c, g, a.dn);
   }
   // dn = d*sv*sm - B2x + TINY
-  a.d += a.dn * s.sv * s.sm;
-  a.sv += a.dn * s.d * s.sm;
-  a.sm += a.dn * s.d * s.sv;
+  a.d = fmaa(a.dn * s.sv, s.sm, a.d);
+  a.sv = fmaa(a.dn * s.d, s.sm, a.sv);
+  a.sm = fmaa(a.dn * s.d, s.sv, a.sm);
   aB2x -= a.dn;
   // ds = d*sv/sm
   {
     const R t = a.ds * ism;
-    a.d += t * s.sv;
-    a.sv += t * s.d;
-    a.sm -= t * s.ds;
+    a.d = fmaa(t, s.sv, a.d);
+    a.sv = fmaa(t, s.d, a.sv);
+    a.sm = fmaa(-t, s.ds, a.sm);
   }
   // sm = S - S_M
   aS += a.sm;
@@ -279,12 +279,12 @@ NMHD_HD void hlld_side_star_rev(const HSide<R> &s, const R Bx, const R S_M, cons
 // Reverse of vB = u*Bx + v*by + w*bz (used by the flux of every region).
 template <class R>
 NMHD_HD void hlld_side_vB_rev(const HSide<R> &s, const R Bx, HAdj<R> &a, R &aBx) {
-  a.u += a.vB * Bx;
-  aBx += a.vB * s.u;
-  a.v += a.vB * s.by;
-  a.by += a.vB * s.v;
-  a.w += a.vB * s.bz;
-  a.bz += a.vB * s.w;
+  a.u = fmaa(a.vB, Bx, a.u);
+  aBx = fmaa(a.vB, s.u, aBx);
+  a.v = fmaa(a.vB, s.by, a.v);
+  a.by = fmaa(a.vB, s.v, a.by);
+  a.w = fmaa(a.vB, s.bz, a.w);
+  a.bz = fmaa(a.vB, s.w, a.bz);
 }
 
 // Reverse of hlld_side_pre (after pT, cf, e, mx.. have their adjoints).
@@ -293,42 +293,42 @@ NMHD_HD void hlld_side_pre_rev(const HSide<R> &s, const R gamma, const R igm1, c
                                R &aB2x) {
   // pT = p + 0.5*B2
   a.p += a.pT;
-  a.B2 += R(0.5) * a.pT;
+  a.B2 = fmaa(R(0.5), a.pT, a.B2);
   // cf = sqrt(num/(2d))
   if (s.cf > R(0)) {
     const R id = R(1) / s.d;
     const R aQ = a.cf * (R(0.5) / s.cf);
     const R Q = R(0.5) * s.num * id;
     const R anum = R(0.5) * aQ * id;
-    a.d -= aQ * Q * id;
+    a.d = fmaa(-(aQ * Q), id, a.d);
     // num = gpb + sq; sq = sqrt(disc); disc = gpb^2 - 4 gp B2x; gpb = gp + B2
     R agpb = anum, agp = R(0);
     if (s.sq > R(0)) {
       const R adisc = anum * (R(0.5) / s.sq);
-      agpb += adisc * R(2) * s.gpb;
-      agp -= adisc * R(4) * B2x;
-      aB2x -= adisc * R(4) * s.gp;
+      agpb = fmaa(adisc * R(2), s.gpb, agpb);
+      agp = fmaa(-(adisc * R(4)), B2x, agp);
+      aB2x = fmaa(-(adisc * R(4)), s.gp, aB2x);
     }
     agp += agpb;
     a.B2 += agpb;
-    a.p += gamma * agp;
+    a.p = fmaa(gamma, agp, a.p);
   }
   // e = p/gm1 + 0.5*d*v2 + 0.5*B2
-  a.p += a.e * igm1;
-  a.d += R(0.5) * a.e * s.v2;
-  a.v2 += R(0.5) * a.e * s.d;
-  a.B2 += R(0.5) * a.e;
+  a.p = fmaa(a.e, igm1, a.p);
+  a.d = fmaa(R(0.5) * a.e, s.v2, a.d);
+  a.v2 = fmaa(R(0.5) * a.e, s.d, a.v2);
+  a.B2 = fmaa(R(0.5), a.e, a.B2);
   // v2, B2, momenta
-  a.u += R(2) * s.u * a.v2;
-  a.v += R(2) * s.v * a.v2;
-  a.w += R(2) * s.w * a.v2;
+  a.u = fmaa(R(2) * s.u, a.v2, a.u);
+  a.v = fmaa(R(2) * s.v, a.v2, a.v);
+  a.w = fmaa(R(2) * s.w, a.v2, a.w);
   aB2x += a.B2;
-  a.by += R(2) * s.by * a.B2;
-  a.bz += R(2) * s.bz * a.B2;
-  a.d += a.mx * s.u + a.my * s.v + a.mz * s.w;
-  a.u += a.mx * s.d;
-  a.v += a.my * s.d;
-  a.w += a.mz * s.d;
+  a.by = fmaa(R(2) * s.by, a.B2, a.by);
+  a.bz = fmaa(R(2) * s.bz, a.B2, a.bz);
+  a.d = fmaa(a.mz, s.w, fmaa(a.my, s.v, fmaa(a.mx, s.u, a.d)));
+  a.u = fmaa(a.mx, s.d, a.u);
+  a.v = fmaa(a.my, s.d, a.v);
+  a.w = fmaa(a.mz, s.d, a.w);
 }
 
 
@@ -355,36 +355,35 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
   hadj_zero(aX);
   R aSX = R(0);
   // F = F(U) of side X
-  aX.d += lf[0] * u;
-  aX.u += lf[0] * d + lf[1] * mx + lf[2] * my + lf[3] * mz + lf[4] * (e + pT) + lf[5] * by + lf[6] * bz;
-  aX.mx += lf[1] * u;
-  aX.pT += lf[1] + lf[4] * u;
+  aX.d = fmaa(lf[0], u, aX.d);
+  aX.u = fmaa(lf[6], bz, fmaa(lf[5], by, fmaa(lf[4], (e + pT), fmaa(lf[3], mz, fmaa(lf[2], my, fmaa(lf[1], mx, fmaa(lf[0], d, aX.u)))))));
+  aX.mx = fmaa(lf[1], u, aX.mx);
+  aX.pT = fmaa(lf[4], u, aX.pT + lf[1]);
   aB2x -= lf[1];
-  aX.my += lf[2] * u;
-  aX.mz += lf[3] * u;
-  aBx -= lf[2] * by + lf[3] * bz + lf[4] * vB + lf[5] * v + lf[6] * w;
-  aX.by += lf[5] * u - lf[2] * Bx;
-  aX.bz += lf[6] * u - lf[3] * Bx;
-  aX.e += lf[4] * u;
-  aX.vB -= lf[4] * Bx;
-  aX.v -= lf[5] * Bx;
-  aX.w -= lf[6] * Bx;
+  aX.my = fmaa(lf[2], u, aX.my);
+  aX.mz = fmaa(lf[3], u, aX.mz);
+  aBx = fmaa(-lf[6], w, fmaa(-lf[5], v, fmaa(-lf[4], vB, fmaa(-lf[3], bz, fmaa(-lf[2], by, aBx)))));
+  aX.by = fmaa(-lf[2], Bx, fmaa(lf[5], u, aX.by));
+  aX.bz = fmaa(-lf[3], Bx, fmaa(lf[6], u, aX.bz));
+  aX.e = fmaa(lf[4], u, aX.e);
+  aX.vB = fmaa(-lf[4], Bx, aX.vB);
+  aX.v = fmaa(-lf[5], Bx, aX.v);
+  aX.w = fmaa(-lf[6], Bx, aX.w);
   if (rg != 0 && rg != 5) {
     const R S = left ? t.S_L : t.S_R;
     const R ds = left ? t.L.ds : t.R.ds, vs = left ? t.L.vs : t.R.vs, ws = left ? t.L.ws : t.R.ws;
     const R es = left ? t.L.es : t.R.es, bys = left ? t.L.bys : t.R.bys, bzs = left ? t.L.bzs : t.R.bzs;
     const R Us1 = ds * t.S_M, Us2 = ds * vs, Us3 = ds * ws;
     // -S*U
-    aX.d -= S * lf[0];
-    aX.mx -= S * lf[1];
-    aX.my -= S * lf[2];
-    aX.mz -= S * lf[3];
-    aX.e -= S * lf[4];
-    aX.by -= S * lf[5];
-    aX.bz -= S * lf[6];
+    aX.d = fmaa(-S, lf[0], aX.d);
+    aX.mx = fmaa(-S, lf[1], aX.mx);
+    aX.my = fmaa(-S, lf[2], aX.my);
+    aX.mz = fmaa(-S, lf[3], aX.mz);
+    aX.e = fmaa(-S, lf[4], aX.e);
+    aX.by = fmaa(-S, lf[5], aX.by);
+    aX.bz = fmaa(-S, lf[6], aX.bz);
     // d/dS of S*(U* - U) (regions 1, 4) and of -(Sss - S)*U* - S*U (regions 2, 3)
-    aSX += lf[0] * (ds - d) + lf[1] * (Us1 - mx) + lf[2] * (Us2 - my) + lf[3] * (Us3 - mz) +
-           lf[4] * (es - e) + lf[5] * (bys - by) + lf[6] * (bzs - bz);
+    aSX = fmaa(lf[6], (bzs - bz), fmaa(lf[5], (bys - by), fmaa(lf[4], (es - e), fmaa(lf[3], (Us3 - mz), fmaa(lf[2], (Us2 - my), fmaa(lf[1], (Us1 - mx), fmaa(lf[0], (ds - d), aSX)))))));
     R cs = S;  // coefficient of U*
     const bool dstar = rg == 2 || rg == 3;
     if (dstar) {
@@ -395,79 +394,79 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
       const R aSss = lf[2] * (ds * t.vss - Us2) + lf[3] * (ds * t.wss - Us3) + lf[4] * (ess - es) +
                      lf[5] * (t.Byss - bys) + lf[6] * (t.Bzss - bzs);
       // Sss * U**
-      aX.ds += Sss * (lf[0] + lf[1] * t.S_M + lf[2] * t.vss + lf[3] * t.wss);
-      aSM += Sss * lf[1] * ds;
+      aX.ds = fmaa(Sss, (lf[0] + lf[1] * t.S_M + lf[2] * t.vss + lf[3] * t.wss), aX.ds);
+      aSM = fmaa(Sss * lf[1], ds, aSM);
       R avss = Sss * lf[2] * ds, awss = Sss * lf[3] * ds;
       const R aess = Sss * lf[4];
       R aByss = Sss * lf[5], aBzss = Sss * lf[6];
       // ess = eX* + sx * sdX * (vBX* - vBss) * sgn
       R avBss = R(0), afr = R(0), asdLR = R(0);
       aX.es += aess;
-      aX.sd += sx * aess * (vBs - t.vBss) * sgn;
-      aX.vBs += sx * aess * sd * sgn;
-      avBss -= sx * aess * sd * sgn;
+      aX.sd = fmaa(sx * aess * (vBs - t.vBss), sgn, aX.sd);
+      aX.vBs = fmaa(sx * aess * sd, sgn, aX.vBs);
+      avBss = fmaa(-(sx * aess * sd), sgn, avBss);
       // vBss = S_M*Bx + vss*Byss + wss*Bzss
-      aSM += avBss * Bx;
-      aBx += avBss * t.S_M;
-      avss += avBss * t.Byss;
-      aByss += avBss * t.vss;
-      awss += avBss * t.Bzss;
-      aBzss += avBss * t.wss;
+      aSM = fmaa(avBss, Bx, aSM);
+      aBx = fmaa(avBss, t.S_M, aBx);
+      avss = fmaa(avBss, t.Byss, avss);
+      aByss = fmaa(avBss, t.vss, aByss);
+      awss = fmaa(avBss, t.Bzss, awss);
+      aBzss = fmaa(avBss, t.wss, aBzss);
       // Bzss = fr*(sdL*bzRs + sdR*bzLs + sdLR*(wRs - wLs)*sgn)
       {
         const R n = t.L.sd * t.R.bzs + t.R.sd * t.L.bzs + t.sdLR * (t.R.ws - t.L.ws) * sgn;
-        afr += aBzss * n;
+        afr = fmaa(aBzss, n, afr);
         const R c = aBzss * t.fr;
-        aL.sd += c * t.R.bzs;
-        aR.bzs += c * t.L.sd;
-        aR.sd += c * t.L.bzs;
-        aL.bzs += c * t.R.sd;
-        asdLR += c * (t.R.ws - t.L.ws) * sgn;
-        aR.ws += c * t.sdLR * sgn;
-        aL.ws -= c * t.sdLR * sgn;
+        aL.sd = fmaa(c, t.R.bzs, aL.sd);
+        aR.bzs = fmaa(c, t.L.sd, aR.bzs);
+        aR.sd = fmaa(c, t.L.bzs, aR.sd);
+        aL.bzs = fmaa(c, t.R.sd, aL.bzs);
+        asdLR = fmaa(c * (t.R.ws - t.L.ws), sgn, asdLR);
+        aR.ws = fmaa(c * t.sdLR, sgn, aR.ws);
+        aL.ws = fmaa(-(c * t.sdLR), sgn, aL.ws);
       }
       // Byss = fr*(sdL*byRs + sdR*byLs + sdLR*(vRs - vLs)*sgn)
       {
         const R n = t.L.sd * t.R.bys + t.R.sd * t.L.bys + t.sdLR * (t.R.vs - t.L.vs) * sgn;
-        afr += aByss * n;
+        afr = fmaa(aByss, n, afr);
         const R c = aByss * t.fr;
-        aL.sd += c * t.R.bys;
-        aR.bys += c * t.L.sd;
-        aR.sd += c * t.L.bys;
-        aL.bys += c * t.R.sd;
-        asdLR += c * (t.R.vs - t.L.vs) * sgn;
-        aR.vs += c * t.sdLR * sgn;
-        aL.vs -= c * t.sdLR * sgn;
+        aL.sd = fmaa(c, t.R.bys, aL.sd);
+        aR.bys = fmaa(c, t.L.sd, aR.bys);
+        aR.sd = fmaa(c, t.L.bys, aR.sd);
+        aL.bys = fmaa(c, t.R.sd, aL.bys);
+        asdLR = fmaa(c * (t.R.vs - t.L.vs), sgn, asdLR);
+        aR.vs = fmaa(c * t.sdLR, sgn, aR.vs);
+        aL.vs = fmaa(-(c * t.sdLR), sgn, aL.vs);
       }
       // wss = fr*(sdL*wLs + sdR*wRs + (bzRs - bzLs)*sgn)
       {
         const R n = t.L.sd * t.L.ws + t.R.sd * t.R.ws + (t.R.bzs - t.L.bzs) * sgn;
-        afr += awss * n;
+        afr = fmaa(awss, n, afr);
         const R c = awss * t.fr;
-        aL.sd += c * t.L.ws;
-        aL.ws += c * t.L.sd;
-        aR.sd += c * t.R.ws;
-        aR.ws += c * t.R.sd;
-        aR.bzs += c * sgn;
-        aL.bzs -= c * sgn;
+        aL.sd = fmaa(c, t.L.ws, aL.sd);
+        aL.ws = fmaa(c, t.L.sd, aL.ws);
+        aR.sd = fmaa(c, t.R.ws, aR.sd);
+        aR.ws = fmaa(c, t.R.sd, aR.ws);
+        aR.bzs = fmaa(c, sgn, aR.bzs);
+        aL.bzs = fmaa(-c, sgn, aL.bzs);
       }
       // vss = fr*(sdL*vLs + sdR*vRs + (byRs - byLs)*sgn)
       {
         const R n = t.L.sd * t.L.vs + t.R.sd * t.R.vs + (t.R.bys - t.L.bys) * sgn;
-        afr += avss * n;
+        afr = fmaa(avss, n, afr);
         const R c = avss * t.fr;
-        aL.sd += c * t.L.vs;
-        aL.vs += c * t.L.sd;
-        aR.sd += c * t.R.vs;
-        aR.vs += c * t.R.sd;
-        aR.bys += c * sgn;
-        aL.bys -= c * sgn;
+        aL.sd = fmaa(c, t.L.vs, aL.sd);
+        aL.vs = fmaa(c, t.L.sd, aL.vs);
+        aR.sd = fmaa(c, t.R.vs, aR.sd);
+        aR.vs = fmaa(c, t.R.sd, aR.vs);
+        aR.bys = fmaa(c, sgn, aR.bys);
+        aL.bys = fmaa(-c, sgn, aL.bys);
       }
       // sdLR = sqrt(dLs*dRs)
       if (t.sdLR > R(0)) {
         const R c = asdLR * (R(0.5) / t.sdLR);
-        aL.ds += c * t.R.ds;
-        aR.ds += c * t.L.ds;
+        aL.ds = fmaa(c, t.R.ds, aL.ds);
+        aR.ds = fmaa(c, t.L.ds, aR.ds);
       }
       // fr = 1/(sdL + sdR)
       {
@@ -479,17 +478,17 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
       aSM += aSss;
       {
         const R isd = R(1) / sd;
-        aabs += sx * aSss * isd;
-        aX.sd -= sx * aSss * t.absBx * isd * isd;
+        aabs = fmaa(sx * aSss, isd, aabs);
+        aX.sd = fmaa(-(sx * aSss * t.absBx * isd), isd, aX.sd);
       }
     }
-    aX.ds += cs * (lf[0] + lf[1] * t.S_M + lf[2] * vs + lf[3] * ws);
-    aSM += cs * lf[1] * ds;
-    aX.vs += cs * lf[2] * ds;
-    aX.ws += cs * lf[3] * ds;
-    aX.es += cs * lf[4];
-    aX.bys += cs * lf[5];
-    aX.bzs += cs * lf[6];
+    aX.ds = fmaa(cs, (lf[0] + lf[1] * t.S_M + lf[2] * vs + lf[3] * ws), aX.ds);
+    aSM = fmaa(cs * lf[1], ds, aSM);
+    aX.vs = fmaa(cs * lf[2], ds, aX.vs);
+    aX.ws = fmaa(cs * lf[3], ds, aX.ws);
+    aX.es = fmaa(cs, lf[4], aX.es);
+    aX.bys = fmaa(cs, lf[5], aX.bys);
+    aX.bzs = fmaa(cs, lf[6], aX.bzs);
   }
   // hand the side-X adjoints to their side
   const R kl = left ? R(1) : R(0), kr = R(1) - kl;
@@ -499,8 +498,8 @@ NMHD_HD void hlld_region_rev(const HTape<R> &t, const R lf[7], HAdj<R> &aL, HAdj
   NMHD_HAND(ds) NMHD_HAND(vs) NMHD_HAND(ws) NMHD_HAND(es) NMHD_HAND(bys) NMHD_HAND(bzs)
   NMHD_HAND(sd) NMHD_HAND(vBs)
 #undef NMHD_HAND
-  aSL += kl * aSX;
-  aSR += kr * aSX;
+  aSL = fmaa(kl, aSX, aSL);
+  aSR = fmaa(kr, aSX, aSR);
 }
 
 // Adjoint of hlld_g: ls and lBx receive d<lf, f>/d(state) and d<lf, f>/dBx.
@@ -529,26 +528,26 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
       const R aden = -(aSM * t.S_M + apTs * t.pT_s) * iden;
       const R dl = t.L.d, dr = t.R.d, sLv = t.L.sv, sRv = t.R.sv, du = t.R.u - t.L.u;
       // pTn = sRv*dr*pTL - sLv*dl*pTR + dl*dr*sRv*sLv*(ur - ul)
-      aR.sv += apTn * (dr * t.L.pT + dl * dr * sLv * du);
-      aR.d += apTn * (sRv * t.L.pT + dl * sRv * sLv * du);
-      aL.pT += apTn * sRv * dr;
-      aL.sv += apTn * (-dl * t.R.pT + dl * dr * sRv * du);
-      aL.d += apTn * (-sLv * t.R.pT + dr * sRv * sLv * du);
-      aR.pT -= apTn * sLv * dl;
-      aR.u += apTn * dl * dr * sRv * sLv;
-      aL.u -= apTn * dl * dr * sRv * sLv;
+      aR.sv = fmaa(apTn, (dr * t.L.pT + dl * dr * sLv * du), aR.sv);
+      aR.d = fmaa(apTn, (sRv * t.L.pT + dl * sRv * sLv * du), aR.d);
+      aL.pT = fmaa(apTn * sRv, dr, aL.pT);
+      aL.sv = fmaa(apTn, (-dl * t.R.pT + dl * dr * sRv * du), aL.sv);
+      aL.d = fmaa(apTn, (-sLv * t.R.pT + dr * sRv * sLv * du), aL.d);
+      aR.pT = fmaa(-(apTn * sLv), dl, aR.pT);
+      aR.u = fmaa(apTn * dl * dr * sRv, sLv, aR.u);
+      aL.u = fmaa(-(apTn * dl * dr * sRv), sLv, aL.u);
       // SMn = sRv*mxR - sLv*mxL - pTR + pTL
-      aR.sv += aSMn * t.R.mx;
-      aR.mx += aSMn * sRv;
-      aL.sv -= aSMn * t.L.mx;
-      aL.mx -= aSMn * sLv;
+      aR.sv = fmaa(aSMn, t.R.mx, aR.sv);
+      aR.mx = fmaa(aSMn, sRv, aR.mx);
+      aL.sv = fmaa(-aSMn, t.L.mx, aL.sv);
+      aL.mx = fmaa(-aSMn, sLv, aL.mx);
       aR.pT -= aSMn;
       aL.pT += aSMn;
       // den = sRv*dr - sLv*dl
-      aR.sv += aden * dr;
-      aR.d += aden * sRv;
-      aL.sv -= aden * dl;
-      aL.d -= aden * sLv;
+      aR.sv = fmaa(aden, dr, aR.sv);
+      aR.d = fmaa(aden, sRv, aR.d);
+      aL.sv = fmaa(-aden, dl, aL.sv);
+      aL.d = fmaa(-aden, sLv, aL.d);
     }
     // sv = S - u
     aSR += aR.sv;
@@ -568,7 +567,7 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
   const R igm1 = R(1) / (gamma - R(1));
   hlld_side_pre_rev(t.L, gamma, igm1, t.B2x, aL, aB2x);
   hlld_side_pre_rev(t.R, gamma, igm1, t.B2x, aR, aB2x);
-  aBx += R(2) * Bx * aB2x + aabs * sgn;
+  aBx = fmaa(aabs, sgn, fmaa(R(2) * Bx, aB2x, aBx));
 
   ls.dl = aL.d; ls.dr = aR.d; ls.ul = aL.u; ls.ur = aR.u; ls.vl = aL.v; ls.vr = aR.v;
   ls.wl = aL.w; ls.wr = aR.w; ls.pl = aL.p; ls.pr = aR.p; ls.byl = aL.by; ls.byr = aR.by;

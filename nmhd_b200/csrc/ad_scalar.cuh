@@ -22,6 +22,14 @@
 namespace nmhd {
 namespace ad {
 
+// a*b + c rounded once.  The reverse sweeps accumulate their adjoints with it:
+// they are checked against tangent-linear runs and differences to a
+// tolerance, never bitwise against the reference, and a fused multiply-add is
+// correctly rounded on the GPU and on the host alike, so the host build of the
+// tests computes the same bits.  The forward arithmetic never uses it.
+NMHD_HD float fmaa(float a, float b, float c) { return fmaf(a, b, c); }
+NMHD_HD double fmaa(double a, double b, double c) { return fma(a, b, c); }
+
 template <class R>
 struct Dual {
   R v, d;
