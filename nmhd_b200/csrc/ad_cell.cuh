@@ -672,35 +672,45 @@ NMHD_HD void a_fill_z_item(const GGrid<R> &g, R *lam, int idx) {
   }
 }
 
-// Transpose of g_fill_y_item for field v, gathered at the source: item
-// (xs, sy, sz, v) covers source cells (xs, Sy-2M+sy, sz) (-> bottom margin row
-// sy) and (xs, M+sy, sz) (-> top margin row Sy-M+sy).  Each margin cell is the
-// image of exactly one item, which clears it after reading.  dint and f are
-// shear_shift() of the step's time.
+// Transpose of g_fill_y_item, gathered at the source: item (xs, sy, sz)
+// covers, for all 8 fields, the source cells (xs, Sy-2M+sy, sz) (-> bottom
+// margin row sy) and (xs, M+sy, sz) (-> top margin row Sy-M+sy).  Each margin
+// cell is the image of exactly one item, which clears it after reading; margin
+// and source rows are disjoint, so every load is issued before any store.  With
+// exactly M interior rows the two source cells coincide and take both
+// contributions, bottom first.  dint and f are shear_shift() of the step's time.
 template <class R>
 NMHD_HD void a_fill_y_item(const GGrid<R> &g, int dint, R f, R *lam, int idx) {
   const int M = g.my;
-  const int per_field = g.sx * M * g.sz;
-  const int v = idx / per_field;
-  const int r = idx - v * per_field;
-  const int xs = r % g.sx;
-  const int sy = (r / g.sx) % M;
-  const int sz = r / (g.sx * M);
+  const size_t N = (size_t)g.n;
+  const int xs = idx % g.sx;
+  const int sy = (idx / g.sx) % M;
+  const int sz = idx / (g.sx * M);
   const R coef = (R(1.0f) - f) + f;  // d/dv of (1-f) v + f v
   const int sx_lo = wrapc((xs - dint) % g.sx, g.sx);      // (sx_lo + dint) mod Sx = xs
   const int sx_hi = wrapc((xs + dint + 1) % g.sx, g.sx);  // (sx_hi - dint - 1) mod Sx = xs
-  R *var = lam + (size_t)v * g.n;
   const int src_inc = (sz * g.sy + (g.sy - 2 * M + sy)) * g.sx + xs;
   const int src_dec = (sz * g.sy + (M + sy)) * g.sx + xs;
   const int dst_lo = (sz * g.sy + sy) * g.sx + sx_lo;
   const int dst_hi = (sz * g.sy + (g.sy - M + sy)) * g.sx + sx_hi;
-  const R llo = var[dst_lo];
-  var[dst_lo] = R(0);
-  var[src_inc] = fmaa(coef, llo, var[src_inc]);
-  if (!(v == 6 && sy == 0)) {
-    const R lhi = var[dst_hi];
-    var[dst_hi] = R(0);
-    var[src_dec] = fmaa(coef, lhi, var[src_dec]);
+  R llo[8], lhi[8], ai[8], ad[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    llo[v] = lam[v * N + dst_lo];
+    lhi[v] = (v == 6 && sy == 0) ? R(0) : lam[v * N + dst_hi];  // By of row Sy-M is interior
+    ai[v] = lam[v * N + src_inc];
+    ad[v] = lam[v * N + src_dec];
+  }
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    lam[v * N + dst_lo] = R(0);
+    if (!(v == 6 && sy == 0)) lam[v * N + dst_hi] = R(0);
+    if (src_inc == src_dec) {
+      lam[v * N + src_inc] = fmaa(coef, lhi[v], fmaa(coef, llo[v], ai[v]));
+    } else {
+      lam[v * N + src_inc] = fmaa(coef, llo[v], ai[v]);
+      lam[v * N + src_dec] = fmaa(coef, lhi[v], ad[v]);
+    }
   }
 }
 

@@ -273,7 +273,7 @@ void adj_step(Ex &ex, const GGrid<R> &g, int time_order, double time, R dt, cons
     int dint;
     R f;
     shear_shift(g, time, dint, f);
-    ex.items(8 * g.sx * g.my * g.sz, OpAFillY<R>{g, dint, f, lam_f});
+    ex.items(g.sx * g.my * g.sz, OpAFillY<R>{g, dint, f, lam_f});
   }
 }
 

@@ -98,13 +98,15 @@ def _case(name):
     elif name == "euler":
         cfg, s = shearing_box(n_radial=12, n_azimuthal=16, n_vertical=6, l_azimuthal=4.0, seed=4)
         cfg.time_order = 1
+    elif name == "shear_thin":  # interior rows = margin_y: both shear images share their sources
+        cfg, s = shearing_box(n_radial=4, n_azimuthal=16, n_vertical=6, l_radial=0.25, l_azimuthal=4.0, seed=6)
     else:  # first-order reconstruction
         cfg, s = orszag_tang_3d(12, ny=10, nz=8)
         cfg.space_order = 1
     return cfg, s
 
 
-CASES = ["ot", "shear", "shear_mz", "euler", "order1"]
+CASES = ["ot", "shear", "shear_mz", "euler", "order1", "shear_thin"]
 
 
 @pytest.mark.parametrize("case", CASES)
