@@ -150,20 +150,19 @@ __device__ __forceinline__ void flux_cell(const GridParams &g, const float *__re
   }
 }
 
-// corner_magnet_flux (src/library/mhd_solver.inlrb:641-653) at edge address e:
-// the a-flux of B_b, upwinded by the sum of the four cell velocities v_b
-// around the edge; mb, ma are the offsets of -1 along b and along a.
-__device__ __forceinline__ float corner(const float *__restrict__ vb, const float *__restrict__ fb, int e,
-                                        int mb, int ma) {
-  const float w = __ldg(vb + e) + __ldg(vb + e + mb) + __ldg(vb + e + ma) + __ldg(vb + e + ma + mb);
-  const float f0 = __ldg(fb + e + mb);
-  const float f1 = __ldg(fb + e);
+// Upwind choice of corner_magnet_flux (src/library/mhd_solver.inlrb:641-653)
+// for the wind sum w of the four cell velocities around an edge: f0 (the flux
+// one step down the wind axis) for w > 0, f1 for w < 0, their mean at a tie.
+__device__ __forceinline__ float upwind(float w, float f0, float f1) {
   return w > 0.0f ? f0 : (w < 0.0f ? f1 : 0.5f * (f0 + f1));
 }
 
 // Constrained transport of one stage (add_flux_kernel's B part,
 // mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
-// new face B on the cell's lower x-, y- and z-face, written into wo.
+// new face B on the cell's lower x-, y- and z-face, written into wo.  The 18
+// corner fluxes (corner(), at the cell's edges and one step up each in-plane
+// axis) read 39 distinct velocities and 30 distinct fluxes; each is loaded
+// once and every wind sum keeps corner()'s order.
 template <bool kPow2>
 __device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
                                         const float *__restrict__ wb, float *__restrict__ wo,
@@ -172,29 +171,56 @@ __device__ __forceinline__ void ct_cell(const GridParams &g, const float *__rest
   const int o = (z * g.sy + y) * g.sx + x;
   const Offsets f = offsets(g, x, y, z);
   const int xm = f.xm1, xp = f.xp1, ym = f.ym1, yp = f.yp1, zm = f.zm1, zp = f.zp1;
-  const float *vx = win + N, *vy = win + 2 * N, *vz = win + 3 * N;
-  const float *FxBy = flux + 5 * N, *FxBz = flux + 6 * N;
-  const float *FyBz = flux + 12 * N, *FyBx = flux + 13 * N;
-  const float *FzBx = flux + 19 * N, *FzBy = flux + 20 * N;
-  // corners at the cell's edge (00) and one step up each in-plane axis
-  const float XY00 = corner(vy, FxBy, o, ym, xm);        // F_x(B_y), wind v_y
-  const float XY01 = corner(vy, FxBy, o + yp, -yp, xm);
-  const float XY10 = corner(vy, FxBy, o + xp, ym, -xp);
-  const float YX00 = corner(vx, FyBx, o, xm, ym);        // F_y(B_x), wind v_x
-  const float YX01 = corner(vx, FyBx, o + yp, xm, -yp);
-  const float YX10 = corner(vx, FyBx, o + xp, -xp, ym);
-  const float XZ00 = corner(vz, FxBz, o, zm, xm);        // F_x(B_z), wind v_z
-  const float XZ01 = corner(vz, FxBz, o + zp, -zp, xm);
-  const float XZ10 = corner(vz, FxBz, o + xp, zm, -xp);
-  const float ZX00 = corner(vx, FzBx, o, xm, zm);        // F_z(B_x), wind v_x
-  const float ZX01 = corner(vx, FzBx, o + zp, xm, -zp);
-  const float ZX10 = corner(vx, FzBx, o + xp, -xp, zm);
-  const float YZ00 = corner(vz, FyBz, o, zm, ym);        // F_y(B_z), wind v_z
-  const float YZ01 = corner(vz, FyBz, o + zp, -zp, ym);
-  const float YZ10 = corner(vz, FyBz, o + yp, zm, -yp);
-  const float ZY00 = corner(vy, FzBy, o, ym, zm);        // F_z(B_y), wind v_y
-  const float ZY01 = corner(vy, FzBy, o + zp, ym, -zp);
-  const float ZY10 = corner(vy, FzBy, o + yp, -yp, zm);
+  const float *vx = win + N + o, *vy = win + 2 * N + o, *vz = win + 3 * N + o;
+  // velocities around the cell (offsets from o)
+  const float x_0 = __ldg(vx), x_xm = __ldg(vx + xm), x_ym = __ldg(vx + ym), x_ymxm = __ldg(vx + ym + xm);
+  const float x_yp = __ldg(vx + yp), x_ypxm = __ldg(vx + yp + xm), x_xp = __ldg(vx + xp);
+  const float x_xpym = __ldg(vx + xp + ym), x_zm = __ldg(vx + zm), x_zmxm = __ldg(vx + zm + xm);
+  const float x_zp = __ldg(vx + zp), x_zpxm = __ldg(vx + zp + xm), x_xpzm = __ldg(vx + xp + zm);
+  const float y_0 = __ldg(vy), y_ym = __ldg(vy + ym), y_xm = __ldg(vy + xm), y_xmym = __ldg(vy + xm + ym);
+  const float y_yp = __ldg(vy + yp), y_ypxm = __ldg(vy + yp + xm), y_xp = __ldg(vy + xp);
+  const float y_xpym = __ldg(vy + xp + ym), y_zm = __ldg(vy + zm), y_zmym = __ldg(vy + zm + ym);
+  const float y_zp = __ldg(vy + zp), y_zpym = __ldg(vy + zp + ym), y_ypzm = __ldg(vy + yp + zm);
+  const float z_0 = __ldg(vz), z_zm = __ldg(vz + zm), z_xm = __ldg(vz + xm), z_xmzm = __ldg(vz + xm + zm);
+  const float z_zp = __ldg(vz + zp), z_zpxm = __ldg(vz + zp + xm), z_xp = __ldg(vz + xp);
+  const float z_xpzm = __ldg(vz + xp + zm), z_ym = __ldg(vz + ym), z_ymzm = __ldg(vz + ym + zm);
+  const float z_zpym = __ldg(vz + zp + ym), z_yp = __ldg(vz + yp), z_ypzm = __ldg(vz + yp + zm);
+  // B fluxes (offsets from o)
+  const float *FxBy = flux + 5 * N + o, *FxBz = flux + 6 * N + o;
+  const float *FyBz = flux + 12 * N + o, *FyBx = flux + 13 * N + o;
+  const float *FzBx = flux + 19 * N + o, *FzBy = flux + 20 * N + o;
+  const float xy_0 = __ldg(FxBy), xy_ym = __ldg(FxBy + ym), xy_yp = __ldg(FxBy + yp), xy_xp = __ldg(FxBy + xp),
+              xy_xpym = __ldg(FxBy + xp + ym);
+  const float yx_0 = __ldg(FyBx), yx_xm = __ldg(FyBx + xm), yx_yp = __ldg(FyBx + yp),
+              yx_ypxm = __ldg(FyBx + yp + xm), yx_xp = __ldg(FyBx + xp);
+  const float xz_0 = __ldg(FxBz), xz_zm = __ldg(FxBz + zm), xz_zp = __ldg(FxBz + zp), xz_xp = __ldg(FxBz + xp),
+              xz_xpzm = __ldg(FxBz + xp + zm);
+  const float zx_0 = __ldg(FzBx), zx_xm = __ldg(FzBx + xm), zx_zp = __ldg(FzBx + zp),
+              zx_zpxm = __ldg(FzBx + zp + xm), zx_xp = __ldg(FzBx + xp);
+  const float yz_0 = __ldg(FyBz), yz_zm = __ldg(FyBz + zm), yz_zp = __ldg(FyBz + zp), yz_yp = __ldg(FyBz + yp),
+              yz_ypzm = __ldg(FyBz + yp + zm);
+  const float zy_0 = __ldg(FzBy), zy_ym = __ldg(FzBy + ym), zy_zp = __ldg(FzBy + zp),
+              zy_zpym = __ldg(FzBy + zp + ym), zy_yp = __ldg(FzBy + yp);
+  // corner(vb, fb, e, mb, ma): wind vb[e] + vb[e+mb] + vb[e+ma] + vb[e+ma+mb],
+  // f0 = fb[e+mb], f1 = fb[e]
+  const float XY00 = upwind(y_0 + y_ym + y_xm + y_xmym, xy_ym, xy_0);            // F_x(B_y), wind v_y
+  const float XY01 = upwind(y_yp + y_0 + y_ypxm + y_xm, xy_0, xy_yp);
+  const float XY10 = upwind(y_xp + y_xpym + y_0 + y_ym, xy_xpym, xy_xp);
+  const float YX00 = upwind(x_0 + x_xm + x_ym + x_ymxm, yx_xm, yx_0);            // F_y(B_x), wind v_x
+  const float YX01 = upwind(x_yp + x_ypxm + x_0 + x_xm, yx_ypxm, yx_yp);
+  const float YX10 = upwind(x_xp + x_0 + x_xpym + x_ym, yx_0, yx_xp);
+  const float XZ00 = upwind(z_0 + z_zm + z_xm + z_xmzm, xz_zm, xz_0);            // F_x(B_z), wind v_z
+  const float XZ01 = upwind(z_zp + z_0 + z_zpxm + z_xm, xz_0, xz_zp);
+  const float XZ10 = upwind(z_xp + z_xpzm + z_0 + z_zm, xz_xpzm, xz_xp);
+  const float ZX00 = upwind(x_0 + x_xm + x_zm + x_zmxm, zx_xm, zx_0);            // F_z(B_x), wind v_x
+  const float ZX01 = upwind(x_zp + x_zpxm + x_0 + x_xm, zx_zpxm, zx_zp);
+  const float ZX10 = upwind(x_xp + x_0 + x_xpzm + x_zm, zx_0, zx_xp);
+  const float YZ00 = upwind(z_0 + z_zm + z_ym + z_ymzm, yz_zm, yz_0);            // F_y(B_z), wind v_z
+  const float YZ01 = upwind(z_zp + z_0 + z_zpym + z_ym, yz_0, yz_zp);
+  const float YZ10 = upwind(z_yp + z_ypzm + z_0 + z_zm, yz_ypzm, yz_yp);
+  const float ZY00 = upwind(y_0 + y_ym + y_zm + y_zmym, zy_ym, zy_0);            // F_z(B_y), wind v_y
+  const float ZY01 = upwind(y_zp + y_zpym + y_0 + y_ym, zy_zpym, zy_zp);
+  const float ZY10 = upwind(y_yp + y_0 + y_ypzm + y_zm, zy_0, zy_yp);
   const float dx = g.dx, dy = g.dy, dz = g.dz, ix = g.inv_dx, iy = g.inv_dy, iz = g.inv_dz;
   float pb = 0.0f;
   pb = pb + 0.5f * (divs<kPow2>(XY01 - XY00, dy, iy) + divs<kPow2>(XZ01 - XZ00, dz, iz));
