@@ -52,7 +52,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const Ste
 }
 
 template <bool kPow2>
-__global__ void __launch_bounds__(kThreads, 3) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
+__global__ void __launch_bounds__(kThreads, 4) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
                                                            float *w1, float *wp,
                                                            const float *__restrict__ flux, float *dt_hist,
                                                            int out_sel, int half, int final_stage, int z0,
