@@ -54,9 +54,10 @@ __device__ __forceinline__ int find_box(int nb, long long i, F begin) {
 
 // One stage kernel over all boxes.  KIND 0: face fluxes, 1: constrained
 // transport, 2: conserved update + primitive recovery (+ CFL and clock in the
-// final stage).
+// final stage).  3 CTAs/SM, except 4 for the conserved update (bound by
+// memory latency; more would spill, as would 4 for the CT kind).
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, 3)
+__global__ void __launch_bounds__(kThreads, KIND == 2 ? 4 : 3)
     k_batch_stage(const BoxDesc *__restrict__ boxes, int nb, int total_tiles, int in_sel, int out_sel, int half,
                   int final_stage) {
   __shared__ BoxDesc sb;

@@ -13,6 +13,18 @@
 // The per-cell work lives in cell_ops.cuh, shared with the batch kernels.
 #include "cell_ops.cuh"
 
+// Resident CTAs per SM asked of the compiler (register budget) for the two
+// update kernels, both bound by memory latency: measured on the 128x256x64
+// box, k_cell_ct is fastest at 4 (64 registers; 5 spills), k_cell_prim at 6
+// with power-of-two spacings (40 registers, 16 bytes of spill) and at 4
+// otherwise (no spill).
+#ifndef NMHD_CT_MIN_BLOCKS
+#define NMHD_CT_MIN_BLOCKS 4
+#endif
+#ifndef NMHD_PRIM_MIN_BLOCKS
+#define NMHD_PRIM_MIN_BLOCKS (kPow2 ? 6 : 4)
+#endif
+
 namespace nmhd {
 
 namespace {
@@ -36,7 +48,7 @@ __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const S
 }
 
 template <bool kPow2>
-__global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
+__global__ void __launch_bounds__(kThreads, NMHD_CT_MIN_BLOCKS) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
                                                          float *w1, float *wp,
                                                          const float *__restrict__ flux, int in_sel,
                                                          int out_sel, int half, int z0, int z1) {
@@ -52,7 +64,7 @@ __global__ void __launch_bounds__(kThreads, 4) k_cell_ct(GridParams g, const Ste
 }
 
 template <bool kPow2>
-__global__ void __launch_bounds__(kThreads, 4) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
+__global__ void __launch_bounds__(kThreads, NMHD_PRIM_MIN_BLOCKS) k_cell_prim(GridParams g, StepCtl *ctl, float *w0,
                                                            float *w1, float *wp,
                                                            const float *__restrict__ flux, float *dt_hist,
                                                            int out_sel, int half, int final_stage, int z0,
