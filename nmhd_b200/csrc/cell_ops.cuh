@@ -157,50 +157,85 @@ __device__ __forceinline__ float upwind(float w, float f0, float f1) {
   return w > 0.0f ? f0 : (w < 0.0f ? f1 : 0.5f * (f0 + f1));
 }
 
-// Constrained transport of one stage (add_flux_kernel's B part,
-// mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
-// new face B on the cell's lower x-, y- and z-face, written into wo.  The 18
-// corner fluxes (corner(), at the cell's edges and one step up each in-plane
-// axis) read 39 distinct velocities and 30 distinct fluxes; each is loaded
-// once and every wind sum keeps corner()'s order.
-template <bool kPow2>
-__device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
-                                        const float *__restrict__ wb, float *__restrict__ wo,
-                                        const float *__restrict__ flux, int x, int y, int z, float dt) {
+// Sources of the constrained-transport inputs around one cell: velocity
+// component c (0..2) and B flux k (0..5: F_x(B_y), F_x(B_z), F_y(B_z),
+// F_y(B_x), F_z(B_x), F_z(B_y)) of the neighbour (dx, dy, dz), each in -1..1.
+// CtGlobal reads HBM through the periodic neighbour offsets of the cell;
+// a shared-memory tile is the other source (cell_stage.cu).
+struct CtGlobal {
+  const float *v[3];
+  const float *f[6];
+  int xm, xp, ym, yp, zm, zp;
+  __device__ __forceinline__ int off(int dx, int dy, int dz) const {
+    return (dx < 0 ? xm : dx > 0 ? xp : 0) + (dy < 0 ? ym : dy > 0 ? yp : 0) + (dz < 0 ? zm : dz > 0 ? zp : 0);
+  }
+  __device__ __forceinline__ float vel(int c, int dx, int dy, int dz) const { return __ldg(v[c] + off(dx, dy, dz)); }
+  __device__ __forceinline__ float flx(int k, int dx, int dy, int dz) const { return __ldg(f[k] + off(dx, dy, dz)); }
+};
+
+__device__ __forceinline__ CtGlobal ct_global(const GridParams &g, const float *win, const float *flux, int x,
+                                              int y, int z) {
   const size_t N = (size_t)g.n;
   const int o = (z * g.sy + y) * g.sx + x;
   const Offsets f = offsets(g, x, y, z);
-  const int xm = f.xm1, xp = f.xp1, ym = f.ym1, yp = f.yp1, zm = f.zm1, zp = f.zp1;
-  const float *vx = win + N + o, *vy = win + 2 * N + o, *vz = win + 3 * N + o;
-  // velocities around the cell (offsets from o)
-  const float x_0 = __ldg(vx), x_xm = __ldg(vx + xm), x_ym = __ldg(vx + ym), x_ymxm = __ldg(vx + ym + xm);
-  const float x_yp = __ldg(vx + yp), x_ypxm = __ldg(vx + yp + xm), x_xp = __ldg(vx + xp);
-  const float x_xpym = __ldg(vx + xp + ym), x_zm = __ldg(vx + zm), x_zmxm = __ldg(vx + zm + xm);
-  const float x_zp = __ldg(vx + zp), x_zpxm = __ldg(vx + zp + xm), x_xpzm = __ldg(vx + xp + zm);
-  const float y_0 = __ldg(vy), y_ym = __ldg(vy + ym), y_xm = __ldg(vy + xm), y_xmym = __ldg(vy + xm + ym);
-  const float y_yp = __ldg(vy + yp), y_ypxm = __ldg(vy + yp + xm), y_xp = __ldg(vy + xp);
-  const float y_xpym = __ldg(vy + xp + ym), y_zm = __ldg(vy + zm), y_zmym = __ldg(vy + zm + ym);
-  const float y_zp = __ldg(vy + zp), y_zpym = __ldg(vy + zp + ym), y_ypzm = __ldg(vy + yp + zm);
-  const float z_0 = __ldg(vz), z_zm = __ldg(vz + zm), z_xm = __ldg(vz + xm), z_xmzm = __ldg(vz + xm + zm);
-  const float z_zp = __ldg(vz + zp), z_zpxm = __ldg(vz + zp + xm), z_xp = __ldg(vz + xp);
-  const float z_xpzm = __ldg(vz + xp + zm), z_ym = __ldg(vz + ym), z_ymzm = __ldg(vz + ym + zm);
-  const float z_zpym = __ldg(vz + zp + ym), z_yp = __ldg(vz + yp), z_ypzm = __ldg(vz + yp + zm);
-  // B fluxes (offsets from o)
-  const float *FxBy = flux + 5 * N + o, *FxBz = flux + 6 * N + o;
-  const float *FyBz = flux + 12 * N + o, *FyBx = flux + 13 * N + o;
-  const float *FzBx = flux + 19 * N + o, *FzBy = flux + 20 * N + o;
-  const float xy_0 = __ldg(FxBy), xy_ym = __ldg(FxBy + ym), xy_yp = __ldg(FxBy + yp), xy_xp = __ldg(FxBy + xp),
-              xy_xpym = __ldg(FxBy + xp + ym);
-  const float yx_0 = __ldg(FyBx), yx_xm = __ldg(FyBx + xm), yx_yp = __ldg(FyBx + yp),
-              yx_ypxm = __ldg(FyBx + yp + xm), yx_xp = __ldg(FyBx + xp);
-  const float xz_0 = __ldg(FxBz), xz_zm = __ldg(FxBz + zm), xz_zp = __ldg(FxBz + zp), xz_xp = __ldg(FxBz + xp),
-              xz_xpzm = __ldg(FxBz + xp + zm);
-  const float zx_0 = __ldg(FzBx), zx_xm = __ldg(FzBx + xm), zx_zp = __ldg(FzBx + zp),
-              zx_zpxm = __ldg(FzBx + zp + xm), zx_xp = __ldg(FzBx + xp);
-  const float yz_0 = __ldg(FyBz), yz_zm = __ldg(FyBz + zm), yz_zp = __ldg(FyBz + zp), yz_yp = __ldg(FyBz + yp),
-              yz_ypzm = __ldg(FyBz + yp + zm);
-  const float zy_0 = __ldg(FzBy), zy_ym = __ldg(FzBy + ym), zy_zp = __ldg(FzBy + zp),
-              zy_zpym = __ldg(FzBy + zp + ym), zy_yp = __ldg(FzBy + yp);
+  CtGlobal s;
+  s.v[0] = win + N + o;
+  s.v[1] = win + 2 * N + o;
+  s.v[2] = win + 3 * N + o;
+  s.f[0] = flux + 5 * N + o;
+  s.f[1] = flux + 6 * N + o;
+  s.f[2] = flux + 12 * N + o;
+  s.f[3] = flux + 13 * N + o;
+  s.f[4] = flux + 19 * N + o;
+  s.f[5] = flux + 20 * N + o;
+  s.xm = f.xm1;
+  s.xp = f.xp1;
+  s.ym = f.ym1;
+  s.yp = f.yp1;
+  s.zm = f.zm1;
+  s.zp = f.zp1;
+  return s;
+}
+
+// Constrained transport of one stage (add_flux_kernel's B part,
+// mhd_solver.inlrb:695-712, summed over the x, y, z sweeps in that order):
+// new face B on the lower x-, y- and z-face of cell o, written into wo.  The
+// 18 corner fluxes (corner(), at the cell's edges and one step up each
+// in-plane axis) read 39 distinct velocities and 30 distinct fluxes; each is
+// read once and every wind sum keeps corner()'s order.
+template <bool kPow2, class Src>
+__device__ __forceinline__ void ct_core(const GridParams &g, const Src &S, const float *__restrict__ wb,
+                                        float *__restrict__ wo, int o, float dt) {
+  const size_t N = (size_t)g.n;
+  // velocities around the cell
+  const float x_0 = S.vel(0, 0, 0, 0), x_xm = S.vel(0, -1, 0, 0), x_ym = S.vel(0, 0, -1, 0);
+  const float x_ymxm = S.vel(0, -1, -1, 0), x_yp = S.vel(0, 0, 1, 0), x_ypxm = S.vel(0, -1, 1, 0);
+  const float x_xp = S.vel(0, 1, 0, 0), x_xpym = S.vel(0, 1, -1, 0), x_zm = S.vel(0, 0, 0, -1);
+  const float x_zmxm = S.vel(0, -1, 0, -1), x_zp = S.vel(0, 0, 0, 1), x_zpxm = S.vel(0, -1, 0, 1);
+  const float x_xpzm = S.vel(0, 1, 0, -1);
+  const float y_0 = S.vel(1, 0, 0, 0), y_ym = S.vel(1, 0, -1, 0), y_xm = S.vel(1, -1, 0, 0);
+  const float y_xmym = S.vel(1, -1, -1, 0), y_yp = S.vel(1, 0, 1, 0), y_ypxm = S.vel(1, -1, 1, 0);
+  const float y_xp = S.vel(1, 1, 0, 0), y_xpym = S.vel(1, 1, -1, 0), y_zm = S.vel(1, 0, 0, -1);
+  const float y_zmym = S.vel(1, 0, -1, -1), y_zp = S.vel(1, 0, 0, 1), y_zpym = S.vel(1, 0, -1, 1);
+  const float y_ypzm = S.vel(1, 0, 1, -1);
+  const float z_0 = S.vel(2, 0, 0, 0), z_zm = S.vel(2, 0, 0, -1), z_xm = S.vel(2, -1, 0, 0);
+  const float z_xmzm = S.vel(2, -1, 0, -1), z_zp = S.vel(2, 0, 0, 1), z_zpxm = S.vel(2, -1, 0, 1);
+  const float z_xp = S.vel(2, 1, 0, 0), z_xpzm = S.vel(2, 1, 0, -1), z_ym = S.vel(2, 0, -1, 0);
+  const float z_ymzm = S.vel(2, 0, -1, -1), z_zpym = S.vel(2, 0, -1, 1), z_yp = S.vel(2, 0, 1, 0);
+  const float z_ypzm = S.vel(2, 0, 1, -1);
+  // B fluxes
+  const float xy_0 = S.flx(0, 0, 0, 0), xy_ym = S.flx(0, 0, -1, 0), xy_yp = S.flx(0, 0, 1, 0);
+  const float xy_xp = S.flx(0, 1, 0, 0), xy_xpym = S.flx(0, 1, -1, 0);
+  const float xz_0 = S.flx(1, 0, 0, 0), xz_zm = S.flx(1, 0, 0, -1), xz_zp = S.flx(1, 0, 0, 1);
+  const float xz_xp = S.flx(1, 1, 0, 0), xz_xpzm = S.flx(1, 1, 0, -1);
+  const float yz_0 = S.flx(2, 0, 0, 0), yz_zm = S.flx(2, 0, 0, -1), yz_zp = S.flx(2, 0, 0, 1);
+  const float yz_yp = S.flx(2, 0, 1, 0), yz_ypzm = S.flx(2, 0, 1, -1);
+  const float yx_0 = S.flx(3, 0, 0, 0), yx_xm = S.flx(3, -1, 0, 0), yx_yp = S.flx(3, 0, 1, 0);
+  const float yx_ypxm = S.flx(3, -1, 1, 0), yx_xp = S.flx(3, 1, 0, 0);
+  const float zx_0 = S.flx(4, 0, 0, 0), zx_xm = S.flx(4, -1, 0, 0), zx_zp = S.flx(4, 0, 0, 1);
+  const float zx_zpxm = S.flx(4, -1, 0, 1), zx_xp = S.flx(4, 1, 0, 0);
+  const float zy_0 = S.flx(5, 0, 0, 0), zy_ym = S.flx(5, 0, -1, 0), zy_zp = S.flx(5, 0, 0, 1);
+  const float zy_zpym = S.flx(5, 0, -1, 1), zy_yp = S.flx(5, 0, 1, 0);
   // corner(vb, fb, e, mb, ma): wind vb[e] + vb[e+mb] + vb[e+ma] + vb[e+ma+mb],
   // f0 = fb[e+mb], f1 = fb[e]
   const float XY00 = upwind(y_0 + y_ym + y_xm + y_xmym, xy_ym, xy_0);            // F_x(B_y), wind v_y
@@ -237,6 +272,14 @@ __device__ __forceinline__ void ct_cell(const GridParams &g, const float *__rest
   pb = pb - divs<kPow2>(0.5f * (YZ10 - YZ00), dy, iy);
   pb = pb + 0.5f * (divs<kPow2>(ZX10 - ZX00, dx, ix) + divs<kPow2>(ZY10 - ZY00, dy, iy));
   wo[7 * N + o] = wb[7 * N + o] + dt * pb;
+}
+
+// ct_core reading HBM directly (the batched-ensemble kernels).
+template <bool kPow2>
+__device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
+                                        const float *__restrict__ wb, float *__restrict__ wo,
+                                        const float *__restrict__ flux, int x, int y, int z, float dt) {
+  ct_core<kPow2>(g, ct_global(g, win, flux, x, y, z), wb, wo, (z * g.sy + y) * g.sx + x, dt);
 }
 
 // Rest of the stage for cell (x, y, z): flux divergence of rho, m, E
