@@ -160,8 +160,7 @@ __device__ __forceinline__ float upwind(float w, float f0, float f1) {
 // Sources of the constrained-transport inputs around one cell: velocity
 // component c (0..2) and B flux k (0..5: F_x(B_y), F_x(B_z), F_y(B_z),
 // F_y(B_x), F_z(B_x), F_z(B_y)) of the neighbour (dx, dy, dz), each in -1..1.
-// CtGlobal reads HBM through the periodic neighbour offsets of the cell;
-// a shared-memory tile is the other source (cell_stage.cu).
+// CtGlobal reads HBM through the periodic neighbour offsets of the cell.
 struct CtGlobal {
   const float *v[3];
   const float *f[6];
@@ -274,7 +273,7 @@ __device__ __forceinline__ void ct_core(const GridParams &g, const Src &S, const
   wo[7 * N + o] = wb[7 * N + o] + dt * pb;
 }
 
-// ct_core reading HBM directly (the batched-ensemble kernels).
+// ct_core reading HBM directly.
 template <bool kPow2>
 __device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
                                         const float *__restrict__ wb, float *__restrict__ wo,

@@ -15,11 +15,12 @@
 
 // Resident CTAs per SM asked of the compiler (register budget) for the two
 // update kernels, both bound by memory latency: measured on the 128x256x64
-// box, k_cell_ct is fastest at 5 with power-of-two spacings (48 registers, no
-// spill; 6 is slower) and k_cell_prim at 6 (40 registers, 16 bytes of spill);
-// with other spacings both take 4, where they do not spill.
+// box, k_cell_ct is fastest at 4 (64 registers; 5 spills) and k_cell_prim at
+// 6 with power-of-two spacings (40 registers, 16 bytes of spill), 4 otherwise
+// (no spill).  Staging the CT stencil through a shared-memory tile (34x6x4
+// cells, 9 fields) measured no faster than these direct loads.
 #ifndef NMHD_CT_MIN_BLOCKS
-#define NMHD_CT_MIN_BLOCKS (kPow2 ? 5 : 4)
+#define NMHD_CT_MIN_BLOCKS 4
 #endif
 #ifndef NMHD_PRIM_MIN_BLOCKS
 #define NMHD_PRIM_MIN_BLOCKS (kPow2 ? 6 : 4)
@@ -47,62 +48,20 @@ __global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const S
   flux_cell(g, pick(ctl, in_sel, w0, w1, wp), flux, x, y, z, dt);
 }
 
-// Shared-memory source of ct_core: the CTA's cells plus one cell of halo on
-// every side (34 x 6 x 4), 3 velocities and 6 B fluxes each, filled with
-// coalesced loads (periodic wrap applied once per tile cell); each thread then
-// reads its 69 inputs at fixed offsets from its own tile cell.
-constexpr int TX = BX + 2, TY = BY + 2, TZ = BZ + 2, kTileCells = TX * TY * TZ;
-constexpr int kCtFields = 9;  // v_x, v_y, v_z, F_x(B_y), F_x(B_z), F_y(B_z), F_y(B_x), F_z(B_x), F_z(B_y)
-
-struct CtTile {
-  const float *t;  // field 0 at this thread's cell
-  __device__ __forceinline__ float vel(int c, int dx, int dy, int dz) const {
-    return t[c * kTileCells + (dz * TY + dy) * TX + dx];
-  }
-  __device__ __forceinline__ float flx(int k, int dx, int dy, int dz) const {
-    return t[(3 + k) * kTileCells + (dz * TY + dy) * TX + dx];
-  }
-};
-
-__device__ __forceinline__ int wrap_mod(int v, int s) {
-  v %= s;
-  return v < 0 ? v + s : v;
-}
-
 template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, NMHD_CT_MIN_BLOCKS) k_cell_ct(GridParams g, const StepCtl *ctl, float *w0,
                                                                           float *w1, float *wp,
                                                                           const float *__restrict__ flux, int in_sel,
                                                                           int out_sel, int half, int z0, int z1) {
-  __shared__ float tile[kCtFields * kTileCells];
   if (ctl->done) return;
-  const size_t N = (size_t)g.n;
-  const int bx0 = blockIdx.x * BX, by0 = blockIdx.y * BY, bz0 = z0 + blockIdx.z * BZ;
-  const float *win = pick(ctl, in_sel, w0, w1, wp);
-  const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
-  for (int i = tid; i < kTileCells; i += kThreads) {
-    const int ix = i % TX, iy = (i / TX) % TY, iz = i / (TX * TY);
-    const int gx = wrap_mod(bx0 - 1 + ix, g.sx), gy = wrap_mod(by0 - 1 + iy, g.sy);
-    const int gz = wrap_mod(bz0 - 1 + iz, g.sz);
-    const int gi = (gz * g.sy + gy) * g.sx + gx;
-    tile[0 * kTileCells + i] = __ldg(win + N + gi);
-    tile[1 * kTileCells + i] = __ldg(win + 2 * N + gi);
-    tile[2 * kTileCells + i] = __ldg(win + 3 * N + gi);
-    tile[3 * kTileCells + i] = __ldg(flux + 5 * N + gi);
-    tile[4 * kTileCells + i] = __ldg(flux + 6 * N + gi);
-    tile[5 * kTileCells + i] = __ldg(flux + 12 * N + gi);
-    tile[6 * kTileCells + i] = __ldg(flux + 13 * N + gi);
-    tile[7 * kTileCells + i] = __ldg(flux + 19 * N + gi);
-    tile[8 * kTileCells + i] = __ldg(flux + 20 * N + gi);
-  }
-  __syncthreads();
-  const int x = bx0 + threadIdx.x, y = by0 + threadIdx.y, z = bz0 + threadIdx.z;
+  const int x = blockIdx.x * BX + threadIdx.x;
+  const int y = blockIdx.y * BY + threadIdx.y;
+  const int z = z0 + blockIdx.z * BZ + threadIdx.z;
   if (x >= g.sx || y >= g.sy || z >= z1) return;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
-  const CtTile src{tile + ((threadIdx.z + 1) * TY + (threadIdx.y + 1)) * TX + (threadIdx.x + 1)};
-  ct_core<kPow2>(g, src, pick(ctl, 0, w0, w1, wp), const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)),
-                 (z * g.sy + y) * g.sx + x, dt);
+  ct_cell<kPow2>(g, pick(ctl, in_sel, w0, w1, wp), pick(ctl, 0, w0, w1, wp),
+                 const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)), flux, x, y, z, dt);
 }
 
 template <bool kPow2>
