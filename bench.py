@@ -289,10 +289,12 @@ def run_gpu_arm(args):
         peak, peak_kind = load_peaks()
         # the RK2 step is the unit: 160 algorithmic bytes per cell-update
         achieved = BYTES_PER_CELL_UPDATE * cells / (kernel_ms_step * 1e-3) / 1e9
-        traffic = None
+        traffic, winst = None, None
         tf = os.path.join(ROOT, "profiles", "traffic_" + wl + ".json")
         if os.path.exists(tf):
-            traffic = json.load(open(tf)).get("dram_bytes_per_step")
+            tj = json.load(open(tf))
+            traffic = tj.get("dram_bytes_per_step")
+            winst = tj.get("warp_instructions_per_step")
         launches_per_step = sum(k for _, k in prof.values())
         line = {
             "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s",
@@ -312,6 +314,18 @@ def run_gpu_arm(args):
             "gpu_launches": int(round(launches_per_step * args.steps)),
             "clocks": clocks.summary(),
         }
+        if winst:
+            # the bound the step actually meets: instruction issue (one warp
+            # instruction per cycle per SM sub-partition), from the ncu count
+            # of warp instructions per step at the sampled SM clock
+            cs = line["clocks"] or {}
+            mhz = cs.get("sm_mhz") or 1965.0
+            sms = torch.cuda.get_device_properties(dev).multi_processor_count
+            peak_i = sms * 4 * mhz * 1e6 / 1e9
+            ach_i = winst / (ms_per_step * 1e-3) / 1e9
+            line["issue_roofline"] = {"bound": "issue", "achieved": ach_i, "peak": peak_i,
+                                      "unit": "G warp-instructions/s", "frac": ach_i / peak_i,
+                                      "warp_instructions_per_step": winst, "sm_mhz": mhz, "sms": sms}
         if tuning:
             line["autotune_ms_per_step"] = {f"v{a}_r{b}_z{c}": round(d, 4) for a, b, c, d in tuning}
         if world == 1 and not args.no_cpu:
