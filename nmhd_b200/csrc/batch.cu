@@ -54,10 +54,14 @@ __device__ __forceinline__ int find_box(int nb, long long i, F begin) {
 
 // One stage kernel over all boxes.  KIND 0: face fluxes, 1: constrained
 // transport, 2: conserved update + primitive recovery (+ CFL and clock in the
-// final stage).  3 CTAs/SM, except 4 for the conserved update (bound by
-// memory latency; more would spill, as would 4 for the CT kind).
+// final stage).  Resident CTAs per SM asked of the compiler: the flux kind
+// NMHD_BATCH_FLUX_MIN_BLOCKS, the CT kind 3 (4 would spill), the conserved
+// update 4.
+#ifndef NMHD_BATCH_FLUX_MIN_BLOCKS
+#define NMHD_BATCH_FLUX_MIN_BLOCKS 3
+#endif
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, KIND == 2 ? 4 : 3)
+__global__ void __launch_bounds__(kThreads, KIND == 0 ? NMHD_BATCH_FLUX_MIN_BLOCKS : (KIND == 1 ? 3 : 4))
     k_batch_stage(const BoxDesc *__restrict__ boxes, int nb, int total_tiles, int in_sel, int out_sel, int half,
                   int final_stage) {
   __shared__ BoxDesc sb;
@@ -93,8 +97,8 @@ __global__ void __launch_bounds__(kThreads, KIND == 2 ? 4 : 3)
       if (inside) {
         const float *win = pick(ctl, in_sel, sb.w0, sb.w1, sb.wp), *wb = pick(ctl, 0, sb.w0, sb.w1, sb.wp);
         float *wo = const_cast<float *>(pick(ctl, out_sel, sb.w0, sb.w1, sb.wp));
-        if (g.pow2_spacing) ct_cell<true>(g, win, wb, wo, sb.flux, x, y, z, dt);
-        else ct_cell<false>(g, win, wb, wo, sb.flux, x, y, z, dt);
+        if (g.pow2_spacing) ct_cell<true, true>(g, win, wb, wo, sb.flux, x, y, z, dt);
+        else ct_cell<false, true>(g, win, wb, wo, sb.flux, x, y, z, dt);
       }
     } else {
       float tcfl = __uint_as_float(0x7f800000u);

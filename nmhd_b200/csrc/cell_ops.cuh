@@ -160,7 +160,8 @@ __device__ __forceinline__ float upwind(float w, float f0, float f1) {
 // Sources of the constrained-transport inputs around one cell: velocity
 // component c (0..2) and B flux k (0..5: F_x(B_y), F_x(B_z), F_y(B_z),
 // F_y(B_x), F_z(B_x), F_z(B_y)) of the neighbour (dx, dy, dz), each in -1..1.
-// CtGlobal reads HBM through the periodic neighbour offsets of the cell.
+// CtGlobal and CtGlobalLean read HBM through the periodic neighbour offsets
+// of the cell.
 struct CtGlobal {
   const float *v[3];
   const float *f[6];
@@ -187,6 +188,41 @@ __device__ __forceinline__ CtGlobal ct_global(const GridParams &g, const float *
   s.f[3] = flux + 13 * N + o;
   s.f[4] = flux + 19 * N + o;
   s.f[5] = flux + 20 * N + o;
+  s.xm = f.xm1;
+  s.xp = f.xp1;
+  s.ym = f.ym1;
+  s.yp = f.yp1;
+  s.zm = f.zm1;
+  s.zp = f.zp1;
+  return s;
+}
+
+// The same inputs through two base pointers (fewer live registers: the
+// batched kernels, which inline both spacing variants, spill less with it).
+struct CtGlobalLean {
+  const float *win, *flux;  // the stage input and the flux scratch, at cell o
+  size_t N;
+  int xm, xp, ym, yp, zm, zp;
+  __device__ __forceinline__ int off(int dx, int dy, int dz) const {
+    return (dx < 0 ? xm : dx > 0 ? xp : 0) + (dy < 0 ? ym : dy > 0 ? yp : 0) + (dz < 0 ? zm : dz > 0 ? zp : 0);
+  }
+  __device__ __forceinline__ float vel(int c, int dx, int dy, int dz) const {
+    return __ldg(win + (1 + c) * N + off(dx, dy, dz));
+  }
+  __device__ __forceinline__ float flx(int k, int dx, int dy, int dz) const {
+    // F_x(B_y), F_x(B_z), F_y(B_z), F_y(B_x), F_z(B_x), F_z(B_y): fields 5, 6, 12, 13, 19, 20
+    return __ldg(flux + (5 + (k >> 1) * 7 + (k & 1)) * N + off(dx, dy, dz));
+  }
+};
+
+__device__ __forceinline__ CtGlobalLean ct_global_lean(const GridParams &g, const float *win, const float *flux, int x,
+                                              int y, int z) {
+  const int o = (z * g.sy + y) * g.sx + x;
+  const Offsets f = offsets(g, x, y, z);
+  CtGlobalLean s;
+  s.win = win + o;
+  s.flux = flux + o;
+  s.N = (size_t)g.n;
   s.xm = f.xm1;
   s.xp = f.xp1;
   s.ym = f.ym1;
@@ -273,12 +309,16 @@ __device__ __forceinline__ void ct_core(const GridParams &g, const Src &S, const
   wo[7 * N + o] = wb[7 * N + o] + dt * pb;
 }
 
-// ct_core reading HBM directly.
-template <bool kPow2>
+// ct_core reading HBM directly (kLean: through CtGlobalLean).
+template <bool kPow2, bool kLean = false>
 __device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
                                         const float *__restrict__ wb, float *__restrict__ wo,
                                         const float *__restrict__ flux, int x, int y, int z, float dt) {
-  ct_core<kPow2>(g, ct_global(g, win, flux, x, y, z), wb, wo, (z * g.sy + y) * g.sx + x, dt);
+  const int o = (z * g.sy + y) * g.sx + x;
+  if (kLean)
+    ct_core<kPow2>(g, ct_global_lean(g, win, flux, x, y, z), wb, wo, o, dt);
+  else
+    ct_core<kPow2>(g, ct_global(g, win, flux, x, y, z), wb, wo, o, dt);
 }
 
 // Rest of the stage for cell (x, y, z): flux divergence of rho, m, E

@@ -19,6 +19,12 @@
 // 6 with power-of-two spacings (40 registers, 16 bytes of spill), 4 otherwise
 // (no spill).  Staging the CT stencil through a shared-memory tile (34x6x4
 // cells, 9 fields) measured no faster than these direct loads.
+// k_cell_flux is issue-bound: 4 CTAs/SM (64 registers, 16 bytes of spill) hide
+// its fixed-latency waits better than 3 (78 registers): -3 % per launch; 5
+// spills 100 bytes and is slower.
+#ifndef NMHD_FLUX_MIN_BLOCKS
+#define NMHD_FLUX_MIN_BLOCKS 4
+#endif
 #ifndef NMHD_CT_MIN_BLOCKS
 #define NMHD_CT_MIN_BLOCKS 4
 #endif
@@ -34,7 +40,7 @@ using namespace cell;
 
 // Every kernel covers the z planes [z0, z1) (the whole box, or one chunk of
 // the chunked pipeline).
-__global__ void __launch_bounds__(kThreads, 3) k_cell_flux(GridParams g, const StepCtl *ctl, const float *w0,
+__global__ void __launch_bounds__(kThreads, NMHD_FLUX_MIN_BLOCKS) k_cell_flux(GridParams g, const StepCtl *ctl, const float *w0,
                                                            const float *w1, const float *wp,
                                                            float *__restrict__ flux, int in_sel, int half, int z0,
                                                            int z1) {
