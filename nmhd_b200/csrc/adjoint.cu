@@ -38,7 +38,8 @@ namespace {
 constexpr int BX = 32, BY = 4, BZ = 2;
 
 // Resident CTAs per SM asked of the compiler: the FP32 HLLD adjoint is
-// latency-bound at one 256-thread CTA per SM, so it is held to 128 registers.
+// latency-bound at one 256-thread CTA per SM, so it is held to 128 registers
+// (2 CTAs).
 template <class F>
 struct MinBlocks {
   static constexpr int value = 1;
@@ -46,6 +47,25 @@ struct MinBlocks {
 template <int AX>
 struct MinBlocks<OpAFlux<float, AX>> {
   static constexpr int value = 2;
+};
+// The gather passes (reconstruction transposes, primitive and face-B
+// adjoints) are bound by memory latency: 8 CTAs/SM (32 registers, no spill)
+// took the adjoint kernels from 72.6 to 68.6 ms on 64^3 x 200 steps; 6 gained
+// nothing.
+#ifndef NMHD_AD_GATHER_MIN_BLOCKS
+#define NMHD_AD_GATHER_MIN_BLOCKS 8
+#endif
+template <int AX>
+struct MinBlocks<OpARecon<float, AX>> {
+  static constexpr int value = NMHD_AD_GATHER_MIN_BLOCKS;
+};
+template <>
+struct MinBlocks<OpAPrim<float>> {
+  static constexpr int value = NMHD_AD_GATHER_MIN_BLOCKS;
+};
+template <>
+struct MinBlocks<OpABface<float>> {
+  static constexpr int value = NMHD_AD_GATHER_MIN_BLOCKS;
 };
 
 template <class F, int kMinBlocks>
