@@ -197,6 +197,34 @@ __device__ __forceinline__ CtGlobal ct_global(const GridParams &g, const float *
   return s;
 }
 
+// The same inputs for a cell whose neighbours need no periodic wrap: x
+// neighbours at constant offsets, y and z ones at +-Sx and +-Sx*Sy.
+struct CtInterior {
+  const float *v[3];
+  const float *f[6];
+  int sx, sxy;
+  __device__ __forceinline__ int off(int dx, int dy, int dz) const { return dx + dy * sx + dz * sxy; }
+  __device__ __forceinline__ float vel(int c, int dx, int dy, int dz) const { return __ldg(v[c] + off(dx, dy, dz)); }
+  __device__ __forceinline__ float flx(int k, int dx, int dy, int dz) const { return __ldg(f[k] + off(dx, dy, dz)); }
+};
+
+__device__ __forceinline__ CtInterior ct_interior(const GridParams &g, const float *win, const float *flux, int o) {
+  const size_t N = (size_t)g.n;
+  CtInterior s;
+  s.v[0] = win + N + o;
+  s.v[1] = win + 2 * N + o;
+  s.v[2] = win + 3 * N + o;
+  s.f[0] = flux + 5 * N + o;
+  s.f[1] = flux + 6 * N + o;
+  s.f[2] = flux + 12 * N + o;
+  s.f[3] = flux + 13 * N + o;
+  s.f[4] = flux + 19 * N + o;
+  s.f[5] = flux + 20 * N + o;
+  s.sx = g.sx;
+  s.sxy = g.sx * g.sy;
+  return s;
+}
+
 // The same inputs through two base pointers (fewer live registers: the
 // batched kernels, which inline both spacing variants, spill less with it).
 struct CtGlobalLean {

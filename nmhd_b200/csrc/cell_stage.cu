@@ -66,8 +66,17 @@ __global__ void __launch_bounds__(kThreads, NMHD_CT_MIN_BLOCKS) k_cell_ct(GridPa
   if (x >= g.sx || y >= g.sy || z >= z1) return;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
-  ct_cell<kPow2>(g, pick(ctl, in_sel, w0, w1, wp), pick(ctl, 0, w0, w1, wp),
-                 const_cast<float *>(pick(ctl, out_sel, w0, w1, wp)), flux, x, y, z, dt);
+  const float *win = pick(ctl, in_sel, w0, w1, wp), *wb = pick(ctl, 0, w0, w1, wp);
+  float *wo = const_cast<float *>(pick(ctl, out_sel, w0, w1, wp));
+  // CTAs whose cells and their +-1 neighbours all lie inside the box (uniform
+  // per CTA) address the neighbours without the periodic wrap
+  const int bx0 = blockIdx.x * BX, by0 = blockIdx.y * BY, bz0 = z0 + blockIdx.z * BZ;
+  const bool inner = bx0 >= 1 && bx0 + BX < g.sx && by0 >= 1 && by0 + BY < g.sy && bz0 >= 1 && bz0 + BZ < g.sz;
+  const int o = (z * g.sy + y) * g.sx + x;
+  if (inner)
+    ct_core<kPow2>(g, ct_interior(g, win, flux, o), wb, wo, o, dt);
+  else
+    ct_core<kPow2>(g, ct_global(g, win, flux, x, y, z), wb, wo, o, dt);
 }
 
 template <bool kPow2>
