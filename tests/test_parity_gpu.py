@@ -91,6 +91,30 @@ def test_gpu_full_size_mri_box_matches_oracle_and_keeps_div_b(gpu):
     assert abs(d1["mass"] - d0["mass"]) < 1e-6 * d0["mass"]
 
 
+def test_gpu_large_box_matches_oracle_and_keeps_div_b(gpu):
+    """The 512(radial) x 1024(azimuthal) x 256 box of the large-box benchmark
+    (136 M cells with margins): one step bitwise against the oracle, then div B
+    at roundoff and mass conserved after ten more steps.  The oracle's step takes
+    ~22 GB of host memory and a minute or two on the host cores."""
+    import psutil
+    if psutil.virtual_memory().available < 32 * 2 ** 30:
+        pytest.skip("not enough host memory for the oracle at this size")
+    cfg, s = shearing_box(n_radial=512, n_azimuthal=1024, n_vertical=256, seed=3)
+    o = oracle.proceed(cfg, s, 1)
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        del s
+        d0 = sol.diagnostics()
+        sol.step(1)
+        assert sol.current_time() == o["time"]
+        assert_same(sol.get_state(), o["state"])
+        del o
+        sol.step(10)
+        d1 = sol.diagnostics()
+    assert d1["max_div_b"] < 1e-4 * math.sqrt(2 / 400) * 512
+    assert abs(d1["mass"] - d0["mass"]) < 1e-6 * d0["mass"]
+
+
 def test_chunked_proceed_equals_single_call(gpu):
     cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=9)
     with MHDSolver(cfg) as a, MHDSolver(cfg) as b:
