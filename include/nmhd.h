@@ -47,6 +47,21 @@ typedef enum nmhd_problem {
   NMHD_PROBLEM_SHEARING_BOX = 1  /* Coriolis + tidal acceleration, shearing-periodic Y margins */
 } nmhd_problem;
 
+/* Options beyond the reference's scheme (nmhd_config.flags). */
+typedef enum nmhd_flag {
+  /* Refill the margins of the RK2 predictor from the interior before the
+   * second stage (the Y shear fill with the displacement at t + dt/2, and the
+   * Z copy).  The reference fills margins once per step and advances them
+   * like the interior, so its second stage reads margin cells evolved in the
+   * margin's own frame (from wrapped neighbours within two cells of the box
+   * edge) and its interior depends on the margin width; with this flag the
+   * interior results are the same, bitwise, for any margin width from 2, and
+   * differ from the reference's scheme by truncation error.  Whole boxes
+   * only (nmhd_proceed and the one-slab step); the batched, multi-slab and
+   * adjoint paths return NMHD_ERR_NOT_SUPPORTED or reject the config. */
+  NMHD_FLAG_HALO_PER_STAGE = 1
+} nmhd_flag;
+
 /* Runtime form of the reference's compile-time simulation_config.h
  * (src/library/simulation_config_default.h, application overrides). */
 typedef struct nmhd_config {
@@ -59,7 +74,7 @@ typedef struct nmhd_config {
   float q, omega;                 /* kDifferentialRotationIndex, kOmega (shearing box) */
   int32_t space_order;            /* 2: minbee (reference default), 1: piecewise constant */
   int32_t time_order;             /* 2: midpoint RK2 (reference default), 1: Euler */
-  int32_t flags;                  /* reserved, 0 */
+  int32_t flags;                  /* nmhd_flag bits, 0: the reference's scheme */
   /* kParallelSizeY: 0 or 1 for a whole box; P > 1 makes this solver one
    * radial slab of a box split over P ranks along Y (size_y counts the slab's
    * rows and margins, extent_y is the whole box's).  Its Y margins then come

@@ -17,6 +17,8 @@ from dataclasses import dataclass, asdict
 import numpy as np
 
 PROBLEMS = {"none": 0, "shearing_box": 1}
+# nmhd_config.flags bits (nmhd_flag in include/nmhd.h)
+FLAG_HALO_PER_STAGE = 1  # refill the RK2 predictor's margins before the second stage
 
 
 class NmhdConfig(ctypes.Structure):

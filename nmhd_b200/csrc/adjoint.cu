@@ -236,6 +236,8 @@ nmhd_status validate(nmhd_solver *s, int nsteps, int ckpt, const nmhd_loss_spec 
     return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "no interior cells");
   if (s->cfg.parallel_size_y > 1)
     return set_err(s, NMHD_ERR_NOT_SUPPORTED, "the differentiated step covers a whole box, not a radial slab");
+  if (s->cfg.flags)
+    return set_err(s, NMHD_ERR_NOT_SUPPORTED, "the differentiated step is the reference's scheme (flags 0)");
   return NMHD_OK;
 }
 

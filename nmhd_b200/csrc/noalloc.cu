@@ -64,7 +64,7 @@ extern "C" nmhd_status nmhd_advance_noalloc(const nmhd_config *cfg, const float 
   if (cfg->margin_y < 0 || cfg->margin_z < 0 || cfg->size_y - 2 * cfg->margin_y < cfg->margin_y ||
       (cfg->margin_z > 0 && cfg->size_z - 2 * cfg->margin_z < cfg->margin_z) ||
       !(cfg->gamma > 1.0f) || !(cfg->cfl > 0.0f) || (cfg->space_order != 1 && cfg->space_order != 2) ||
-      (cfg->time_order != 1 && cfg->time_order != 2) || cfg->parallel_size_y > 1 ||
+      (cfg->time_order != 1 && cfg->time_order != 2) || cfg->parallel_size_y > 1 || cfg->flags != 0 ||
       (cfg->problem != NMHD_PROBLEM_NONE && cfg->problem != NMHD_PROBLEM_SHEARING_BOX))
     return noalloc_fail(NMHD_ERR_INVALID_ARGUMENT, "invalid configuration (a whole box is required)");
   int dev = 0;

@@ -119,6 +119,10 @@ nmhd_status validate(const nmhd_config *c, std::string &why) {
   if (c->space_order != 1 && c->space_order != 2) { why = "space_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->time_order != 1 && c->time_order != 2) { why = "time_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->parallel_size_y < 0) { why = "parallel_size_y must be >= 0"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->flags & ~NMHD_FLAG_HALO_PER_STAGE) { why = "unknown flags"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if ((c->flags & NMHD_FLAG_HALO_PER_STAGE) && c->parallel_size_y > 1) {
+    why = "per-stage margin fill is for whole boxes"; return NMHD_ERR_NOT_SUPPORTED;
+  }
   if (c->parallel_size_y > 1 && c->margin_y < 1) {
     why = "a radial slab (parallel_size_y > 1) needs margin_y >= 1"; return NMHD_ERR_INVALID_ARGUMENT;
   }
@@ -171,6 +175,7 @@ void enqueue_step(nmhd_solver *s) {
     enqueue_stage(s, 0, 1, 0, 1, st);
   } else {
     enqueue_stage(s, 0, 2, 1, 0, st);
+    if (s->cfg.flags & NMHD_FLAG_HALO_PER_STAGE) nmhd::launch_fill_predictor(g, s->ctl, s->wp, st);
     enqueue_stage(s, 2, 1, 0, 1, st);
   }
 }
@@ -548,6 +553,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       whole(0, 2, 1, 0);
       NMHD_CUDA(s, cudaEventRecord(ev[3], q));
       upd_k(0, 2, 1, 0);
+      if (s->cfg.flags & NMHD_FLAG_HALO_PER_STAGE) nmhd::launch_fill_predictor(g, s->ctl, s->wp, q);
       NMHD_CUDA(s, cudaEventRecord(ev[4], q));
       flux_k(2, 0);
       whole(2, 1, 0, 1);
@@ -790,6 +796,7 @@ nmhd_status nmhd_step_stages(nmhd_solver *s) {
     enqueue_stage(s, 0, 1, 0, 1, s->stream);
   } else {
     enqueue_stage(s, 0, 2, 1, 0, s->stream);
+    if (s->cfg.flags & NMHD_FLAG_HALO_PER_STAGE) nmhd::launch_fill_predictor(s->g, s->ctl, s->wp, s->stream);
     enqueue_stage(s, 2, 1, 0, 1, s->stream);
   }
   NMHD_CUDA(s, cudaGetLastError());

@@ -150,6 +150,34 @@ __global__ void __launch_bounds__(kBlock) k_fill_y(GridParams g, StepCtl *ctl, f
   margin::fill_y_item(g, ctl->time, w, idx);
 }
 
+// Margin fill of the RK2 predictor wp before the second stage
+// (NMHD_FLAG_HALO_PER_STAGE): Y shear fill at the predictor's time t + dt/2,
+// then (second launch) the Z copy.
+__global__ void __launch_bounds__(kBlock) k_fill_predictor_y(GridParams g, StepCtl *ctl, float *wp) {
+  if (ctl->done) return;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= g.sx * g.my * g.sz) return;
+  float dt = step_dt(ctl, nullptr);
+  dt = dt / 2.0f;
+  margin::fill_y_item(g, ctl->time + (double)dt, wp, idx);
+}
+
+__global__ void __launch_bounds__(kBlock) k_fill_predictor_z(GridParams g, StepCtl *ctl, float *wp) {
+  if (ctl->done) return;
+  const int unit = g.sx * g.sy * g.mz;
+  const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= unit) return;
+  const int n = g.n;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    float *var = wp + v * n;
+    const float lo = var[n - 2 * unit + idx];
+    const float hi = var[unit + idx];
+    var[idx] = lo;
+    var[n - unit + idx] = hi;
+  }
+}
+
 // Halo exchange of a radial slab (kParallelSizeY > 1), split around the
 // caller's transport: k_halo_pack gathers this slab's shear-shifted boundary
 // rows into the two outgoing messages, k_halo_unpack scatters the two
@@ -577,6 +605,11 @@ void launch_cfl_margin(const GridParams &g, StepCtl *ctl, float *w0, float *w1, 
 void launch_fill(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t st) {
   if (g.my > 0) k_fill_y<<<blocks_for((long long)g.sx * g.my * g.sz), kBlock, 0, st>>>(g, ctl, w0, w1);
   if (g.mz > 0) k_fill_z<<<blocks_for((long long)g.sx * g.sy * g.mz), kBlock, 0, st>>>(g, ctl, w0, w1);
+}
+
+void launch_fill_predictor(const GridParams &g, StepCtl *ctl, float *wp, cudaStream_t st) {
+  if (g.my > 0) k_fill_predictor_y<<<blocks_for((long long)g.sx * g.my * g.sz), kBlock, 0, st>>>(g, ctl, wp);
+  if (g.mz > 0) k_fill_predictor_z<<<blocks_for((long long)g.sx * g.sy * g.mz), kBlock, 0, st>>>(g, ctl, wp);
 }
 
 void launch_halo_pack(const GridParams &g, StepCtl *ctl, const float *w0, const float *w1, float *send_inc,

@@ -57,6 +57,8 @@ constexpr int kFluxFields = 21;  // 3 face directions x 7 flux components
 void launch_cfl_all(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
 void launch_cfl_margin(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
 void launch_fill(const GridParams &g, StepCtl *ctl, float *w0, float *w1, cudaStream_t stream);
+// Margins of the RK2 predictor wp refilled at t + dt/2 (NMHD_FLAG_HALO_PER_STAGE).
+void launch_fill_predictor(const GridParams &g, StepCtl *ctl, float *wp, cudaStream_t stream);
 // Radial slab halo: gather the outgoing Y-boundary messages / scatter the
 // incoming ones into the Y margins and copy the Z margins.
 void launch_halo_pack(const GridParams &g, StepCtl *ctl, const float *w0, const float *w1, float *send_inc,

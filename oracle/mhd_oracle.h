@@ -33,7 +33,7 @@ typedef struct oracle_config {
   float q, omega;
   int32_t space_order; /* 2 minbee, 1 piecewise constant */
   int32_t time_order;  /* 2 midpoint, 1 Euler */
-  int32_t flags;
+  int32_t flags;       /* 1: margins refilled before the second RK2 stage */
 } oracle_config;
 
 /* float build (the reference's FP32) */

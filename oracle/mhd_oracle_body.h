@@ -568,6 +568,9 @@ int FN(oracle_proceed)(const oracle_config *cfg, real *state, double *time, int6
       FN(stage)(&s, dt, s.w, s.w, s.w);
     } else {
       FN(stage)(&s, dt / 2, s.w, s.w, s.wp);
+      /* nmhd_config flag HALO_PER_STAGE (no reference counterpart): the
+         predictor's margins refilled at its time t + dt/2 */
+      if (cfg->flags & 1) FN(shear_fill_impl)(cfg, &s.g, &s.k, s.wp, *time + (double)(dt / 2));
       FN(stage)(&s, dt, s.wp, s.w, s.w);
     }
     *time += (double)dt;

@@ -115,6 +115,33 @@ def test_gpu_large_box_matches_oracle_and_keeps_div_b(gpu):
     assert abs(d1["mass"] - d0["mass"]) < 1e-6 * d0["mass"]
 
 
+@pytest.mark.parametrize("case", ["ot_m2", "shear_m2", "shear_m4_mz2"])
+@pytest.mark.parametrize("variant", [2, 0])
+def test_per_stage_margin_fill_matches_oracle(gpu, case, variant):
+    """NMHD_FLAG_HALO_PER_STAGE: the predictor's margins refilled before the
+    second stage; bitwise the oracle's mode, for the default and the tiled
+    kernels."""
+    from nmhd_b200.config import FLAG_HALO_PER_STAGE
+    if case == "ot_m2":
+        cfg, s = orszag_tang_3d(16)
+        cfg.margin_y, cfg.size_y = 2, 20
+        s = np.concatenate([s[:, :, -2:], s, s[:, :, :2]], axis=2)
+    else:
+        m = 2 if case == "shear_m2" else 4
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=23, margin=m)
+        if case == "shear_m4_mz2":
+            cfg.margin_z, cfg.size_z = 2, 12
+            s = np.concatenate([s[:, -2:], s, s[:, :2]], axis=1)
+    cfg.flags = FLAG_HALO_PER_STAGE
+    o = oracle.proceed(cfg, s, 10)
+    with MHDSolver(cfg) as sol:
+        sol.set_kernel(variant, 8, 0)
+        sol.set_state(s)
+        sol.step(10)
+        assert sol.current_time() == o["time"]
+        assert_same(sol.get_state(), o["state"])
+
+
 def test_chunked_proceed_equals_single_call(gpu):
     cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=9)
     with MHDSolver(cfg) as a, MHDSolver(cfg) as b:
