@@ -260,6 +260,46 @@ def run_gpu_arm(args):
     cells = cfg.interior_cells
     value = world * cells * args.steps / (ms * 1e-3) / 1e6
 
+    # -- opt-in fast arithmetic (NMHD_FLAG_FAST_ARITHMETIC): same box, timed the
+    # same way; its deviation after one step from the exact step of the same
+    # state, relative to each quantity's scale ------------------------------
+    fast = None
+    if not args.no_fast:
+        from dataclasses import replace as _replace
+        from nmhd_b200.config import FLAG_FAST_ARITHMETIC
+        exact1 = sol.get_state()
+        t_state = sol.current_time()
+        fs = MHDSolver(_replace(cfg, flags=cfg.flags | FLAG_FAST_ARITHMETIC))
+        fs.set_stream(stream.cuda_stream)
+        fs.set_state(exact1)
+        fs.set_time(t_state, 0)
+        ref_sol = MHDSolver(cfg)
+        ref_sol.set_stream(stream.cuda_stream)
+        ref_sol.set_state(exact1)
+        ref_sol.set_time(t_state, 0)
+        ref_sol.step(1)
+        fs.step(1)
+        ys = slice(cfg.margin_y, cfg.size_y - cfg.margin_y)  # interior rows
+        a, b = fs.get_state()[:, :, ys], ref_sol.get_state()[:, :, ys]
+        fdev = max(float(np.abs(a[g_].astype(np.float64) - b[g_]).max() / max(np.abs(b[g_]).max(), 1e-30))
+                   for g_ in ([0], [1, 2, 3], [4], [5, 6, 7]))
+        ref_sol.close()
+        fs.step(args.warmup)
+        torch.cuda.synchronize(dev)
+        barrier()
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(stream)
+        fs.step(args.steps)
+        f1.record(stream)
+        torch.cuda.synchronize(dev)
+        fms = max_over_ranks(f0.elapsed_time(f1))
+        fast = {"value": world * cells * args.steps / (fms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+                "ms_per_step": fms / args.steps, "one_step_max_rel_dev": fdev,
+                "note": "opt-in flag, not bitwise: contracted and approximate face-flux arithmetic; "
+                        "one_step_max_rel_dev = largest |fast - exact| over the interior after one step "
+                        "from the same state, relative to each quantity's scale"}
+        fs.close()
+
     # -- per-kernel times (CUDA events around each launch, same stream) -------
     prof = sol.profile(max(3, min(20, args.steps)))
     kernel_ms_step = sum(t * k for t, k in prof.values())
@@ -326,6 +366,8 @@ def run_gpu_arm(args):
             line["issue_roofline"] = {"bound": "issue", "achieved": ach_i, "peak": peak_i,
                                       "unit": "G warp-instructions/s", "frac": ach_i / peak_i,
                                       "warp_instructions_per_step": winst, "sm_mhz": mhz, "sms": sms}
+        if fast:
+            line["fast_arithmetic"] = fast
         if tuning:
             line["autotune_ms_per_step"] = {f"v{a}_r{b}_z{c}": round(d, 4) for a, b, c, d in tuning}
         if world == 1 and not args.no_cpu:
@@ -653,6 +695,7 @@ def main():
     ap.add_argument("--workload", default="mri_shearing_box_128x256x64",
                     choices=sorted(WORKLOADS) + sorted(ENSEMBLES) + sorted(ADJOINTS) + sorted(SLABS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
     ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint workload: steps per run (default 200)")

@@ -59,7 +59,17 @@ typedef enum nmhd_flag {
    * differ from the reference's scheme by truncation error.  Whole boxes
    * only (nmhd_proceed and the one-slab step); the batched, multi-slab and
    * adjoint paths return NMHD_ERR_NOT_SUPPORTED or reject the config. */
-  NMHD_FLAG_HALO_PER_STAGE = 1
+  NMHD_FLAG_HALO_PER_STAGE = 1,
+  /* Face fluxes with fused multiply-adds, approximate division and square
+   * root, and the HLLD solver's FP64 sub-expressions in float (kernel variant
+   * 2 only; the update kernels stay exact).  Not bitwise: on noisy flows one
+   * step from the same state is within 1e-5 of the reference's, relative to
+   * each quantity's scale; on flows with exact symmetries, where the
+   * reference's corner wind sums are exactly zero and CT takes the mean of
+   * the two fluxes, rounding-size differences pick one of them and B
+   * differs by up to ~1e-3 of its scale after one step.  The batched and
+   * adjoint paths reject it. */
+  NMHD_FLAG_FAST_ARITHMETIC = 2
 } nmhd_flag;
 
 /* Runtime form of the reference's compile-time simulation_config.h

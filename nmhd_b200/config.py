@@ -19,6 +19,7 @@ import numpy as np
 PROBLEMS = {"none": 0, "shearing_box": 1}
 # nmhd_config.flags bits (nmhd_flag in include/nmhd.h)
 FLAG_HALO_PER_STAGE = 1  # refill the RK2 predictor's margins before the second stage
+FLAG_FAST_ARITHMETIC = 2  # contracted, approximate face-flux arithmetic (not bitwise)
 
 
 class NmhdConfig(ctypes.Structure):

@@ -509,7 +509,6 @@ NMHD_HD void hlld_adjoint(const R gamma, const R Bx, const HState<R> &in, const 
   HTape<R> t;
   hlld_tape(gamma, Bx, in, t);
   const int rg = t.region;
-  const bool left = rg <= 2;
   HAdj<R> aL, aR;
   hadj_zero(aL);
   hadj_zero(aR);

@@ -5,6 +5,11 @@
 // are compiled with -fmad=false (no multiply-add contraction), so each float
 // operation rounds exactly once, as in the reference.  IEEE division and square
 // root (-prec-div=true, -prec-sqrt=true, no flush-to-zero) are the defaults.
+//
+// With NMHD_FAST_ARITH (the fast-arithmetic flux kernel, cell_fast.cu, compiled
+// with contraction and approximate division and square root) the FP64
+// sub-expressions are evaluated in float: results within the documented
+// tolerance of the reference instead of bitwise.
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -63,11 +68,16 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
   const float B2_R = B2x + By_R * By_R + Bz_R * Bz_R;
   const float v2_R = velx_R * velx_R + vely_R * vely_R + velz_R * velz_R;
   const float gm1 = gamma - 1.0f;
+#if NMHD_FAST_ARITH
+  const float etot_L = pres_L / gm1 + 0.5f * dens_L * v2_L + 0.5f * B2_L;
+  const float etot_R = pres_R / gm1 + 0.5f * dens_R * v2_R + 0.5f * B2_R;
+#else
   // etot = p/(gamma-1) + 0.5*rho*v2 + 0.5*B2, the last two terms in double
   const float etot_L = (float)((double)(pres_L / gm1) + 0.5 * (double)dens_L * (double)v2_L +
                                0.5 * (double)B2_L);
   const float etot_R = (float)((double)(pres_R / gm1) + 0.5 * (double)dens_R * (double)v2_R +
                                0.5 * (double)B2_R);
+#endif
 
   const float gpl = gamma * pres_L, gpr = gamma * pres_R;
   const float gpbl = gpl + B2_L, gpbr = gpr + B2_R;
@@ -79,6 +89,14 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
   const float S_L = fminf(velx_L, velx_R) - cfmax;
   const float S_R = fmaxf(velx_L, velx_R) + cfmax;
 
+#if NMHD_FAST_ARITH
+  const float pT_L = pres_L + 0.5f * B2_L;
+  const float pT_R = pres_R + 0.5f * B2_R;
+  const float sRv = S_R - velx_R, sLv = S_L - velx_L;
+  const float rden = 1.0f / (sRv * dens_R - sLv * dens_L);
+  const float S_M = (sRv * momx_R - sLv * momx_L - pT_R + pT_L) * rden;
+  const float pT_s = (sRv * dens_R * pT_L - sLv * dens_L * pT_R + dens_L * dens_R * sRv * sLv * (velx_R - velx_L)) * rden;
+#else
   // p + 0.5*B2: exact 0.5*B2 in double, one double add, rounded to float
   const float pT_L = (float)((double)pres_L + 0.5 * (double)B2_L);
   const float pT_R = (float)((double)pres_R + 0.5 * (double)B2_R);
@@ -91,6 +109,7 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
   float pT_s = sRv * dens_R * pT_L - sLv * dens_L * pT_R;
   pT_s = pT_s + dens_L * dens_R * sRv * sLv * (velx_R - velx_L);
   pT_s = (float)((double)pT_s * rden);
+#endif
 
   const float sLm = S_L - S_M, sRm = S_R - S_M;
   const float dens_L_s = dens_L * sLv / sLm;

@@ -119,7 +119,9 @@ nmhd_status validate(const nmhd_config *c, std::string &why) {
   if (c->space_order != 1 && c->space_order != 2) { why = "space_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->time_order != 1 && c->time_order != 2) { why = "time_order must be 1 or 2"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->parallel_size_y < 0) { why = "parallel_size_y must be >= 0"; return NMHD_ERR_INVALID_ARGUMENT; }
-  if (c->flags & ~NMHD_FLAG_HALO_PER_STAGE) { why = "unknown flags"; return NMHD_ERR_INVALID_ARGUMENT; }
+  if (c->flags & ~(NMHD_FLAG_HALO_PER_STAGE | NMHD_FLAG_FAST_ARITHMETIC)) {
+    why = "unknown flags"; return NMHD_ERR_INVALID_ARGUMENT;
+  }
   if ((c->flags & NMHD_FLAG_HALO_PER_STAGE) && c->parallel_size_y > 1) {
     why = "per-stage margin fill is for whole boxes"; return NMHD_ERR_NOT_SUPPORTED;
   }
@@ -151,7 +153,10 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
     nmhd::launch_tile_stage(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
                             half, final_stage, s->shape, st);
   } else if (s->variant == 2) {
-    nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
+    if (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)
+      nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
+    else
+      nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
     nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                              final_stage, st);
   } else if (s->variant == 3) {
@@ -526,6 +531,8 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       if (s->variant == 3) return;
       if (s->variant == 0)
         nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
+      else if (s->variant == 2 && (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC))
+        nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
       else if (s->variant == 2)
         nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
       else
@@ -597,6 +604,8 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk) {
   if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
   if (variant < 0 || variant > 3) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0, 1, 2 or 3");
+  if ((s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC) && variant != 2)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "fast arithmetic exists for kernel variant 2 only");
   if (variant == 0 && tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
     return fail(s, NMHD_ERR_INVALID_ARGUMENT, "tile_rows must be 4, 8 or 16");
   if (z_chunk < 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "z_chunk must be >= 0");
@@ -627,15 +636,18 @@ int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials)
   if (s->cfg.parallel_size_y > 1)
     return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
   const GridParams &g = s->g;
-  const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order, s->cfg.time_order};
+  const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order,
+                       s->cfg.time_order + 8 * s->cfg.flags};
   std::vector<TuneChoice> cands;
   cands.push_back({2, 8, 0});
-  cands.push_back({1, 8, 0});
-  for (int zc : {4, 8, 16})
-    if (zc < g.sz) cands.push_back({3, 8, zc});
-  for (int rows : {4, 8, 16})
-    for (int zc : {0, 8, 16, 32})
-      if (zc == 0 || zc < g.sz) cands.push_back({0, rows, zc});
+  if (!(s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)) {  // the fast flux kernel exists for variant 2 only
+    cands.push_back({1, 8, 0});
+    for (int zc : {4, 8, 16})
+      if (zc < g.sz) cands.push_back({3, 8, zc});
+    for (int rows : {4, 8, 16})
+      for (int zc : {0, 8, 16, 32})
+        if (zc == 0 || zc < g.sz) cands.push_back({0, rows, zc});
+  }
   // save the state and the clock; every trial starts from them
   StepCtl h0;
   nmhd_status st = read_ctl(s, h0);
