@@ -13,8 +13,10 @@
 #ifndef NMHD_HPP
 #define NMHD_HPP
 
+#include <chrono>
 #include <cmath>
 #include <cstdio>
+#include <functional>
 #include <fstream>
 #include <iomanip>
 #include <map>
@@ -206,13 +208,40 @@ class MHDSolver {
   bool read(const std::string &path) { return nmhd_read(s_, path.c_str()) == NMHD_OK; }
   bool write(const std::string &path) { return nmhd_write(s_, path.c_str()) == NMHD_OK; }
 
+  // proceed(goal_time, wallclock_time_limit): true when the goal time was
+  // reached.  Without a monitor the steps run in device-resident batches;
+  // with one, as in the reference's loop (mhd_solver.inlrb:857-860), the
+  // monitor is called before every step and a non-zero return stops the run
+  // before that step (proceed then returns false).
   bool proceed(float goal_time, double wallclock_time_limit = -1, long long max_steps = 0) {
-    int64_t done = 0;
-    nmhd_status st = nmhd_proceed(s_, goal_time, wallclock_time_limit, max_steps, &done);
-    last_steps_ = done;
-    if (st < 0) throw Error(st, nmhd_last_error(s_));
-    return st == NMHD_GOAL_REACHED;
+    if (!monitor_) {
+      int64_t done = 0;
+      nmhd_status st = nmhd_proceed(s_, goal_time, wallclock_time_limit, max_steps, &done);
+      last_steps_ = done;
+      if (st < 0) throw Error(st, nmhd_last_error(s_));
+      return st == NMHD_GOAL_REACHED;
+    }
+    const auto t0 = std::chrono::steady_clock::now();
+    last_steps_ = 0;
+    for (;;) {
+      if (max_steps > 0 && last_steps_ >= max_steps) return false;
+      if (monitor_(*this)) return false;
+      double left = -1;
+      if (wallclock_time_limit > 0) {
+        left = wallclock_time_limit - std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+        if (left <= 0) return false;
+      }
+      int64_t done = 0;
+      nmhd_status st = nmhd_proceed(s_, goal_time, left, 1, &done);
+      last_steps_ += done;
+      if (st < 0) throw Error(st, nmhd_last_error(s_));
+      if (st == NMHD_GOAL_REACHED) return true;
+      if (st == NMHD_TIMEOUT) return false;
+    }
   }
+  // The application's monitor() (e.g. src/application/kepler_disk_demo/
+  // mhd_solver.curb:107-130); an empty function removes it.
+  void set_monitor(std::function<int(MHDSolver &)> m) { monitor_ = std::move(m); }
 
   double current_time() const { return nmhd_current_time(s_); }
   int generation() const { return (int)nmhd_generation(s_); }
@@ -254,6 +283,7 @@ class MHDSolver {
   nmhd_config cfg_;
   nmhd_solver *s_ = nullptr;
   long long last_steps_ = 0;
+  std::function<int(MHDSolver &)> monitor_;
 };
 
 }  // namespace nmhd

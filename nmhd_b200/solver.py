@@ -122,10 +122,63 @@ class MHDSolver:
         return code == 0
 
     # -- time stepping ---------------------------------------------------
+    def monitor(self) -> int:
+        """MHDSolver::monitor(): the application's per-step hook.  A subclass
+        that overrides it makes proceed() call it before every step, as the
+        reference's loop does (mhd_solver.inlrb:857-860); a non-zero return
+        stops the run before that step."""
+        return 0
+
+    def dump(self, tag) -> bool:
+        """MHDSolver::dump(tag): the state dump ``tag.bin`` (the reference's
+        applications define their own)."""
+        return self.write(str(tag) + ".bin")
+
+    def initial_event(self) -> int:
+        """Application hook called by the host program before the run."""
+        return 0
+
+    def final_event(self) -> int:
+        """Application hook called by the host program after the run."""
+        return 0
+
+    def _proceed_monitored(self, goal_time, wallclock_time_limit, max_steps):
+        import time as _t
+        t0 = _t.monotonic()
+        steps = 0
+        while True:
+            if max_steps > 0 and steps >= max_steps:
+                self.last_steps = steps
+                return False
+            if self.monitor():
+                self.last_steps = steps
+                return False
+            left = -1.0
+            if wallclock_time_limit > 0:
+                left = wallclock_time_limit - (_t.monotonic() - t0)
+                if left <= 0:
+                    self.last_steps = steps
+                    return False
+            done = ctypes.c_int64(0)
+            code = self._L.nmhd_proceed(self._h, float(goal_time), float(left), 1, ctypes.byref(done))
+            self.last_status = code
+            steps += done.value
+            _check(self._L, self._h, code)
+            if code == _lib.GOAL_REACHED:
+                self.last_steps = steps
+                return True
+            if code == _lib.TIMEOUT:
+                self.last_steps = steps
+                return False
+
     def proceed(self, goal_time, wallclock_time_limit=-1.0, max_steps=0) -> bool:
         """MHDSolver::proceed: integrate until ``goal_time`` (True) or until the
         wallclock limit in seconds passes (False); ``max_steps`` > 0 also stops
-        after that many steps (False).  Raises on numerical or CUDA errors."""
+        after that many steps (False).  Raises on numerical or CUDA errors.
+        Steps run in device-resident batches unless a subclass overrides
+        monitor()."""
+        if type(self).monitor is not MHDSolver.monitor:
+            return self._proceed_monitored(goal_time, wallclock_time_limit, max_steps)
         done = ctypes.c_int64(0)
         code = self._L.nmhd_proceed(self._h, float(goal_time), float(wallclock_time_limit),
                                     int(max_steps), ctypes.byref(done))

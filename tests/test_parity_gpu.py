@@ -324,3 +324,35 @@ def test_chunked_pipeline_variant_bitwise(gpu, zc, case):
         sol.step(10)
         assert sol.current_time() == o["time"]
         assert_same(sol.get_state(), o["state"])
+
+
+def test_monitor_hook_runs_before_every_step(gpu):
+    """A monitor() override is called before every step, as in the
+    reference's loop; a non-zero return stops the run before that step; the
+    steps taken are bitwise the batched ones."""
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=31)
+
+    class Counting(MHDSolver):
+        def __init__(self, cfg, stop_at):
+            super().__init__(cfg)
+            self.calls, self.gens, self.stop_at = 0, [], stop_at
+
+        def monitor(self):
+            self.calls += 1
+            self.gens.append(self.generation())
+            return self.generation() >= self.stop_at
+
+    with Counting(cfg, 7) as sol:
+        sol.set_state(s)
+        assert sol.proceed(1e30) is False
+        assert sol.gens == list(range(8)) and sol.generation() == 7
+        got = sol.get_state()
+    with MHDSolver(cfg) as ref:
+        ref.set_state(s)
+        ref.step(7)
+        assert np.array_equal(got, ref.get_state())
+    # reaching the goal ends the loop without another monitor call
+    with Counting(cfg, 10 ** 6) as sol:
+        sol.set_state(s)
+        assert sol.proceed(0.05) is True
+        assert sol.calls == sol.generation()
