@@ -39,7 +39,21 @@ WORKLOADS = {
                                         l_azimuthal=4.0, l_vertical=1.0, seed=1),
     "mri_shearing_box_512x1024x256": dict(n_radial=512, n_azimuthal=1024, n_vertical=256,
                                           l_radial=1.0, l_azimuthal=4.0, l_vertical=1.0, seed=3),
+    # the 256^3 performance anchors: a cubic shearing box and the Orszag-Tang vortex
+    "mri_shearing_box_256": dict(n_radial=256, n_azimuthal=256, n_vertical=256, l_radial=1.0,
+                                 l_azimuthal=1.0, l_vertical=1.0, seed=5),
+    "orszag_tang_256": dict(problem="orszag_tang", n=256),
 }
+
+
+def make_workload(name):
+    """(config, state) of a named single-box workload."""
+    kw = dict(WORKLOADS[name])
+    if kw.pop("problem", "shearing_box") == "orszag_tang":
+        from nmhd_b200.problems import orszag_tang_3d
+        return orszag_tang_3d(**kw)
+    from nmhd_b200.problems import shearing_box
+    return shearing_box(**kw)
 REF_BINARY = {"mri_shearing_box_128x256x64": "shear256x128x64"}
 ENSEMBLES = {"mri_ensemble_64": dict(n_boxes=64, seed=0),
              # many small boxes (sides 8..16 radial/vertical, 2-4x azimuthal):
@@ -123,9 +137,8 @@ class ClockSampler:
 def cpu_reference_run(workload, steps, threads=None):
     """Run the host-compiled reference solver (oracle/_ref) on the workload;
     returns (interior cell-updates/s, steps, seconds, threads, kind)."""
-    from nmhd_b200.problems import shearing_box
     from oracle import oracle
-    cfg, state = shearing_box(**WORKLOADS[workload])
+    cfg, state = make_workload(workload)
     name = REF_BINARY.get(workload)
     threads = threads or os.cpu_count()
     if name and oracle.ref_binary(name):
@@ -211,13 +224,12 @@ def run_reference_arm(args):
 
 def run_gpu_arm(args):
     import torch
-    from nmhd_b200.problems import shearing_box
     from nmhd_b200.solver import MHDSolver
 
     rank, world, local, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
     wl = args.workload
-    cfg, state = shearing_box(**WORKLOADS[wl])
+    cfg, state = make_workload(wl)
     stream = torch.cuda.Stream(device=dev)
     sol = MHDSolver(cfg)
     sol.set_stream(stream.cuda_stream)
