@@ -158,7 +158,15 @@ struct OpABface {
   GGrid<R> g;
   const R *wb, *wo, *lout, *lamU, *lamE;
   R *lamBn, *lb;
-  NMHD_HD void operator()(int x, int y, int z) const { a_bface_cell(g, wb, wo, lout, lamU, lamE, lamBn, lb, x, y, z); }
+  R *lamBc;  // cleared here for the reconstruction passes that follow
+  NMHD_HD void operator()(int x, int y, int z) const {
+    a_bface_cell(g, wb, wo, lout, lamU, lamE, lamBn, lb, x, y, z);
+    const size_t N = (size_t)g.n;
+    const int o = cell_at(g, x, y, z);
+    lamBc[o] = R(0);
+    lamBc[N + o] = R(0);
+    lamBc[2 * N + o] = R(0);
+  }
 };
 template <class R, int AX>
 struct OpAFlux {
@@ -240,8 +248,7 @@ template <class Ex, class R>
 void adj_stage(Ex &ex, const GGrid<R> &g, const R *win, const R *wb, const R *wo, const R *flux, R h,
                const R *lout, R *lin, R *lb, const AdjScratch<R> &sc) {
   ex.cells(g, OpAPrim<R>{g, wb, flux, lout, sc.lamU, sc.lamE, lb, h});
-  ex.cells(g, OpABface<R>{g, wb, wo, lout, sc.lamU, sc.lamE, sc.lamBn, lb});
-  ex.zero(sc.lamBc, (size_t)3 * g.n);
+  ex.cells(g, OpABface<R>{g, wb, wo, lout, sc.lamU, sc.lamE, sc.lamBn, lb, sc.lamBc});
   // one face axis at a time through the shared face scratch
   ex.cells(g, OpAFlux<R, 0>{g, win, sc.lamBn, sc.lamU, sc.face, h});
   ex.cells(g, OpARecon<R, 0>{g, sc.face, lin, sc.lamBc, h});

@@ -165,6 +165,7 @@ struct Workspace {
   void *mem = nullptr;
   size_t bytes = 0;
   long long tape_budget = -1;  // bytes for the tapes of segments beyond the last; -1: automatic
+  int parity = 0;              // StepCtl::parity as the production steps leave it (host copy)
   int kept_segments = 0;       // of the last run
   StepCtl *ctl = nullptr;
   float *dt_dev = nullptr, *hist_dummy = nullptr;
@@ -262,31 +263,36 @@ nmhd_status write_ctl(nmhd_solver *s, Workspace &w, double time, long long gen, 
   h.hist_cap = nmhd::kDtHistCap;
   h.dt_seq = frozen ? w.dt_dev : nullptr;
   h.dt_seq_base = 0;
+  w.parity = 0;
   AD_CUDA(cudaMemcpyAsync(w.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, s->stream));
   AD_CUDA(cudaStreamSynchronize(s->stream));
   return NMHD_OK;
 }
 
 // One FP32 step with the production kernels on explicit buffers: t.wf holds
-// W^n (its margins are filled in place), the raw W^{n+1} goes to t.wo.
+// W^n (its margins are filled in place), the raw W^{n+1} goes to t.wo.  The
+// kernels take the current state as buffer `parity` of (w0, w1) and the final
+// stage flips the device parity; the pair is passed in the order that makes
+// t.wf the current buffer, so the parity needs no reset between steps.
 void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl) {
   const GridParams &g = s->g;
   cudaStream_t st = s->stream;
   float *hist = cfl ? w.dt_dev : w.hist_dummy;
-  cudaMemsetAsync(&w.ctl->parity, 0, sizeof(int), st);  // buffer 0 = t.wf, 1 = t.wo, 2 = t.ws
+  float *b0 = w.parity ? t.wo : t.wf, *b1 = w.parity ? t.wf : t.wo;  // buffer 2 = t.ws
   if (g.my > 0 || g.mz > 0) {
-    nmhd::launch_fill(g, w.ctl, t.wf, t.wo, st);
-    if (cfl) nmhd::launch_cfl_margin(g, w.ctl, t.wf, t.wo, st);
+    nmhd::launch_fill(g, w.ctl, b0, b1, st);
+    if (cfl) nmhd::launch_cfl_margin(g, w.ctl, b0, b1, st);
   }
   if (s->cfg.time_order == 1) {
-    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f1, 0, 0, st);
-    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f1, hist, 0, 1, 0, 1, st);
+    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, st);
+    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, st);
   } else {
-    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f1, 0, 1, st);
-    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f1, hist, 0, 2, 1, 0, st);
-    nmhd::launch_cell_flux(g, w.ctl, t.wf, t.wo, t.ws, t.f2, 2, 0, st);
-    nmhd::launch_cell_update(g, w.ctl, t.wf, t.wo, t.ws, t.f2, hist, 2, 1, 0, 1, st);
+    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, st);
+    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, st);
+    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, st);
+    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, st);
   }
+  w.parity ^= 1;
 }
 
 float elapsed(cudaEvent_t a, cudaEvent_t b) {
