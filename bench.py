@@ -10,10 +10,20 @@ src/application/optimize_mhd/main_detail.curb:39-44, counted over interior
 cells).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl nmhd|reference]
+                  [--workload NAME]
 
 N > 1 runs under torch.distributed (one rank per GPU): independent replicas of
 the box, one per GPU (the time step has no data-parallel exchange on one box;
-"scaling": "weak").  Rank 0 prints one JSON line.
+"scaling": "weak").  Rank 0 prints one JSON line: the device-timed rate
+(value), the same through the C ABI with host buffers (e2e), the HBM roofline
+of the step and, for the default box, its instruction-issue roofline, the
+opt-in fast-arithmetic step beside the exact one, the reference's CPU path on
+a bounded sample (cpu_baseline), and the SM clocks seen while timing.
+
+Other workloads (--workload): the 512 x 1024 x 256 box, the 256^3 anchors
+(mri_shearing_box_256, orszag_tang_256), the batched ensembles
+(mri_ensemble_64, mri_ensemble_small_512), the adjoint (mri_adjoint_64) and
+one box split into radial slabs over N GPUs (mri_slabs_*, strong scaling).
 """
 from __future__ import annotations
 
