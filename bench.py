@@ -584,6 +584,7 @@ def run_adjoint_arm(args):
     sol = MHDSolver(cfg)
     sol.set_stream(stream.cuda_stream)
     sol.set_state(s)
+    sol.set_adjoint_tape_budget(args.tape_budget)
     for _ in range(args.warmup):
         sol.adjoint(steps, window=window, ckpt_every=K)
     # forward: the production path (nmhd_proceed, CUDA graphs) over the same steps
@@ -618,7 +619,8 @@ def run_adjoint_arm(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing box)",
         "config": {"workload": args.workload, "cells_interior": cfg.interior_cells,
                    "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
-                   "ckpt_every": K, "segments_kept_on_tape": sol.adjoint_kept_segments(),
+                   "ckpt_every": K, "tape_budget_bytes": args.tape_budget,
+                   "segments_kept_on_tape": sol.adjoint_kept_segments(),
                    "segments": -(-steps // K),
                    "parallelism": "replicas" if world > 1 else "single"},
         "forward_ms": fwd_ms, "adjoint_total_ms": tot, "adjoint_reverse_ms": rev,
@@ -721,6 +723,8 @@ def main():
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
     ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint workload: steps per run (default 200)")
+    ap.add_argument("--tape-budget", type=int, default=-1,
+                    help="adjoint workload: bytes of tape beyond the last segment (-1: half the free HBM)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     if args.impl == "reference":

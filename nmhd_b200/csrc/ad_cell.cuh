@@ -357,28 +357,28 @@ NMHD_HD typename Wide64<T>::type g_stress_cell(const GGrid<R> &g, const T *w, in
 //   lamBc 3 fields: adjoint of the cell-centred transverse B averages.
 
 template <class R>
-NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *flux, const R *lout, R *lamU, R *lamE, R *lb,
+NMHD_HD void a_prim_cell(const GGrid<R> &g, const R *wb, const R *wo, const R *lout, R *lamU, R *lamE, R *lb,
                          int x, int y, int z, R h) {
   const size_t N = (size_t)g.n;
   const int o = cell_at(g, x, y, z);
-  const int oxp = cell_at(g, x + 1, y, z), oyp = cell_at(g, x, y + 1, z), ozp = cell_at(g, x, y, z + 1);
-  const R *Fx = flux, *Fy = flux + 7 * N, *Fz = flux + 14 * N;
-  // the linearisation point: the updated conserved state (inverse spacings:
-  // the adjoint needs no correctly rounded quotients)
-  R pace[4];
-  for (int v = 0; v < 4; ++v) {
-    R pc = R(0);
-    pc = pc + (Fx[v * N + o] - Fx[v * N + oxp]) * g.idx;
-    pc = pc + (Fy[v * N + o] - Fy[v * N + oyp]) * g.idy;
-    pc = pc + (Fz[v * N + o] - Fz[v * N + ozp]) * g.idz;
-    pace[v] = pc;
-  }
+  // the linearisation point, the updated conserved state, from the stage's
+  // output: its density is the updated density, its velocity m/rho after the
+  // Kepler kick, which is undone here (vx' = vx - c vy, vy' = vy + c vx + h T,
+  // c = 2 omega h)
   const R gm1 = g.gamma - R(1.0f);
   const R rho0 = wb[o], vx0 = wb[N + o], vy0 = wb[2 * N + o], vz0 = wb[3 * N + o];
-  const R rho = rho0 + h * pace[0];
-  const R mx = rho0 * vx0 + h * pace[1];
-  const R my = rho0 * vy0 + h * pace[2];
-  const R mz = rho0 * vz0 + h * pace[3];
+  const R rho = wo[o];
+  R vx = wo[N + o], vy = wo[2 * N + o];
+  const R vz = wo[3 * N + o];
+  if (g.shear) {
+    const R c = R(2.0f) * g.omega * h;
+    const R tidal = h * (R(2.0f) * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((R)y + R(0.5f))));
+    const R vyk = vy - tidal, id = R(1) / (R(1) + c * c);
+    const R vxp = (vx + c * vyk) * id;
+    vy = (vyk - c * vx) * id;
+    vx = vxp;
+  }
+  const R mx = rho * vx, my = rho * vy, mz = rho * vz;
   R l_vx = lout[N + o], l_vy = lout[2 * N + o];
   const R l_vz = lout[3 * N + o];
   if (g.shear) {

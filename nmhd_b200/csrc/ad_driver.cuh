@@ -17,9 +17,11 @@
 namespace nmhd {
 namespace ad {
 
-// Number of fields of one step's tape: filled input (8), stage-1 fluxes (21),
-// predictor (8), stage-2 fluxes (21), raw output (8).
-constexpr int kTapeFields = 66;
+// Number of fields of one step's tape: filled input (8), predictor (8), raw
+// output (8).  The stages' face fluxes go to one shared scratch of 21 fields:
+// the adjoint recomputes what it needs of them.
+constexpr int kTapeFields = 24;
+constexpr int kFluxScratchFields = 21;
 // Scratch fields of the adjoint of a stage: lamU 5, lamE 1, lamBn 3, face 30, lamBc 3.
 constexpr int kAdjScratchFields = 42;
 
@@ -29,13 +31,12 @@ struct StepTape {
 };
 
 template <class T>
-StepTape<T> tape_at(T *base, size_t n) {
+StepTape<T> tape_at(T *base, size_t n, T *flux_scratch) {
   StepTape<T> t;
   t.wf = base;
-  t.f1 = base + 8 * n;
-  t.ws = base + 29 * n;
-  t.f2 = base + 37 * n;
-  t.wo = base + 58 * n;
+  t.ws = base + 8 * n;
+  t.wo = base + 16 * n;
+  t.f1 = t.f2 = flux_scratch;
   return t;
 }
 
@@ -148,10 +149,10 @@ struct OpStress {
 template <class R>
 struct OpAPrim {
   GGrid<R> g;
-  const R *wb, *flux, *lout;
+  const R *wb, *wo, *lout;
   R *lamU, *lamE, *lb;
   R h;
-  NMHD_HD void operator()(int x, int y, int z) const { a_prim_cell(g, wb, flux, lout, lamU, lamE, lb, x, y, z, h); }
+  NMHD_HD void operator()(int x, int y, int z) const { a_prim_cell(g, wb, wo, lout, lamU, lamE, lb, x, y, z, h); }
 };
 template <class R>
 struct OpABface {
@@ -245,9 +246,9 @@ void fwd_step(Ex &ex, const GGrid<R> &g, int time_order, double time, R dt, cons
 // ---------------------------------------------------------------------------
 // Adjoint
 template <class Ex, class R>
-void adj_stage(Ex &ex, const GGrid<R> &g, const R *win, const R *wb, const R *wo, const R *flux, R h,
-               const R *lout, R *lin, R *lb, const AdjScratch<R> &sc) {
-  ex.cells(g, OpAPrim<R>{g, wb, flux, lout, sc.lamU, sc.lamE, lb, h});
+void adj_stage(Ex &ex, const GGrid<R> &g, const R *win, const R *wb, const R *wo, R h, const R *lout, R *lin,
+               R *lb, const AdjScratch<R> &sc) {
+  ex.cells(g, OpAPrim<R>{g, wb, wo, lout, sc.lamU, sc.lamE, lb, h});
   ex.cells(g, OpABface<R>{g, wb, wo, lout, sc.lamU, sc.lamE, sc.lamBn, lb, sc.lamBc});
   // one face axis at a time through the shared face scratch
   ex.cells(g, OpAFlux<R, 0>{g, win, sc.lamBn, sc.lamU, sc.face, h});
@@ -268,11 +269,11 @@ void adj_step(Ex &ex, const GGrid<R> &g, int time_order, double time, R dt, cons
   const size_t n8 = (size_t)8 * g.n;
   ex.zero(lam_f, n8);
   if (time_order == 1) {
-    adj_stage(ex, g, t.wf, t.wf, t.wo, t.f1, dt, lam_next, lam_f, lam_f, sc);
+    adj_stage(ex, g, t.wf, t.wf, t.wo, dt, lam_next, lam_f, lam_f, sc);
   } else {
     ex.zero(lam_s, n8);
-    adj_stage(ex, g, t.ws, t.wf, t.wo, t.f2, dt, lam_next, lam_s, lam_f, sc);
-    adj_stage(ex, g, t.wf, t.wf, t.ws, t.f1, dt / R(2), lam_s, lam_f, lam_f, sc);
+    adj_stage(ex, g, t.ws, t.wf, t.wo, dt, lam_next, lam_s, lam_f, sc);
+    adj_stage(ex, g, t.wf, t.wf, t.ws, dt / R(2), lam_s, lam_f, lam_f, sc);
   }
   // margin fill: W_f = Fz(Fy(W^n)), so apply Fz^T then Fy^T
   if (g.mz > 0) ex.items(g.sx * g.sy * g.mz, OpAFillZ<R>{g, lam_f});

@@ -8,9 +8,9 @@
 // kernels of ad_driver.cuh over double and Dual<double>.  The adjoint kernels
 // are the transposes in ad_cell.cuh / ad_hlld.cuh, one launch per pass.
 //
-// Memory: checkpoints (8 fields) every K steps, plus the tape (66 fields per
-// step: filled input, predictor, raw output, both stages' fluxes) of the last
-// segments, plus 3 adjoint states and 42 scratch fields.  The forward run
+// Memory: checkpoints (8 fields) every K steps, plus the tape (24 fields per
+// step: filled input, predictor, raw output) of the last segments, one shared
+// 21-field flux scratch, plus 3 adjoint states and 42 scratch fields.  The forward run
 // keeps as many trailing segments on the tape as the tape budget allows (at
 // least one; by default as many as fit in half of the free device memory),
 // and the reverse sweep recomputes only the earlier segments, from their
@@ -331,11 +331,12 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   // arena: checkpoints, one segment's tape, the primal pass's ping-pong
   // partner, 3 adjoint states, adjoint scratch, reduction partials
   const size_t nb = (n + 255) / 256;
-  R *ckpt = nullptr, *tape = nullptr, *spare = nullptr, *lam = nullptr, *scr = nullptr;
+  R *ckpt = nullptr, *tape = nullptr, *fscr = nullptr, *spare = nullptr, *lam = nullptr, *scr = nullptr;
   double *partial = nullptr, *acc = nullptr;
   auto carve = [&](Arena &ar) {
     ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
     tape = ar.take<R>((size_t)kseg * tape_steps * kTapeFields * n);
+    fscr = ar.take<R>((size_t)kFluxScratchFields * n);
     spare = ar.take<R>(8 * n);
     lam = want_grad ? ar.take<R>(24 * n) : nullptr;
     scr = want_grad ? ar.take<R>((size_t)kAdjScratchFields * n) : nullptr;
@@ -377,7 +378,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
 
   // ---- forward run with checkpoints -------------------------------------------
   AD_CUDA(cudaEventRecord(w.ev[0], q));
-  StepTape<R> t0tape = tape_at(tape, n);
+  StepTape<R> t0tape = tape_at(tape, n, fscr);
   R *A = t0tape.wf, *B = spare;
   if constexpr (Prec<R>::kProduction) {
     AD_CUDA(cudaMemcpyAsync(A, cur, sizeof(float) * 8 * n, cudaMemcpyDeviceToDevice, q));
@@ -405,7 +406,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
       AD_CUDA(cudaMemcpyAsync(ckpt + (size_t)(i / K) * 8 * n, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     StepTape<R> t = {A, t0tape.f1, t0tape.ws, t0tape.f2, B};
     if (i >= kept0) {
-      t = tape_at(tape + (size_t)(i - kept0) * kTapeFields * n, n);
+      t = tape_at(tape + (size_t)(i - kept0) * kTapeFields * n, n, fscr);
       if (t.wf != A) AD_CUDA(cudaMemcpyAsync(t.wf, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     }
     if constexpr (Prec<R>::kProduction) {
@@ -463,19 +464,19 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
     if (!kept)
       AD_CUDA(cudaMemcpyAsync(segtape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     for (int i = n0; i < (kept ? n0 : n1); ++i) {
-      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n);
+      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr);
       if constexpr (Prec<R>::kProduction)
         prod_step(s, w, t, false);
       else
         fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
       if (i + 1 < n1) {
-        const StepTape<R> tn1 = tape_at(segtape + (size_t)(i + 1 - n0) * kTapeFields * n, n);
+        const StepTape<R> tn1 = tape_at(segtape + (size_t)(i + 1 - n0) * kTapeFields * n, n, fscr);
         AD_CUDA(cudaMemcpyAsync(tn1.wf, t.wo, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
       }
     }
     AD_CUDA(cudaEventRecord(w.ev[3], q));
     for (int i = n1 - 1; i >= n0; --i) {
-      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n);
+      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr);
       if (in_window(L, i + 1)) ex.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
       adj_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
       std::swap(lamA, lamF);
@@ -553,10 +554,11 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
   Workspace &w = workspace(s);
   const size_t n = (size_t)s->g.n;
   const size_t nb = (n + 255) / 256;
-  D *tape = nullptr, *spare = nullptr, *partial = nullptr, *acc = nullptr;
+  D *tape = nullptr, *fscr = nullptr, *spare = nullptr, *partial = nullptr, *acc = nullptr;
   double *dir_dev = nullptr;
   auto carve = [&](Arena &ar) {
     tape = ar.take<D>((size_t)kTapeFields * n);
+    fscr = ar.take<D>((size_t)kFluxScratchFields * n);
     spare = ar.take<D>(8 * n);
     dir_dev = ar.take<double>(8 * n);
     partial = ar.take<D>(nb);
@@ -581,7 +583,7 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
       if (!dir[v]) return set_err(s, NMHD_ERR_INVALID_ARGUMENT, "dir field pointer is NULL");
       AD_CUDA(cudaMemcpyAsync(dir_dev + (size_t)v * n, dir[v], sizeof(double) * n, cudaMemcpyHostToDevice, q));
     }
-  StepTape<D> t = tape_at(tape, n);
+  StepTape<D> t = tape_at(tape, n, fscr);
   D *A = t.wf, *B = spare;
   ex.items((int)(8 * n), OpWiden<D>{cur, dir ? dir_dev : nullptr, shift, A});
   AD_CUDA(cudaMemsetAsync(acc, 0, sizeof(D), q));

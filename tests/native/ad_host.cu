@@ -69,8 +69,8 @@ void forward(const nmhd_config &c, T *state, double time, const T *dts, int nste
   HostExec ex;
   const GGrid<T> g = make_ggrid<T>(c);
   const size_t n = (size_t)g.n;
-  std::vector<T> tape((size_t)kTapeFields * n);
-  StepTape<T> t = tape_at(tape.data(), n);
+  std::vector<T> tape((size_t)kTapeFields * n), fscr((size_t)kFluxScratchFields * n);
+  StepTape<T> t = tape_at(tape.data(), n, fscr.data());
   std::memcpy(t.wf, state, sizeof(T) * 8 * n);
   for (int i = 0; i < nsteps; ++i) {
     fwd_step(ex, g, c.time_order, time, dts[i], t);
@@ -135,8 +135,8 @@ void adh_tlm(const nmhd_config *c, const double *state, const double *dir, doubl
   HostExec ex;
   const GGrid<double> g = make_ggrid<double>(*c);
   const size_t n = (size_t)g.n;
-  std::vector<D> tape((size_t)kTapeFields * n);
-  StepTape<D> t = tape_at(tape.data(), n);
+  std::vector<D> tape((size_t)kTapeFields * n), fscr((size_t)kFluxScratchFields * n);
+  StepTape<D> t = tape_at(tape.data(), n, fscr.data());
   for (size_t i = 0; i < 8 * n; ++i) t.wf[i] = D(state[i], dir ? dir[i] : 0.0);
   D acc(0.0);
   if (in_window(*l, 0)) acc = acc + stress(g, t.wf);
@@ -160,14 +160,14 @@ static void adjoint(const nmhd_config &c, const R *state, double time, const R *
   HostExec ex;
   const GGrid<R> g = make_ggrid<R>(c);
   const size_t n = (size_t)g.n;
-  std::vector<R> tapes((size_t)nsteps * kTapeFields * n);
+  std::vector<R> tapes((size_t)nsteps * kTapeFields * n), fscr((size_t)kFluxScratchFields * n);
   std::vector<double> tn(nsteps + 1);
   tn[0] = time;
   double acc = 0.0;
   std::memcpy(tapes.data(), state, sizeof(R) * 8 * n);
   if (in_window(l, 0)) acc += stress(g, state);
   for (int i = 0; i < nsteps; ++i) {
-    StepTape<R> t = tape_at(tapes.data() + (size_t)i * kTapeFields * n, n);
+    StepTape<R> t = tape_at(tapes.data() + (size_t)i * kTapeFields * n, n, fscr.data());
     fwd_step(ex, g, c.time_order, tn[i], dts[i], t);
     tn[i + 1] = tn[i] + (double)dts[i];
     if (in_window(l, i + 1)) acc += stress(g, t.wo);
@@ -180,7 +180,7 @@ static void adjoint(const nmhd_config &c, const R *state, double time, const R *
   const AdjScratch<R> sc = scratch_at(scr.data(), n);
   ex.zero(lamA, 8 * n);
   for (int i = nsteps - 1; i >= 0; --i) {
-    StepTape<R> t = tape_at(tapes.data() + (size_t)i * kTapeFields * n, n);
+    StepTape<R> t = tape_at(tapes.data() + (size_t)i * kTapeFields * n, n, fscr.data());
     if (in_window(l, i + 1)) ex.cells(g, OpAStress<R>{g, t.wo, lamA, s});
     adj_step(ex, g, c.time_order, tn[i], dts[i], t, lamA, lamS, lamF, sc);
     R *tmp = lamA;

@@ -88,7 +88,7 @@ def test_checkpoint_interval_and_tape_budget_do_not_change_the_gradient(gpu, ckp
     gradient bitwise unchanged."""
     cfg, s = _case("shear")
     nseg = -(-6 // ckpt)
-    seg_bytes = min(ckpt, 6) * 66 * cfg.cells * 4
+    seg_bytes = min(ckpt, 6) * 24 * cfg.cells * 4  # 24 tape fields per step
     with MHDSolver(cfg) as sol:
         sol.set_state(s)
         sol.set_adjoint_tape_budget(0)
