@@ -220,9 +220,12 @@ const char *nmhd_noalloc_last_error(void);
  * and seed) advanced together.  No counterpart in the reference, which runs
  * one compile-time box per process.  Every box has its own configuration,
  * state, clock and CFL time step (reduced per box), and is advanced bitwise as
- * nmhd_proceed would advance it alone.  Each kernel of a step is one
- * persistent launch over all boxes; batches of steps are one CUDA graph.
- * Batched boxes use time_order 2 and no Z margins. */
+ * nmhd_proceed would advance it alone.  Each kernel of a step is one launch
+ * over all boxes (per group of 128 boxes, whose descriptors travel in the
+ * launch's parameter block), either persistent (a resident grid walking tile
+ * ranges) or one 32x4x2-cell tile per CTA, as nmhd_batch_autotune picks;
+ * batches of steps are one CUDA graph.  Batched boxes use time_order 2 and no
+ * Z margins. */
 typedef struct nmhd_batch nmhd_batch;
 nmhd_status nmhd_batch_create(const nmhd_config *boxes, int n, nmhd_batch **out);
 void nmhd_batch_destroy(nmhd_batch *b);
@@ -236,6 +239,18 @@ nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *gene
  * (semantics of nmhd_proceed, per box; a box that reached the goal waits).
  * *steps_done: steps taken by the box that took most. */
 nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
+/* Schedule of stage kernel `kernel` (0 face fluxes, 1 constrained transport,
+ * 2 conserved update): persistent = 1 for the resident grid walking tile
+ * ranges, 0 for one tile per CTA (the default). */
+nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent);
+/* Schedule autotuner of the batch (the batched counterpart of nmhd_autotune).
+ * Times `reps` launches of each stage kernel (face fluxes, constrained
+ * transport, conserved update) in both schedules on the boxes' current states
+ * with CUDA events, keeps the faster per kernel, and leaves states and clocks
+ * unchanged.  trials_out (may be NULL) receives up to max_trials rows of
+ * (kernel, persistent, ms per launch).  Returns the number of rows written or a
+ * negative nmhd_status.  Both schedules give bitwise the same result. */
+int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_trials);
 const char *nmhd_batch_last_error(const nmhd_batch *b);
 
 /* ---- Differentiation ---------------------------------------------------------

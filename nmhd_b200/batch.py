@@ -86,6 +86,19 @@ class BatchSolver:
         self.proceed(math.inf, nsteps)
         return self.last_steps
 
+    def set_schedule(self, kernel, persistent):
+        """Schedule of stage kernel ``kernel`` (0 fluxes, 1 constrained
+        transport, 2 conserved update): persistent or one tile per CTA."""
+        self._check(self._L.nmhd_batch_set_schedule(self._h, int(kernel), int(bool(persistent))))
+
+    def autotune(self, reps=5):
+        """Pick each stage kernel's schedule (persistent or one tile per CTA)
+        by timing both on the current states; states and clocks are left
+        unchanged.  Returns rows (kernel, persistent, ms per launch)."""
+        out = np.zeros((6, 3), dtype=np.float64)
+        k = self._check(self._L.nmhd_batch_autotune(self._h, int(reps), out.ctypes.data, 6))
+        return [(int(a), bool(b), float(c)) for a, b, c in out[:k]]
+
     @property
     def cells(self):
         return sum(c.cells for c in self.configs)

@@ -52,66 +52,123 @@ __device__ __forceinline__ int find_box(int nb, long long i, F begin) {
   return lo;
 }
 
-// One stage kernel over all boxes.  KIND 0: face fluxes, 1: constrained
-// transport, 2: conserved update + primitive recovery (+ CFL and clock in the
-// final stage).  Resident CTAs per SM asked of the compiler: the flux kind
-// NMHD_BATCH_FLUX_MIN_BLOCKS, the CT kind 3 (4 would spill), the conserved
-// update 4.
-#ifndef NMHD_BATCH_FLUX_MIN_BLOCKS
-#define NMHD_BATCH_FLUX_MIN_BLOCKS 3
+}  // namespace
+
+// Boxes of one launch group.  The descriptors travel by value in the kernel's
+// parameter block (read through the constant bank with a CTA-uniform index), so
+// the per-cell code sees its box constants the way the single-box kernels see
+// their GridParams argument, without holding them in registers; descriptors
+// staged through shared memory cost 16 registers per thread and one resident
+// CTA per SM.  Batches of more boxes are split into groups, one launch per
+// group and kernel.
+constexpr int kGroupBoxes = 128;
+struct BatchGroup {
+  int nb;                           // boxes in this group
+  int total_tiles;                  // tiles of this group
+  int tile_begin[kGroupBoxes + 1];  // group-local first tile of each box; [nb] = total_tiles
+  BoxDesc box[kGroupBoxes];
+};
+static_assert(sizeof(BatchGroup) <= 32764, "kernel parameter block limit");
+
+namespace {
+
+// Box of group-local tile t (uniform per CTA).
+__device__ __forceinline__ int group_box(const BatchGroup &p, int t) {
+  int lo = 0, hi = p.nb - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (p.tile_begin[mid] <= t) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+#ifndef NMHD_BATCH_CT_INNER
+#define NMHD_BATCH_CT_INNER 1
 #endif
+
+// One tile (32 x 4 x 2 cells) of one stage kernel.  KIND 0: face fluxes, 1:
+// constrained transport, 2: conserved update + primitive recovery (+ CFL and
+// clock in the final stage).
 template <int KIND>
-__global__ void __launch_bounds__(kThreads, KIND == 0 ? NMHD_BATCH_FLUX_MIN_BLOCKS : (KIND == 1 ? 3 : 4))
-    k_batch_stage(const BoxDesc *__restrict__ boxes, int nb, int total_tiles, int in_sel, int out_sel, int half,
-                  int final_stage) {
-  __shared__ BoxDesc sb;
+__device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, int out_sel, int half,
+                                           int final_stage, float *red) {
+  const GridParams &g = d.g;
+  StepCtl *ctl = d.ctl;
+  const int lt = t - d.tile_begin;
+  const int bx0 = lt % d.tiles_x * BX, by0 = lt / d.tiles_x % d.tiles_y * BY, bz0 = lt / (d.tiles_x * d.tiles_y) * BZ;
+  const int x = bx0 + threadIdx.x, y = by0 + threadIdx.y, z = bz0 + threadIdx.z;
+  const bool inside = x < g.sx && y < g.sy && z < g.sz;
+  float dt = step_dt(ctl, nullptr);
+  if (half) dt = dt / 2.0f;
+  if (KIND == 0) {
+    if (inside) flux_cell(g, pick(ctl, in_sel, d.w0, d.w1, d.wp), d.flux, x, y, z, dt);
+  } else if (KIND == 1) {
+    if (inside) {
+      const float *win = pick(ctl, in_sel, d.w0, d.w1, d.wp), *wb = pick(ctl, 0, d.w0, d.w1, d.wp);
+      float *wo = const_cast<float *>(pick(ctl, out_sel, d.w0, d.w1, d.wp));
+      const int o = (z * g.sy + y) * g.sx + x;
+      // tiles whose cells and their +-1 neighbours all lie inside the box
+      // address the neighbours without the periodic wrap
+      const bool inner = NMHD_BATCH_CT_INNER && bx0 >= 1 && bx0 + BX < g.sx && by0 >= 1 && by0 + BY < g.sy &&
+                         bz0 >= 1 && bz0 + BZ < g.sz;
+      if (g.pow2_spacing) {
+        if (inner) ct_core<true>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
+        else ct_core<true>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
+      } else {
+        if (inner) ct_core<false>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
+        else ct_core<false>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
+      }
+    }
+  } else {
+    float tcfl = __uint_as_float(0x7f800000u);
+    int bad = 0;
+    if (inside) {
+      const float *wb = pick(ctl, 0, d.w0, d.w1, d.wp);
+      float *wo = const_cast<float *>(pick(ctl, out_sel, d.w0, d.w1, d.wp));
+      tcfl = g.pow2_spacing ? prim_cell<true>(g, wb, wo, d.flux, x, y, z, dt, final_stage != 0, &bad)
+                            : prim_cell<false>(g, wb, wo, d.flux, x, y, z, dt, final_stage != 0, &bad);
+    }
+    if (final_stage) finish_tile(ctl, (unsigned)(d.tiles_x * d.tiles_y * d.tiles_z), tcfl, bad, d.dt_hist, red);
+  }
+}
+
+// One stage kernel over the tiles of a group, in one of two schedules picked
+// per kernel by nmhd_batch_autotune.  kPersist: a grid of as many CTAs as are
+// resident at once, each walking a contiguous range of tiles; otherwise one
+// tile per CTA (the default: measured faster for every kernel on the 64-box
+// and 512-box ensembles, since the hardware scheduler then balances uneven
+// tiles across the SMs).  Resident CTAs per SM asked of the compiler:
+// NMHD_BATCH_MIN_BLOCKS_<kind>: 4, 3 (4 spills ~100 bytes), 4.
+#ifndef NMHD_BATCH_MIN_BLOCKS_0
+#define NMHD_BATCH_MIN_BLOCKS_0 4
+#endif
+#ifndef NMHD_BATCH_MIN_BLOCKS_1
+#define NMHD_BATCH_MIN_BLOCKS_1 3
+#endif
+#ifndef NMHD_BATCH_MIN_BLOCKS_2
+#define NMHD_BATCH_MIN_BLOCKS_2 4
+#endif
+template <int KIND, bool kPersist>
+__global__ void __launch_bounds__(kThreads, KIND == 0 ? NMHD_BATCH_MIN_BLOCKS_0
+                                                      : (KIND == 1 ? NMHD_BATCH_MIN_BLOCKS_1 : NMHD_BATCH_MIN_BLOCKS_2))
+    k_batch_stage(const __grid_constant__ BatchGroup p, int in_sel, int out_sel, int half, int final_stage) {
   __shared__ float red[kThreads / 32];
-  const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
-  // a contiguous range of tiles per CTA: consecutive tiles mostly share a box
-  const int t0 = (int)((long long)total_tiles * blockIdx.x / gridDim.x);
-  const int t1 = (int)((long long)total_tiles * (blockIdx.x + 1) / gridDim.x);
-  if (t0 >= t1) return;
-  int b = find_box(nb, t0, [&](int k) { return (long long)boxes[k].tile_begin; });
-  int b_end = -1;  // first tile past the box held in sb
+  if (!kPersist) {
+    const int t = blockIdx.x;
+    const BoxDesc &d = p.box[group_box(p, t)];
+    if (d.ctl->done) return;
+    batch_tile<KIND>(d, t, in_sel, out_sel, half, final_stage, red);
+    return;
+  }
+  const int t0 = (int)((long long)p.total_tiles * blockIdx.x / gridDim.x);
+  const int t1 = (int)((long long)p.total_tiles * (blockIdx.x + 1) / gridDim.x);
+  int b = group_box(p, t0);
   for (int t = t0; t < t1; ++t) {
-    if (t >= b_end) {
-      if (b_end >= 0) ++b;  // boxes are laid out in tile order
-      __syncthreads();      // everyone is done with the previous box
-      constexpr int kWords = sizeof(BoxDesc) / sizeof(int);
-      if (tid < kWords) reinterpret_cast<int *>(&sb)[tid] = reinterpret_cast<const int *>(boxes + b)[tid];
-      __syncthreads();
-      b_end = sb.tile_begin + sb.tiles_x * sb.tiles_y * sb.tiles_z;
-    }
-    const GridParams &g = sb.g;
-    StepCtl *ctl = sb.ctl;
-    if (ctl->done) continue;
-    const int lt = t - sb.tile_begin;
-    const int bx = lt % sb.tiles_x, by = (lt / sb.tiles_x) % sb.tiles_y, bz = lt / (sb.tiles_x * sb.tiles_y);
-    const int x = bx * BX + threadIdx.x, y = by * BY + threadIdx.y, z = bz * BZ + threadIdx.z;
-    const bool inside = x < g.sx && y < g.sy && z < g.sz;
-    float dt = step_dt(ctl, nullptr);
-    if (half) dt = dt / 2.0f;
-    if (KIND == 0) {
-      if (inside) flux_cell(g, pick(ctl, in_sel, sb.w0, sb.w1, sb.wp), sb.flux, x, y, z, dt);
-    } else if (KIND == 1) {
-      if (inside) {
-        const float *win = pick(ctl, in_sel, sb.w0, sb.w1, sb.wp), *wb = pick(ctl, 0, sb.w0, sb.w1, sb.wp);
-        float *wo = const_cast<float *>(pick(ctl, out_sel, sb.w0, sb.w1, sb.wp));
-        if (g.pow2_spacing) ct_cell<true, true>(g, win, wb, wo, sb.flux, x, y, z, dt);
-        else ct_cell<false, true>(g, win, wb, wo, sb.flux, x, y, z, dt);
-      }
-    } else {
-      float tcfl = __uint_as_float(0x7f800000u);
-      int bad = 0;
-      if (inside) {
-        const float *wb = pick(ctl, 0, sb.w0, sb.w1, sb.wp);
-        float *wo = const_cast<float *>(pick(ctl, out_sel, sb.w0, sb.w1, sb.wp));
-        tcfl = g.pow2_spacing ? prim_cell<true>(g, wb, wo, sb.flux, x, y, z, dt, final_stage != 0, &bad)
-                              : prim_cell<false>(g, wb, wo, sb.flux, x, y, z, dt, final_stage != 0, &bad);
-      }
-      if (final_stage)
-        finish_tile(ctl, (unsigned)(sb.tiles_x * sb.tiles_y * sb.tiles_z), tcfl, bad, sb.dt_hist, red);
-    }
+    while (t >= p.tile_begin[b + 1]) ++b;
+    const BoxDesc &d = p.box[b];
+    if (d.ctl->done) continue;
+    batch_tile<KIND>(d, t, in_sel, out_sel, half, final_stage, red);
   }
 }
 
@@ -164,6 +221,7 @@ __global__ void __launch_bounds__(256) k_batch_cfl(const BoxDesc *__restrict__ b
 }  // namespace
 }  // namespace nmhd
 
+using nmhd::BatchGroup;
 using nmhd::BoxDesc;
 using nmhd::GridParams;
 using nmhd::StepCtl;
@@ -178,7 +236,9 @@ struct nmhd_batch {
   StepCtl *ctls = nullptr;
   int total_tiles = 0;
   long long total_fill = 0, total_mcfl = 0, total_cells = 0;
-  int ctas[3] = {0, 0, 0};
+  std::vector<nmhd::BatchGroup> groups;  // launch groups of at most kGroupBoxes boxes
+  bool persist[3] = {false, false, false};  // schedule of each stage kernel (nmhd_batch_autotune)
+  int ctas[3] = {0, 0, 0};                  // resident CTAs of each persistent stage kernel
   int device = 0;
   cudaStream_t stream = nullptr;
   bool cfl_ready = false;
@@ -209,6 +269,25 @@ int grid_for(long long work, int cap) {
   return (int)std::max(1LL, std::min<long long>(blocks, cap));
 }
 
+template <int KIND>
+void launch_stage(const nmhd::BatchGroup &p, bool persist, int ctas, cudaStream_t st, int in_sel, int out_sel,
+                  int half, int fin) {
+  const dim3 blk(nmhd::cell::BX, nmhd::cell::BY, nmhd::cell::BZ);
+  if (persist)
+    nmhd::k_batch_stage<KIND, true><<<std::min(ctas, p.total_tiles), blk, 0, st>>>(p, in_sel, out_sel, half, fin);
+  else
+    nmhd::k_batch_stage<KIND, false><<<p.total_tiles, blk, 0, st>>>(p, in_sel, out_sel, half, fin);
+}
+
+// Kernel `kind` of one stage over every group.
+void launch_kind(nmhd_batch *b, int kind, int in_sel, int out_sel, int half, int fin) {
+  for (const BatchGroup &p : b->groups) {
+    if (kind == 0) launch_stage<0>(p, b->persist[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
+    else if (kind == 1) launch_stage<1>(p, b->persist[1], b->ctas[1], b->stream, in_sel, out_sel, half, fin);
+    else launch_stage<2>(p, b->persist[2], b->ctas[2], b->stream, in_sel, out_sel, half, fin);
+  }
+}
+
 void enqueue_batch_step(nmhd_batch *b) {
   using namespace nmhd;
   cudaStream_t st = b->stream;
@@ -217,14 +296,8 @@ void enqueue_batch_step(nmhd_batch *b) {
     k_batch_fill<<<grid_for(b->total_fill, cap), 256, 0, st>>>(b->d_boxes, b->n, b->total_fill);
   if (b->total_mcfl > 0)
     k_batch_cfl<<<grid_for(b->total_mcfl, cap), 256, 0, st>>>(b->d_boxes, b->n, b->total_mcfl, 0);
-  const dim3 blk(cell::BX, cell::BY, cell::BZ);
   auto stage = [&](int in_sel, int out_sel, int half, int fin) {
-    k_batch_stage<0><<<std::min(b->ctas[0], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
-                                                                           in_sel, out_sel, half, fin);
-    k_batch_stage<1><<<std::min(b->ctas[1], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
-                                                                           in_sel, out_sel, half, fin);
-    k_batch_stage<2><<<std::min(b->ctas[2], b->total_tiles), blk, 0, st>>>(b->d_boxes, b->n, b->total_tiles,
-                                                                           in_sel, out_sel, half, fin);
+    for (int kind = 0; kind < 3; ++kind) launch_kind(b, kind, in_sel, out_sel, half, fin);
   };
   stage(0, 2, 1, 0);
   stage(2, 1, 0, 1);
@@ -313,14 +386,29 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
     h[i].goal = INFINITY;
     h[i].hist_cap = nmhd::kDtHistCap;
   }
-  // persistent launch: as many CTAs as fit on the GPU at once
+  // persistent schedule: as many CTAs as fit on the GPU at once
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   int occ[3] = {1, 1, 1};
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0>, nmhd::cell::kThreads, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1>, nmhd::cell::kThreads, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0, true>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1, true>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2, true>, nmhd::cell::kThreads, 0);
   for (int k = 0; k < 3; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
+  // launch groups: consecutive boxes, tiles numbered from 0 within a group
+  for (int i0 = 0; i0 < n; i0 += nmhd::kGroupBoxes) {
+    BatchGroup p;
+    std::memset(&p, 0, sizeof p);
+    p.nb = std::min(nmhd::kGroupBoxes, n - i0);
+    for (int j = 0; j < p.nb; ++j) {
+      BoxDesc d = b->boxes[i0 + j];
+      d.tile_begin = p.total_tiles;
+      p.box[j] = d;
+      p.tile_begin[j] = p.total_tiles;
+      p.total_tiles += d.tiles_x * d.tiles_y * d.tiles_z;
+    }
+    p.tile_begin[p.nb] = p.total_tiles;
+    b->groups.push_back(p);
+  }
   e = cudaMemcpyAsync(b->d_boxes, b->boxes.data(), sizeof(BoxDesc) * n, cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess) e = cudaMemcpyAsync(b->ctls, h.data(), sizeof(StepCtl) * n, cudaMemcpyHostToDevice, b->stream);
   if (e == cudaSuccess) e = cudaStreamSynchronize(b->stream);
@@ -466,6 +554,91 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
     *steps_done = gen1 - gen0;
   }
   return result;
+}
+
+nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent) {
+  if (!b || kernel < 0 || kernel > 2 || (persistent != 0 && persistent != 1))
+    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..2 and persistent 0 or 1");
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  b->persist[kernel] = persistent != 0;
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  return NMHD_OK;
+}
+
+int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_trials) {
+  if (!b || reps <= 0) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  std::vector<StepCtl> h0;
+  nmhd_status st = read_ctls(b, h0);
+  if (st != NMHD_OK) return st;
+  for (int i = 0; i < b->n; ++i)
+    if (h0[i].status) return bfail(b, NMHD_ERR_NUMERICAL, "box " + std::to_string(i) + " holds an invalid state");
+  // every box live, with the CFL time step of its current state
+  std::vector<StepCtl> h = h0;
+  for (StepCtl &c : h) {
+    c.goal = INFINITY;
+    c.done = 0;
+    if (!b->cfl_ready) {
+      c.cfl_cur = c.cfl_next = 0x7f800000u;
+      c.blocks_done = 0;
+    }
+  }
+  st = write_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  const int cap = 148 * 16;
+  if (!b->cfl_ready) {
+    if (b->total_fill > 0)
+      nmhd::k_batch_fill<<<grid_for(b->total_fill, cap), 256, 0, b->stream>>>(b->d_boxes, b->n, b->total_fill);
+    nmhd::k_batch_cfl<<<grid_for(b->total_cells, cap), 256, 0, b->stream>>>(b->d_boxes, b->n, b->total_cells, 1);
+  }
+  // The first stage's kernels (state -> fluxes -> predictor) leave the state
+  // and the clocks alone, so each can be launched again and again on it.
+  const bool saved[3] = {b->persist[0], b->persist[1], b->persist[2]};
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  cudaError_t e = cudaEventCreate(&e0);
+  if (e == cudaSuccess) e = cudaEventCreate(&e1);
+  for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind) launch_kind(b, kind, 0, 2, 1, 0);
+  int written = 0;
+  for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind) {
+    double best = 1e30;
+    bool choice = saved[kind];
+    for (int persist = 0; persist < 2 && e == cudaSuccess; ++persist) {
+      b->persist[kind] = persist != 0;
+      launch_kind(b, kind, 0, 2, 1, 0);  // warm-up
+      e = cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) launch_kind(b, kind, 0, 2, 1, 0);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      const double per = ms / reps;
+      if (trials_out && written < max_trials) {
+        trials_out[3 * written + 0] = kind;
+        trials_out[3 * written + 1] = persist;
+        trials_out[3 * written + 2] = per;
+        ++written;
+      }
+      if (per < best) {
+        best = per;
+        choice = persist != 0;
+      }
+    }
+    b->persist[kind] = choice;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (e == cudaSuccess) e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    for (int k = 0; k < 3; ++k) b->persist[k] = saved[k];
+    return bfail(b, NMHD_ERR_CUDA, std::string("nmhd_batch_autotune: ") + cudaGetErrorString(e));
+  }
+  // the graphs hold the previous schedules
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  st = write_ctls(b, h0);  // clocks, goals and CFL minima as they were
+  if (st != NMHD_OK) return st;
+  return written;
 }
 
 const char *nmhd_batch_last_error(const nmhd_batch *b) { return b ? b->err.c_str() : g_batch_error.c_str(); }

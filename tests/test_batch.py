@@ -40,15 +40,24 @@ def test_batch_rejects_unsupported_configs_on_cpu():
 
 
 @pytest.mark.gpu
-def test_batch_boxes_equal_single_box_runs(gpu):
+@pytest.mark.parametrize("schedule", ["per_tile", "persistent", "mixed"])
+def test_batch_boxes_equal_single_box_runs(gpu, schedule):
+    """Every box of a batch equals its single-box run, in each schedule of the
+    stage kernels (persistent tile ranges or one tile per CTA)."""
     from nmhd_b200.batch import BatchSolver
     from nmhd_b200.solver import MHDSolver
+    persist = {"per_tile": (0, 0, 0), "persistent": (1, 1, 1), "mixed": (1, 0, 1)}[schedule]
     boxes, _ = small_ensemble()
     # add two non-shearing boxes of other shapes (power-of-two and not)
     boxes.append(orszag_tang_3d(16))
     boxes.append(orszag_tang_3d(24, ny=20, nz=12))
+    # and a box with interior tiles (cells and their +-1 neighbours away from
+    # every edge), which the CT kernel addresses without the periodic wrap
+    boxes.append(shearing_box(n_radial=24, n_azimuthal=128, n_vertical=8, l_azimuthal=4.0, seed=5))
     steps = 9
     with BatchSolver([c for c, _ in boxes]) as batch:
+        for k, p in enumerate(persist):
+            batch.set_schedule(k, p)
         for i, (c, s) in enumerate(boxes):
             batch.set_state(i, s)
         batch.step(4)
@@ -78,3 +87,58 @@ def test_batch_goal_time_per_box(gpu):
                 t, g = batch.clock(i)
                 assert t == float(np.float32(0.05)) and g == one.generation()
                 assert np.array_equal(batch.get_state(i), one.get_state())
+
+
+@pytest.mark.gpu
+def test_batch_of_more_boxes_than_one_launch_group(gpu):
+    """Batches beyond one launch group (128 boxes) are split into several
+    launches per kernel; boxes on both sides of a group boundary still equal
+    their single-box runs."""
+    from nmhd_b200.batch import BatchSolver
+    from nmhd_b200.solver import MHDSolver
+    boxes, _ = mri_ensemble(n_boxes=131, seed=11, sides=(8,), ratios=(2, 3))
+    steps = 5
+    with BatchSolver([c for c, _ in boxes]) as batch:
+        for i, (c, s) in enumerate(boxes):
+            batch.set_state(i, s)
+        batch.step(steps)
+        for i in (0, 1, 126, 127, 128, 129, 130):
+            c, s = boxes[i]
+            with MHDSolver(c) as one:
+                one.set_state(s)
+                one.step(steps)
+                t, g = batch.clock(i)
+                assert g == steps and t == one.current_time(), f"box {i} clock"
+                assert np.array_equal(batch.get_state(i), one.get_state()), f"box {i} state"
+
+
+@pytest.mark.gpu
+def test_batch_autotune_keeps_states_clocks_and_results(gpu):
+    """The schedule autotuner times both schedules of every stage kernel on the
+    current states, leaves states and clocks unchanged, and the batch then
+    still advances every box bitwise as its single-box run."""
+    from nmhd_b200.batch import BatchSolver
+    from nmhd_b200.solver import MHDSolver
+    boxes, _ = small_ensemble(n=5, seed=4)
+    with BatchSolver([c for c, _ in boxes]) as batch:
+        for i, (c, s) in enumerate(boxes):
+            batch.set_state(i, s)
+        batch.step(3)
+        before = [(batch.clock(i), batch.get_state(i)) for i in range(len(boxes))]
+        trials = batch.autotune(reps=2)
+        assert sorted((k, p) for k, p, _ in trials) == [(k, p) for k in range(3) for p in (False, True)]
+        assert all(ms > 0 for _, _, ms in trials)
+        for i, (clk, st) in enumerate(before):
+            assert batch.clock(i) == clk and np.array_equal(batch.get_state(i), st)
+        batch.step(4)
+        for i, (c, s) in enumerate(boxes):
+            with MHDSolver(c) as one:
+                one.set_state(s)
+                one.step(7)
+                assert np.array_equal(batch.get_state(i), one.get_state()), f"box {i}"
+
+
+def test_batch_schedule_arguments_are_checked_on_cpu():
+    L = _lib.lib()
+    assert L.nmhd_batch_set_schedule(None, 0, 0) == -1
+    assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
