@@ -414,6 +414,8 @@ def run_ensemble_arm(args):
     rank, world, local, dist = dist_setup(args.gpus)
     dev = torch.device("cuda", local)
     all_boxes, params = mri_ensemble(**ENSEMBLES[args.workload])
+    if args.boxes:  # the first N boxes only (small profiling cases)
+        all_boxes = all_boxes[:args.boxes]
     total_interior = sum(c.interior_cells for c, _ in all_boxes)
     # N > 1: the ensemble is partitioned over the ranks (boxes never exchange
     # data); every rank computes the same cost-balanced assignment
@@ -446,25 +448,27 @@ def run_ensemble_arm(args):
         ms = float(t.item())
     value = total_interior * args.steps / (ms * 1e-3) / 1e6
     # plain: each box through its own single-box solver, one after another
-    plain_steps = max(3, args.steps // 4)
+    plain_steps = 0 if args.no_plain else max(3, args.steps // 4)
     solvers = []
-    for c, s in boxes:
+    plain_wall = 0.0
+    for c, s in boxes if plain_steps else []:
         sol = MHDSolver(c)
         sol.set_stream(stream.cuda_stream)
         sol.set_state(s)
         sol.step(args.warmup)
         solvers.append(sol)
-    torch.cuda.synchronize(dev)
-    t0 = time.perf_counter()
-    for sol in solvers:
-        sol.step(plain_steps)
-    torch.cuda.synchronize(dev)
-    plain_wall = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([plain_wall], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        plain_wall = float(t.item())
-    plain = total_interior * plain_steps / plain_wall / 1e6
+    if plain_steps:
+        torch.cuda.synchronize(dev)
+        t0 = time.perf_counter()
+        for sol in solvers:
+            sol.step(plain_steps)
+        torch.cuda.synchronize(dev)
+        plain_wall = time.perf_counter() - t0
+        if dist:
+            t = torch.tensor([plain_wall], dtype=torch.float64, device=dev)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            plain_wall = float(t.item())
+    plain = total_interior * plain_steps / plain_wall / 1e6 if plain_steps else None
     for sol in solvers:
         sol.close()
     if rank == 0:
@@ -481,7 +485,7 @@ def run_ensemble_arm(args):
                                        round(ms, 4) for k, p, ms in tuning},
             "plain_per_box": {"value": plain, "unit": "Mcell-updates/s", "steps": plain_steps,
                               "note": "same boxes, one single-box solver each, stepped one after another"},
-            "batch_speedup": value / plain,
+            "batch_speedup": value / plain if plain else None,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)
@@ -731,6 +735,8 @@ def main():
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
     ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint workload: steps per run (default 200)")
+    ap.add_argument("--boxes", type=int, default=0, help="ensemble workloads: the first N boxes only")
+    ap.add_argument("--no-plain", action="store_true", help="ensemble workloads: skip the per-box plain arm")
     ap.add_argument("--tape-budget", type=int, default=-1,
                     help="adjoint workload: bytes of tape beyond the last segment (-1: half the free HBM)")
     args = ap.parse_args()
