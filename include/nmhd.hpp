@@ -286,6 +286,72 @@ class MHDSolver {
   std::function<int(MHDSolver &)> monitor_;
 };
 
+// Batched ensemble (nmhd_batch_*): many independent boxes advanced together,
+// each bitwise as an MHDSolver would advance it alone.  No counterpart in the
+// reference, which holds one compile-time box per process.
+class Batch {
+ public:
+  explicit Batch(const std::vector<nmhd_config> &boxes) : cfg_(boxes) {
+    nmhd_status st = nmhd_batch_create(cfg_.data(), (int)cfg_.size(), &b_);
+    if (st != NMHD_OK) throw Error(st, nmhd_batch_last_error(nullptr));
+  }
+  ~Batch() { nmhd_batch_destroy(b_); }
+  Batch(const Batch &) = delete;
+  Batch &operator=(const Batch &) = delete;
+
+  int size() const { return (int)cfg_.size(); }
+  size_t cells(int box) const {
+    const nmhd_config &c = cfg_.at(box);
+    return (size_t)c.size_x * c.size_y * c.size_z;
+  }
+  // State of one box as 8 host arrays in .bin order, concatenated.
+  void initialize_state(int box, const std::vector<float> &all) {
+    const float *f[8];
+    for (int v = 0; v < 8; ++v) f[v] = all.data() + v * cells(box);
+    check(nmhd_batch_set_state(b_, box, f, 0));
+  }
+  std::vector<float> state(int box) {
+    std::vector<float> all(8 * cells(box));
+    float *f[8];
+    for (int v = 0; v < 8; ++v) f[v] = all.data() + v * cells(box);
+    check(nmhd_batch_get_state(b_, box, f, 0));
+    return all;
+  }
+  // Every box until goal_time (or max_steps steps): true when all reached it.
+  bool proceed(float goal_time, long long max_steps = 0) {
+    int64_t done = 0;
+    const nmhd_status st = nmhd_batch_proceed(b_, goal_time, max_steps, &done);
+    check(st);
+    last_steps_ = done;
+    return st == NMHD_GOAL_REACHED;
+  }
+  double current_time(int box) {
+    double t = 0;
+    check(nmhd_batch_clock(b_, box, &t, nullptr));
+    return t;
+  }
+  int generation(int box) {
+    int64_t g = 0;
+    check(nmhd_batch_clock(b_, box, nullptr, &g));
+    return (int)g;
+  }
+  // Stage-kernel schedules timed on the current states (states unchanged).
+  void autotune(int reps = 5) {
+    const int k = nmhd_batch_autotune(b_, reps, nullptr, 0);
+    if (k < 0) throw Error((nmhd_status)k, nmhd_batch_last_error(b_));
+  }
+  long long last_steps() const { return last_steps_; }
+  nmhd_batch *handle() { return b_; }
+
+ private:
+  void check(nmhd_status st) {
+    if (st < 0) throw Error(st, nmhd_batch_last_error(b_));
+  }
+  std::vector<nmhd_config> cfg_;
+  nmhd_batch *b_ = nullptr;
+  long long last_steps_ = 0;
+};
+
 }  // namespace nmhd
 
 #endif  // NMHD_HPP

@@ -92,3 +92,18 @@ def test_orszag_tang_face_field_is_divergence_free():
     bx, by = s[5].astype(np.float64), s[6].astype(np.float64)
     div = (np.roll(bx, -1, axis=2) - bx) * 32 + (np.roll(by, -1, axis=1) - by) * 32
     assert np.max(np.abs(div)) < 1e-4
+
+
+def test_cpp_mirror_compiles_and_links(tmp_path):
+    """include/nmhd.hpp (MHDSolver, Batch, checkpoint) compiles as C++17 and
+    links against libnmhd.so (nothing runs)."""
+    import subprocess
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    src = tmp_path / "m.cpp"
+    src.write_text('#include "nmhd.hpp"\n'
+                   'int main() { std::vector<nmhd_config> b(1); '
+                   'if (b.size() == 7) { nmhd::Batch x(b); nmhd::MHDSolver y(b[0]); x.autotune(); y.proceed(1.f); } '
+                   'return 0; }\n')
+    lib = os.path.join(root, "nmhd_b200")
+    subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(root, "include"), str(src),
+                    "-L" + lib, "-lnmhd", "-Wl,-rpath," + lib, "-o", str(tmp_path / "m")], check=True)
