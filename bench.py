@@ -565,7 +565,10 @@ def run_slab_arm(args):
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
                          "unit_of_work": "one RK2 step of one slab (whole-step time); 160 B per cell-update"},
-            "gpu_launches": 7 * args.steps,
+            # per step: halo pack, halo unpack (+ Z fill), margin CFL, and 3
+            # kernels per RK stage (the CFL all-reduce and the halo transfer
+            # are NCCL's)
+            "gpu_launches": (2 * (cfg.margin_y > 0) + (cfg.margin_z > 0) + 1 + 6) * args.steps,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -581,12 +581,22 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       NMHD_CUDA(s, cudaEventElapsedTime(&ms, ev[k], ev[k + 1]));
       acc[k] += ms;
     }
-    cnt[0] += margins;
+    // kernel launches of each class: fill (Y and Z margins), margin CFL, and
+    // per stage the flux class (variant 3: the whole chunked stage) and the
+    // update class (variant 2: CT + conserved update; the per-stage predictor
+    // refill is timed with the first stage's update)
+    const int fills = (g.my > 0) + (g.mz > 0);
+    const int nch = s->variant == 3 ? (g.sz + (s->shape.zc < 1 ? g.sz : s->shape.zc) - 1) /
+                                          (s->shape.zc < 1 ? g.sz : s->shape.zc)
+                                    : 0;
+    const int flux_n = s->variant == 3 ? 3 * nch : 1;
+    const int upd_n = s->variant == 3 ? 0 : (s->variant == 2 ? 2 : 1);
+    cnt[0] += fills;
     cnt[1] += margins;
-    cnt[2] += midpoint;
-    cnt[3] += midpoint;
-    cnt[4] += 1;
-    cnt[5] += 1;
+    cnt[2] += midpoint ? flux_n : 0;
+    cnt[3] += midpoint ? upd_n + ((s->cfg.flags & NMHD_FLAG_HALO_PER_STAGE) ? fills : 0) : 0;
+    cnt[4] += flux_n;
+    cnt[5] += upd_n;
   }
   for (auto &e : ev) cudaEventDestroy(e);
   NMHD_CUDA(s, cudaGetLastError());
