@@ -356,3 +356,23 @@ def test_monitor_hook_runs_before_every_step(gpu):
         sol.set_state(s)
         assert sol.proceed(0.05) is True
         assert sol.calls == sol.generation()
+
+
+@pytest.mark.parametrize("variant,zc,mz,expect", [(2, 0, 0, 8), (2, 0, 2, 9), (0, 0, 0, 6), (3, 4, 0, 2 + 2 * 3 * 2)])
+def test_profile_counts_kernel_launches(gpu, variant, zc, mz, expect):
+    """nmhd_profile reports each class's kernel launches per step (the bench's
+    gpu_launches): fill (Y, Z), margin CFL, flux and update of each stage;
+    the profiled steps advance the state as the graph path would."""
+    cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=61)
+    if mz:
+        cfg.margin_z, cfg.size_z = mz, 8 + 2 * mz
+        s = np.concatenate([s[:, -mz:], s, s[:, :mz]], axis=1)
+    o = oracle.proceed(cfg, s, 3)
+    with MHDSolver(cfg) as sol:
+        sol.set_kernel(variant, 8, zc)
+        sol.set_state(s)
+        prof = sol.profile(3)
+        assert sum(n for _, n in prof.values()) == expect
+        assert all(ms >= 0 for ms, _ in prof.values())
+        assert sol.generation() == 3
+        assert_same(sol.get_state(), o["state"])
