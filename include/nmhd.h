@@ -175,12 +175,16 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * its flux class).  tile_rows is used by variant 0 only, z_chunk by variants
  * 0 and 3.  Every variant gives bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
+/* The solver's kernel selection (any pointer may be NULL). */
+nmhd_status nmhd_get_kernel(const nmhd_solver *s, int *variant, int *tile_rows, int *z_chunk);
 /* Autotuner (replaces the reference's Ruby GA/parallel-tempering tuner of
  * launch dimensions, src/nushio_script/optimization.rb:33-140,
  * optimization_manager.rb:63-256).  Times `steps` steps of every kernel
  * variant and tile shape on this solver's box with CUDA events, starting each
  * trial from the current state, then restores the state and clock and selects
- * the fastest.  trials_out (may be NULL) receives up to max_trials rows of
+ * the fastest; solvers created later in the process for boxes of the same
+ * shape, margins, problem and scheme start with that selection.  trials_out
+ * (may be NULL) receives up to max_trials rows of
  * (variant, tile_rows, z_chunk, ms_per_step).  Returns the number of rows
  * written or a negative nmhd_status.  Every candidate gives bitwise the same
  * result, so tuning never changes the physics. */

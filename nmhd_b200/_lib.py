@@ -57,6 +57,8 @@ _SIGS = [
     ("nmhd_profile", ctypes.c_int, [_P, ctypes.c_int, _P, _P, ctypes.c_int]),
     ("nmhd_kernel_name", ctypes.c_char_p, [ctypes.c_int]),
     ("nmhd_set_kernel", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("nmhd_get_kernel", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                       ctypes.POINTER(ctypes.c_int)]),
     ("nmhd_autotune", ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int]),
     ("nmhd_advance_noalloc", ctypes.c_int, [_P, _P, _P, ctypes.POINTER(ctypes.c_double),
                                             ctypes.POINTER(ctypes.c_int64), ctypes.c_double,

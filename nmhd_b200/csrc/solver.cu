@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <mutex>
 #include <tuple>
 #include <string>
 #include <vector>
@@ -226,6 +227,10 @@ nmhd_status copy_fields(nmhd_solver *s, float *dev_base, const float *const in[8
 
 }  // namespace
 
+// Kernel choice of nmhd_autotune for boxes of this shape, if one was tuned
+// in this process (defined with the autotuner below).
+void apply_tuned(nmhd_solver *s);
+
 extern "C" {
 
 const char *nmhd_version(void) { return kVersion; }
@@ -270,6 +275,7 @@ nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
     nmhd_destroy(s);
     return st;
   }
+  apply_tuned(s);
   *out = s;
   return NMHD_OK;
 }
@@ -627,6 +633,16 @@ nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_ch
   return NMHD_OK;
 }
 
+nmhd_status nmhd_get_kernel(const nmhd_solver *s, int *variant, int *tile_rows, int *z_chunk) {
+  if (!s) return NMHD_ERR_INVALID_ARGUMENT;
+  if (variant) *variant = s->variant;
+  if (tile_rows) *tile_rows = s->shape.ty;
+  if (z_chunk) *z_chunk = s->shape.zc;
+  return NMHD_OK;
+}
+
+}  // extern "C"
+
 namespace {
 struct TuneKey {
   int sx, sy, sz, my, mz, problem, so, to;
@@ -639,15 +655,31 @@ struct TuneChoice {
   int variant, rows, zc;
 };
 std::map<TuneKey, TuneChoice> g_tune_cache;
+std::mutex g_tune_mutex;  // solvers may be created and tuned from several host threads
+
+TuneKey tune_key(const nmhd_solver *s) {
+  const GridParams &g = s->g;
+  return TuneKey{g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order,
+                 s->cfg.time_order + 8 * s->cfg.flags};
+}
 }  // namespace
+
+void apply_tuned(nmhd_solver *s) {
+  std::lock_guard<std::mutex> lock(g_tune_mutex);
+  auto it = g_tune_cache.find(tune_key(s));
+  if (it == g_tune_cache.end()) return;
+  s->variant = it->second.variant;
+  s->shape = nmhd::TileShape{it->second.rows, it->second.zc};
+}
+
+extern "C" {
 
 int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials) {
   if (!s || steps <= 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
   if (s->cfg.parallel_size_y > 1)
     return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
   const GridParams &g = s->g;
-  const TuneKey key = {g.sx, g.sy, g.sz, g.my, g.mz, s->cfg.problem, s->cfg.space_order,
-                       s->cfg.time_order + 8 * s->cfg.flags};
+  const TuneKey key = tune_key(s);
   std::vector<TuneChoice> cands;
   cands.push_back({2, 8, 0});
   if (!(s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)) {  // the fast flux kernel exists for variant 2 only
@@ -729,7 +761,10 @@ int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials)
   drop_graphs(s);
   s->variant = choice.variant;
   s->shape = nmhd::TileShape{choice.rows, choice.zc};
-  g_tune_cache[key] = choice;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[key] = choice;
+  }
   return written;
 }
 

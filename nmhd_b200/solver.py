@@ -255,9 +255,17 @@ class MHDSolver:
         _check(self._L, self._h, self._L.nmhd_set_kernel(self._h, int(variant), int(tile_rows),
                                                          int(z_chunk)))
 
+    def kernel(self):
+        """The current kernel selection: (variant, tile_rows, z_chunk)."""
+        v, r, z = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        _check(self._L, self._h, self._L.nmhd_get_kernel(self._h, ctypes.byref(v), ctypes.byref(r),
+                                                         ctypes.byref(z)))
+        return v.value, r.value, z.value
+
     def autotune(self, steps=5):
         """Time every kernel variant / tile shape on this box and keep the
-        fastest; returns [(variant, tile_rows, z_chunk, ms_per_step), ...]."""
+        fastest (solvers created later for boxes of the same shape and scheme
+        start with it); returns [(variant, tile_rows, z_chunk, ms_per_step), ...]."""
         out = np.zeros((64, 4), np.float64)
         k = _check(self._L, self._h, self._L.nmhd_autotune(self._h, int(steps), out.ctypes.data, 64))
         return [(int(a), int(b), int(c), float(d)) for a, b, c, d in out[:k]]

@@ -297,11 +297,20 @@ def test_autotune_restores_state_and_keeps_results_bitwise(gpu):
         t_mid = sol.current_time()
         trials = sol.autotune(steps=2)
         assert len(trials) >= 5
+        best = min(trials, key=lambda r: r[3])
+        assert sol.kernel() == best[:3]
         assert sol.generation() == 2 and sol.current_time() == t_mid
         assert_same(sol.get_state(), mid)
         sol.step(4)
         assert sol.current_time() == o["time"]
         assert_same(sol.get_state(), o["state"])
+    # a later solver for a box of the same shape and scheme starts with the
+    # tuned selection; another shape keeps the default
+    with MHDSolver(cfg) as again:
+        assert again.kernel() == best[:3]
+    other, _ = shearing_box(n_radial=16, n_azimuthal=64, n_vertical=12, l_azimuthal=4.0, seed=13)
+    with MHDSolver(other) as fresh:
+        assert fresh.kernel()[0] == 2
 
 
 @pytest.mark.parametrize("zc", [1, 2, 5])
