@@ -160,8 +160,9 @@ const char *nmhd_last_error(const nmhd_solver *s);
 /* Per-kernel timing (no counterpart in the reference, which has no timers;
  * replaces its wallclock bench, src/application/optimize_mhd/main_detail.curb:27-57).
  * Runs `steps` steps launching every kernel separately with CUDA events around
- * it on the solver's stream; ms_out[i] receives the mean duration of kernel
- * class i and launches_out[i] (may be NULL) its kernel launches per step.  Returns the
+ * it on the solver's stream; ms_out[i] receives the mean device time per step
+ * of kernel class i and launches_out[i] (may be NULL) its kernel launches per
+ * step.  Returns the
  * number of classes written (at most max), or a negative nmhd_status. */
 int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out, int max);
 /* Kernel selection (the reference picks launch shapes with its Ruby autotuner,

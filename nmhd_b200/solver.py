@@ -271,8 +271,8 @@ class MHDSolver:
         return [(int(a), int(b), int(c), float(d)) for a, b, c, d in out[:k]]
 
     def profile(self, steps):
-        """Mean device time (ms) and launches per step of every kernel class,
-        from CUDA events around separately launched kernels."""
+        """Per kernel class: (mean device ms per step, kernel launches per
+        step), from CUDA events around separately launched kernels."""
         ms = np.zeros(16, np.float64)
         launches = np.zeros(16, np.float64)
         k = _check(self._L, self._h, self._L.nmhd_profile(self._h, int(steps), ms.ctypes.data,
