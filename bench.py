@@ -429,8 +429,8 @@ def run_ensemble_arm(args):
     batch.step(args.warmup)
     # schedule of each stage kernel (persistent or one tile per CTA), timed on these boxes
     tuning = batch.autotune(reps=3)
-    schedule = {("flux", "ct", "update")[k]: "persistent" if p else "per_tile"
-                for k, p, ms in tuning if ms == min(m for kk, _, m in tuning if kk == k)}
+    schedule = {("flux", "ct", "update")[k]: ("persistent" if p else "per_tile") + ("_split" if s else "")
+                for k, p, s, ms in tuning if ms == min(m for kk, _, _, m in tuning if kk == k)}
     batch.step(args.warmup)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
@@ -481,8 +481,8 @@ def run_ensemble_arm(args):
                        "parallelism": "boxes sharded over %d GPUs" % world if world > 1 else "single",
                        "timing": "host wallclock around proceed() (one sync per 16-step graph)",
                        "schedule": schedule},
-            "autotune_ms_per_launch": {"%s_%s" % (("flux", "ct", "update")[k], "persistent" if p else "per_tile"):
-                                       round(ms, 4) for k, p, ms in tuning},
+            "autotune_ms_per_launch": {"%s_%s%s" % (("flux", "ct", "update")[k], "persistent" if p else "per_tile",
+                                                    "_split" if s else ""): round(ms, 4) for k, p, s, ms in tuning},
             "plain_per_box": {"value": plain, "unit": "Mcell-updates/s", "steps": plain_steps,
                               "note": "same boxes, one single-box solver each, stepped one after another"},
             "batch_speedup": value / plain if plain else None,

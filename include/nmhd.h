@@ -228,7 +228,8 @@ const char *nmhd_noalloc_last_error(void);
  * nmhd_proceed would advance it alone.  Each kernel of a step is one launch
  * over all boxes (per group of 128 boxes, whose descriptors travel in the
  * launch's parameter block), either persistent (a resident grid walking tile
- * ranges) or one 32x4x2-cell tile per CTA, as nmhd_batch_autotune picks;
+ * ranges) or one tile per CTA, as nmhd_batch_autotune picks; each box has its
+ * own tile shape (nmhd_batch_tile_shape);
  * batches of steps are one CUDA graph.  Batched boxes use time_order 2 and no
  * Z margins. */
 typedef struct nmhd_batch nmhd_batch;
@@ -244,17 +245,25 @@ nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *gene
  * (semantics of nmhd_proceed, per box; a box that reached the goal waits).
  * *steps_done: steps taken by the box that took most. */
 nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
+/* Tile of box `box` in the batched kernels: tile_x x tile_y x tile_z cells (256
+ * threads), chosen per box to launch the fewest padded cells, at least 8 wide
+ * in x; ties keep 32 x 4 x 2. */
+nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int *tile_y, int *tile_z);
 /* Schedule of stage kernel `kernel` (0 face fluxes, 1 constrained transport,
  * 2 conserved update): persistent = 1 for the resident grid walking tile
- * ranges, 0 for one tile per CTA (the default). */
-nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent);
+ * ranges, 0 for one tile per CTA (the default); split = 1 (the default) runs
+ * the boxes with 32 x 4 x 2 tiles in a launch of their own through a kernel
+ * compiled for that shape (fewer registers), 0 runs every box in one launch of
+ * the general form (half the launches: better for many small boxes). */
+nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split);
 /* Schedule autotuner of the batch (the batched counterpart of nmhd_autotune).
  * Times `reps` launches of each stage kernel (face fluxes, constrained
- * transport, conserved update) in both schedules on the boxes' current states
- * with CUDA events, keeps the faster per kernel, and leaves states and clocks
- * unchanged.  trials_out (may be NULL) receives up to max_trials rows of
- * (kernel, persistent, ms per launch).  Returns the number of rows written or a
- * negative nmhd_status.  Both schedules give bitwise the same result. */
+ * transport, conserved update) in every schedule (persistent or not, split or
+ * not) on the boxes' current states with CUDA events, keeps the fastest per
+ * kernel, and leaves states and clocks unchanged.  trials_out (may be NULL)
+ * receives up to max_trials rows of (kernel, persistent, split, ms per
+ * launch).  Returns the number of rows written or a negative nmhd_status.
+ * Every schedule gives bitwise the same result. */
 int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_trials);
 const char *nmhd_batch_last_error(const nmhd_batch *b);
 

@@ -83,7 +83,9 @@ _SIGS = [
                                         ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64)]),
-    ("nmhd_batch_set_schedule", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int]),
+    ("nmhd_batch_set_schedule", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
+    ("nmhd_batch_tile_shape", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
+                                             ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("nmhd_batch_autotune", ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int]),
     ("nmhd_batch_last_error", ctypes.c_char_p, [_P]),
     ("nmhd_halo_count", ctypes.c_int64, [_P]),

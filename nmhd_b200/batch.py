@@ -86,18 +86,27 @@ class BatchSolver:
         self.proceed(math.inf, nsteps)
         return self.last_steps
 
-    def set_schedule(self, kernel, persistent):
+    def tile_shape(self, i):
+        """Tile of box i in the batched kernels: (x, y, z) cells."""
+        v = [ctypes.c_int() for _ in range(3)]
+        self._check(self._L.nmhd_batch_tile_shape(self._h, int(i), *[ctypes.byref(c) for c in v]))
+        return tuple(c.value for c in v)
+
+    def set_schedule(self, kernel, persistent, split=True):
         """Schedule of stage kernel ``kernel`` (0 fluxes, 1 constrained
-        transport, 2 conserved update): persistent or one tile per CTA."""
-        self._check(self._L.nmhd_batch_set_schedule(self._h, int(kernel), int(bool(persistent))))
+        transport, 2 conserved update): persistent or one tile per CTA; with
+        ``split`` the boxes with 32 x 4 x 2 tiles run in a launch of their own."""
+        self._check(self._L.nmhd_batch_set_schedule(self._h, int(kernel), int(bool(persistent)),
+                                                    int(bool(split))))
 
     def autotune(self, reps=5):
-        """Pick each stage kernel's schedule (persistent or one tile per CTA)
-        by timing both on the current states; states and clocks are left
-        unchanged.  Returns rows (kernel, persistent, ms per launch)."""
-        out = np.zeros((6, 3), dtype=np.float64)
-        k = self._check(self._L.nmhd_batch_autotune(self._h, int(reps), out.ctypes.data, 6))
-        return [(int(a), bool(b), float(c)) for a, b, c in out[:k]]
+        """Pick each stage kernel's schedule (persistent or one tile per CTA,
+        split or not) by timing all of them on the current states; states and
+        clocks are left unchanged.  Returns rows (kernel, persistent, split,
+        ms per launch)."""
+        out = np.zeros((12, 4), dtype=np.float64)
+        k = self._check(self._L.nmhd_batch_autotune(self._h, int(reps), out.ctypes.data, 12))
+        return [(int(a), bool(b), bool(c), float(d)) for a, b, c, d in out[:k]]
 
     @property
     def cells(self):

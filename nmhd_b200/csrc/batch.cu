@@ -14,9 +14,11 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "../../include/nmhd.h"
@@ -30,7 +32,8 @@ struct __align__(8) BoxDesc {
   float *w0, *w1, *wp, *flux, *dt_hist;
   StepCtl *ctl;
   int tile_begin;                 // first tile of this box in the flattened list
-  int tiles_x, tiles_y, tiles_z;  // 32 x 4 x 2-cell tiles per axis
+  int tiles_x, tiles_y, tiles_z;  // tiles per axis
+  int lx, ly, lz;                 // tile of 2^lx x 2^ly x 2^lz cells (256 threads)
   long long fill_begin;           // first Y-margin fill item
   long long mcfl_begin;           // first margin-CFL cell
   long long cell_begin;           // first cell
@@ -65,6 +68,7 @@ constexpr int kGroupBoxes = 128;
 struct BatchGroup {
   int nb;                           // boxes in this group
   int total_tiles;                  // tiles of this group
+  int fixed_tiles;                  // tiles [0, fixed_tiles): the boxes with 32 x 4 x 2 tiles, placed first
   int tile_begin[kGroupBoxes + 1];  // group-local first tile of each box; [nb] = total_tiles
   BoxDesc box[kGroupBoxes];
 };
@@ -87,17 +91,22 @@ __device__ __forceinline__ int group_box(const BatchGroup &p, int t) {
 #define NMHD_BATCH_CT_INNER 1
 #endif
 
-// One tile (32 x 4 x 2 cells) of one stage kernel.  KIND 0: face fluxes, 1:
-// constrained transport, 2: conserved update + primitive recovery (+ CFL and
-// clock in the final stage).
-template <int KIND>
+// One tile of one stage kernel: the box's 2^lx x 2^ly x 2^lz cells on the
+// CTA's 256 threads (a 1-D block).  KIND 0: face fluxes, 1: constrained
+// transport, 2: conserved update + primitive recovery (+ CFL and clock in the
+// final stage).
+// kFixed: the box has the single-box kernels' 32 x 4 x 2 tile (the shape is
+// then a compile-time constant: fewer registers than the general form).
+template <int KIND, bool kFixed>
 __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, int out_sel, int half,
                                            int final_stage, float *red) {
   const GridParams &g = d.g;
   StepCtl *ctl = d.ctl;
+  const int lx = kFixed ? 5 : d.lx, ly = kFixed ? 2 : d.ly, lz = kFixed ? 1 : d.lz;
   const int lt = t - d.tile_begin;
-  const int bx0 = lt % d.tiles_x * BX, by0 = lt / d.tiles_x % d.tiles_y * BY, bz0 = lt / (d.tiles_x * d.tiles_y) * BZ;
-  const int x = bx0 + threadIdx.x, y = by0 + threadIdx.y, z = bz0 + threadIdx.z;
+  const int bx0 = lt % d.tiles_x << lx, by0 = lt / d.tiles_x % d.tiles_y << ly, bz0 = lt / (d.tiles_x * d.tiles_y) << lz;
+  const int tid = threadIdx.x;
+  const int x = bx0 + (tid & ((1 << lx) - 1)), y = by0 + ((tid >> lx) & ((1 << ly) - 1)), z = bz0 + (tid >> (lx + ly));
   const bool inside = x < g.sx && y < g.sy && z < g.sz;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
@@ -110,8 +119,8 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
       const int o = (z * g.sy + y) * g.sx + x;
       // tiles whose cells and their +-1 neighbours all lie inside the box
       // address the neighbours without the periodic wrap
-      const bool inner = NMHD_BATCH_CT_INNER && bx0 >= 1 && bx0 + BX < g.sx && by0 >= 1 && by0 + BY < g.sy &&
-                         bz0 >= 1 && bz0 + BZ < g.sz;
+      const bool inner = NMHD_BATCH_CT_INNER && bx0 >= 1 && bx0 + (1 << lx) < g.sx && by0 >= 1 &&
+                         by0 + (1 << ly) < g.sy && bz0 >= 1 && bz0 + (1 << lz) < g.sz;
       if (g.pow2_spacing) {
         if (inner) ct_core<true>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
         else ct_core<true>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
@@ -149,26 +158,29 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
 #ifndef NMHD_BATCH_MIN_BLOCKS_2
 #define NMHD_BATCH_MIN_BLOCKS_2 4
 #endif
-template <int KIND, bool kPersist>
+template <int KIND, bool kPersist, bool kFixed>
 __global__ void __launch_bounds__(kThreads, KIND == 0 ? NMHD_BATCH_MIN_BLOCKS_0
                                                       : (KIND == 1 ? NMHD_BATCH_MIN_BLOCKS_1 : NMHD_BATCH_MIN_BLOCKS_2))
-    k_batch_stage(const __grid_constant__ BatchGroup p, int in_sel, int out_sel, int half, int final_stage) {
+    k_batch_stage(const __grid_constant__ BatchGroup p, int tb, int te, int in_sel, int out_sel, int half,
+                  int final_stage) {
   __shared__ float red[kThreads / 32];
+  // this launch's tiles [tb, te): all of the group's, or (split) the
+  // fixed-shape boxes' or the others'
   if (!kPersist) {
-    const int t = blockIdx.x;
+    const int t = tb + blockIdx.x;
     const BoxDesc &d = p.box[group_box(p, t)];
     if (d.ctl->done) return;
-    batch_tile<KIND>(d, t, in_sel, out_sel, half, final_stage, red);
+    batch_tile<KIND, kFixed>(d, t, in_sel, out_sel, half, final_stage, red);
     return;
   }
-  const int t0 = (int)((long long)p.total_tiles * blockIdx.x / gridDim.x);
-  const int t1 = (int)((long long)p.total_tiles * (blockIdx.x + 1) / gridDim.x);
+  const int t0 = tb + (int)((long long)(te - tb) * blockIdx.x / gridDim.x);
+  const int t1 = tb + (int)((long long)(te - tb) * (blockIdx.x + 1) / gridDim.x);
   int b = group_box(p, t0);
   for (int t = t0; t < t1; ++t) {
     while (t >= p.tile_begin[b + 1]) ++b;
     const BoxDesc &d = p.box[b];
     if (d.ctl->done) continue;
-    batch_tile<KIND>(d, t, in_sel, out_sel, half, final_stage, red);
+    batch_tile<KIND, kFixed>(d, t, in_sel, out_sel, half, final_stage, red);
   }
 }
 
@@ -238,6 +250,7 @@ struct nmhd_batch {
   long long total_fill = 0, total_mcfl = 0, total_cells = 0;
   std::vector<nmhd::BatchGroup> groups;  // launch groups of at most kGroupBoxes boxes
   bool persist[3] = {false, false, false};  // schedule of each stage kernel (nmhd_batch_autotune)
+  bool split[3] = {true, true, true};       // boxes with 32 x 4 x 2 tiles in a launch of their own
   int ctas[3] = {0, 0, 0};                  // resident CTAs of each persistent stage kernel
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -264,27 +277,56 @@ nmhd_status bfail(nmhd_batch *b, nmhd_status st, const std::string &msg) {
                    std::string(#call) + ": " + cudaGetErrorString(e_));                          \
   } while (0)
 
+// Tile shape of a box: the 256 threads of a CTA as 2^lx x 2^ly x 2^lz cells,
+// at least 8 wide in x (coalesced rows), chosen to launch the fewest padded
+// cells; among equals the widest x, then the shape nearest the single-box
+// kernels' 32 x 4 x 2 (stencil neighbours in y and z inside the tile).  Small
+// or ragged boxes (e.g. 16 or 48 cells wide) would otherwise idle up to half
+// of each warp.
+void pick_tile(const GridParams &g, int &lx, int &ly, int &lz) {
+  auto padded = [&](int a, int b, int c) {
+    return (long long)((g.sx + (1 << a) - 1) >> a << a) * ((g.sy + (1 << b) - 1) >> b << b) *
+           ((g.sz + (1 << c) - 1) >> c << c);
+  };
+  auto key = [&](int a, int b, int c) {
+    return std::make_tuple(padded(a, b, c), -a, std::abs(b - 2) + std::abs(c - 1), -b);
+  };
+  lx = 5, ly = 2, lz = 1;
+  for (int a = 5; a >= 3; --a)
+    for (int b = 0; a + b <= 8; ++b)
+      if (key(a, b, 8 - a - b) < key(lx, ly, lz)) lx = a, ly = b, lz = 8 - a - b;
+}
+
 int grid_for(long long work, int cap) {
   long long blocks = (work + 255) / 256;
   return (int)std::max(1LL, std::min<long long>(blocks, cap));
 }
 
 template <int KIND>
-void launch_stage(const nmhd::BatchGroup &p, bool persist, int ctas, cudaStream_t st, int in_sel, int out_sel,
-                  int half, int fin) {
-  const dim3 blk(nmhd::cell::BX, nmhd::cell::BY, nmhd::cell::BZ);
-  if (persist)
-    nmhd::k_batch_stage<KIND, true><<<std::min(ctas, p.total_tiles), blk, 0, st>>>(p, in_sel, out_sel, half, fin);
-  else
-    nmhd::k_batch_stage<KIND, false><<<p.total_tiles, blk, 0, st>>>(p, in_sel, out_sel, half, fin);
+void launch_stage(const nmhd::BatchGroup &p, bool persist, bool split, int ctas, cudaStream_t st, int in_sel,
+                  int out_sel, int half, int fin) {
+  const dim3 blk(nmhd::cell::kThreads);
+  auto go = [&](auto kernel, int tb, int te) {
+    if (te > tb) kernel<<<persist ? std::min(ctas, te - tb) : te - tb, blk, 0, st>>>(p, tb, te, in_sel, out_sel, half, fin);
+  };
+  if (!split) {  // one launch, every box through the general tile form
+    if (persist) go(nmhd::k_batch_stage<KIND, true, false>, 0, p.total_tiles);
+    else go(nmhd::k_batch_stage<KIND, false, false>, 0, p.total_tiles);
+  } else if (persist) {
+    go(nmhd::k_batch_stage<KIND, true, true>, 0, p.fixed_tiles);
+    go(nmhd::k_batch_stage<KIND, true, false>, p.fixed_tiles, p.total_tiles);
+  } else {
+    go(nmhd::k_batch_stage<KIND, false, true>, 0, p.fixed_tiles);
+    go(nmhd::k_batch_stage<KIND, false, false>, p.fixed_tiles, p.total_tiles);
+  }
 }
 
 // Kernel `kind` of one stage over every group.
 void launch_kind(nmhd_batch *b, int kind, int in_sel, int out_sel, int half, int fin) {
   for (const BatchGroup &p : b->groups) {
-    if (kind == 0) launch_stage<0>(p, b->persist[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
-    else if (kind == 1) launch_stage<1>(p, b->persist[1], b->ctas[1], b->stream, in_sel, out_sel, half, fin);
-    else launch_stage<2>(p, b->persist[2], b->ctas[2], b->stream, in_sel, out_sel, half, fin);
+    if (kind == 0) launch_stage<0>(p, b->persist[0], b->split[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
+    else if (kind == 1) launch_stage<1>(p, b->persist[1], b->split[1], b->ctas[1], b->stream, in_sel, out_sel, half, fin);
+    else launch_stage<2>(p, b->persist[2], b->split[2], b->ctas[2], b->stream, in_sel, out_sel, half, fin);
   }
 }
 
@@ -370,9 +412,10 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
     d.flux = base + 24 * stride;
     d.dt_hist = b->hist + (size_t)nmhd::kDtHistCap * i;
     d.ctl = b->ctls + i;
-    d.tiles_x = (d.g.sx + nmhd::cell::BX - 1) / nmhd::cell::BX;
-    d.tiles_y = (d.g.sy + nmhd::cell::BY - 1) / nmhd::cell::BY;
-    d.tiles_z = (d.g.sz + nmhd::cell::BZ - 1) / nmhd::cell::BZ;
+    pick_tile(d.g, d.lx, d.ly, d.lz);
+    d.tiles_x = (d.g.sx + (1 << d.lx) - 1) >> d.lx;
+    d.tiles_y = (d.g.sy + (1 << d.ly) - 1) >> d.ly;
+    d.tiles_z = (d.g.sz + (1 << d.lz) - 1) >> d.lz;
     d.tile_begin = b->total_tiles;
     d.fill_begin = b->total_fill;
     d.mcfl_begin = b->total_mcfl;
@@ -390,21 +433,29 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
   int occ[3] = {1, 1, 1};
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0, true>, nmhd::cell::kThreads, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1, true>, nmhd::cell::kThreads, 0);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2, true>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0, true, false>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1, true, false>, nmhd::cell::kThreads, 0);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2, true, false>, nmhd::cell::kThreads, 0);
   for (int k = 0; k < 3; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
-  // launch groups: consecutive boxes, tiles numbered from 0 within a group
+  // launch groups: consecutive boxes, tiles numbered from 0 within a group,
+  // the boxes with 32 x 4 x 2 tiles first
   for (int i0 = 0; i0 < n; i0 += nmhd::kGroupBoxes) {
     BatchGroup p;
     std::memset(&p, 0, sizeof p);
     p.nb = std::min(nmhd::kGroupBoxes, n - i0);
+    std::vector<int> order;
+    for (int pass = 0; pass < 2; ++pass)
+      for (int j = 0; j < p.nb; ++j) {
+        const BoxDesc &d = b->boxes[i0 + j];
+        if ((d.lx == 5 && d.ly == 2 && d.lz == 1) == (pass == 0)) order.push_back(i0 + j);
+      }
     for (int j = 0; j < p.nb; ++j) {
-      BoxDesc d = b->boxes[i0 + j];
+      BoxDesc d = b->boxes[order[j]];
       d.tile_begin = p.total_tiles;
       p.box[j] = d;
       p.tile_begin[j] = p.total_tiles;
       p.total_tiles += d.tiles_x * d.tiles_y * d.tiles_z;
+      if (d.lx == 5 && d.ly == 2 && d.lz == 1) p.fixed_tiles = p.total_tiles;
     }
     p.tile_begin[p.nb] = p.total_tiles;
     b->groups.push_back(p);
@@ -556,11 +607,21 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
   return result;
 }
 
-nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent) {
-  if (!b || kernel < 0 || kernel > 2 || (persistent != 0 && persistent != 1))
-    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..2 and persistent 0 or 1");
+nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int *tile_y, int *tile_z) {
+  if (!b || box < 0 || box >= b->n) return NMHD_ERR_INVALID_ARGUMENT;
+  const BoxDesc &d = b->boxes[box];
+  if (tile_x) *tile_x = 1 << d.lx;
+  if (tile_y) *tile_y = 1 << d.ly;
+  if (tile_z) *tile_z = 1 << d.lz;
+  return NMHD_OK;
+}
+
+nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split) {
+  if (!b || kernel < 0 || kernel > 2 || (persistent != 0 && persistent != 1) || (split != 0 && split != 1))
+    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..2, persistent and split 0 or 1");
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
   b->persist[kernel] = persistent != 0;
+  b->split[kernel] = split != 0;
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
   return NMHD_OK;
@@ -594,6 +655,7 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
   // The first stage's kernels (state -> fluxes -> predictor) leave the state
   // and the clocks alone, so each can be launched again and again on it.
   const bool saved[3] = {b->persist[0], b->persist[1], b->persist[2]};
+  const bool saved_split[3] = {b->split[0], b->split[1], b->split[2]};
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -601,9 +663,11 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
   int written = 0;
   for (int kind = 0; kind < 3 && e == cudaSuccess; ++kind) {
     double best = 1e30;
-    bool choice = saved[kind];
-    for (int persist = 0; persist < 2 && e == cudaSuccess; ++persist) {
+    bool choice = saved[kind], choice_split = saved_split[kind];
+    for (int trial = 0; trial < 4 && e == cudaSuccess; ++trial) {
+      const int persist = trial & 1, split = trial >> 1;
       b->persist[kind] = persist != 0;
+      b->split[kind] = split != 0;
       launch_kind(b, kind, 0, 2, 1, 0);  // warm-up
       e = cudaEventRecord(e0, b->stream);
       for (int r = 0; r < reps && e == cudaSuccess; ++r) launch_kind(b, kind, 0, 2, 1, 0);
@@ -614,23 +678,26 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
       if (e != cudaSuccess) break;
       const double per = ms / reps;
       if (trials_out && written < max_trials) {
-        trials_out[3 * written + 0] = kind;
-        trials_out[3 * written + 1] = persist;
-        trials_out[3 * written + 2] = per;
+        trials_out[4 * written + 0] = kind;
+        trials_out[4 * written + 1] = persist;
+        trials_out[4 * written + 2] = split;
+        trials_out[4 * written + 3] = per;
         ++written;
       }
       if (per < best) {
         best = per;
         choice = persist != 0;
+        choice_split = split != 0;
       }
     }
     b->persist[kind] = choice;
+    b->split[kind] = choice_split;
   }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
-    for (int k = 0; k < 3; ++k) b->persist[k] = saved[k];
+    for (int k = 0; k < 3; ++k) b->persist[k] = saved[k], b->split[k] = saved_split[k];
     return bfail(b, NMHD_ERR_CUDA, std::string("nmhd_batch_autotune: ") + cudaGetErrorString(e));
   }
   // the graphs hold the previous schedules

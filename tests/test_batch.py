@@ -40,13 +40,15 @@ def test_batch_rejects_unsupported_configs_on_cpu():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("schedule", ["per_tile", "persistent", "mixed"])
+@pytest.mark.parametrize("schedule", ["per_tile", "persistent", "mixed", "unsplit", "unsplit_persistent"])
 def test_batch_boxes_equal_single_box_runs(gpu, schedule):
     """Every box of a batch equals its single-box run, in each schedule of the
     stage kernels (persistent tile ranges or one tile per CTA)."""
     from nmhd_b200.batch import BatchSolver
     from nmhd_b200.solver import MHDSolver
-    persist = {"per_tile": (0, 0, 0), "persistent": (1, 1, 1), "mixed": (1, 0, 1)}[schedule]
+    persist = {"per_tile": (0, 0, 0), "persistent": (1, 1, 1), "mixed": (1, 0, 1), "unsplit": (0, 0, 0),
+               "unsplit_persistent": (1, 1, 1)}[schedule]
+    split = not schedule.startswith("unsplit")
     boxes, _ = small_ensemble()
     # add two non-shearing boxes of other shapes (power-of-two and not)
     boxes.append(orszag_tang_3d(16))
@@ -56,8 +58,11 @@ def test_batch_boxes_equal_single_box_runs(gpu, schedule):
     boxes.append(shearing_box(n_radial=24, n_azimuthal=128, n_vertical=8, l_azimuthal=4.0, seed=5))
     steps = 9
     with BatchSolver([c for c, _ in boxes]) as batch:
+        # the boxes' tile shapes (fewest padded cells) include narrow ones
+        shapes = {batch.tile_shape(i) for i in range(len(boxes))}
+        assert all(x * y * z == 256 and x >= 8 for x, y, z in shapes) and len(shapes) >= 3, shapes
         for k, p in enumerate(persist):
-            batch.set_schedule(k, p)
+            batch.set_schedule(k, p, split)
         for i, (c, s) in enumerate(boxes):
             batch.set_state(i, s)
         batch.step(4)
@@ -126,8 +131,9 @@ def test_batch_autotune_keeps_states_clocks_and_results(gpu):
         batch.step(3)
         before = [(batch.clock(i), batch.get_state(i)) for i in range(len(boxes))]
         trials = batch.autotune(reps=2)
-        assert sorted((k, p) for k, p, _ in trials) == [(k, p) for k in range(3) for p in (False, True)]
-        assert all(ms > 0 for _, _, ms in trials)
+        assert sorted((k, p, s) for k, p, s, _ in trials) == [(k, p, s) for k in range(3) for p in (False, True)
+                                                              for s in (False, True)]
+        assert all(ms > 0 for _, _, _, ms in trials)
         for i, (clk, st) in enumerate(before):
             assert batch.clock(i) == clk and np.array_equal(batch.get_state(i), st)
         batch.step(4)
@@ -140,5 +146,5 @@ def test_batch_autotune_keeps_states_clocks_and_results(gpu):
 
 def test_batch_schedule_arguments_are_checked_on_cpu():
     L = _lib.lib()
-    assert L.nmhd_batch_set_schedule(None, 0, 0) == -1
+    assert L.nmhd_batch_set_schedule(None, 0, 0, 1) == -1
     assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
