@@ -56,6 +56,8 @@ def test_batch_boxes_equal_single_box_runs(gpu, schedule):
     # and a box with interior tiles (cells and their +-1 neighbours away from
     # every edge), which the CT kernel addresses without the periodic wrap
     boxes.append(shearing_box(n_radial=24, n_azimuthal=128, n_vertical=8, l_azimuthal=4.0, seed=5))
+    # and a single-plane box (its tile is one plane deep)
+    boxes.append(orszag_tang_3d(40, ny=24, nz=1))
     steps = 9
     with BatchSolver([c for c, _ in boxes]) as batch:
         # the boxes' tile shapes (fewest padded cells) include narrow ones
