@@ -1,8 +1,9 @@
 /* Oracle: CPU restatement of the reference ideal-MHD time step.
  *
  * TEST INFRASTRUCTURE ONLY.  Only tests/, __graft_entry__.smoke() and the
- * CPU-baseline leg of bench.py may load this library, and only as the checker
- * or the timed CPU baseline; the product (libnmhd.so) never calls it.
+ * CPU-baseline leg of bench.py may load this library, and only as the
+ * correctness reference or the timed CPU baseline; the product (libnmhd.so)
+ * never calls it.
  *
  * It restates, in plain C, the reference's MHDSolver::proceed
  * (src/library/mhd_solver.inlrb:850-993, generated src/library/mhd_solver.inl)

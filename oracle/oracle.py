@@ -4,8 +4,8 @@ Loads ``oracle/liboracle.so`` (this repository's C restatement of the
 reference time step, mhd_oracle.c) and runs the host-compiled reference
 binaries in ``oracle/_ref`` (built by ``make -C oracle ref`` where the
 reference sources are present).  Only tests/, ``__graft_entry__.smoke()`` and
-bench.py's CPU-baseline leg use this module, as the checker or the timed CPU
-baseline.
+bench.py's CPU-baseline leg use this module, as the correctness reference or
+the timed CPU baseline.
 """
 from __future__ import annotations
 
