@@ -121,13 +121,11 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
       // address the neighbours without the periodic wrap
       const bool inner = NMHD_BATCH_CT_INNER && bx0 >= 1 && bx0 + (1 << lx) < g.sx && by0 >= 1 &&
                          by0 + (1 << ly) < g.sy && bz0 >= 1 && bz0 + (1 << lz) < g.sz;
-      if (g.pow2_spacing) {
-        if (inner) ct_core<true>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
-        else ct_core<true>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
-      } else {
-        if (inner) ct_core<false>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
-        else ct_core<false>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
-      }
+      // always the division form: with power-of-two spacings x / d equals
+      // the product form x * (1 / d) bitwise, and one form instead of two
+      // keeps the kernel within 64 registers
+      if (inner) ct_core<false>(g, ct_interior(g, win, d.flux, o), wb, wo, o, dt);
+      else ct_core<false>(g, ct_global_lean(g, win, d.flux, x, y, z), wb, wo, o, dt);
     }
   } else {
     float tcfl = __uint_as_float(0x7f800000u);
@@ -142,13 +140,13 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
   }
 }
 
-// One stage kernel over the tiles of a group, in one of two schedules picked
-// per kernel by nmhd_batch_autotune.  kPersist: a grid of as many CTAs as are
-// resident at once, each walking a contiguous range of tiles; otherwise one
-// tile per CTA (the default: measured faster for every kernel on the 64-box
-// and 512-box ensembles, since the hardware scheduler then balances uneven
+// One stage kernel over tiles [tb, te) of a group, in the schedule that
+// nmhd_batch_autotune picks per kernel.  kPersist: a grid of as many CTAs as
+// are resident at once, each walking a contiguous range of tiles; otherwise
+// one tile per CTA (the default; the hardware scheduler then balances uneven
 // tiles across the SMs).  Resident CTAs per SM asked of the compiler:
-// NMHD_BATCH_MIN_BLOCKS_<kind>: 4, 3 (4 spills ~100 bytes), 4.
+// NMHD_BATCH_MIN_BLOCKS_<kind>: 4, 3 (4 spills ~100 bytes; the fixed-shape
+// form runs 4 with 40 bytes of spill, as the single-box CT kernel), 4.
 #ifndef NMHD_BATCH_MIN_BLOCKS_0
 #define NMHD_BATCH_MIN_BLOCKS_0 4
 #endif
@@ -159,8 +157,9 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
 #define NMHD_BATCH_MIN_BLOCKS_2 4
 #endif
 template <int KIND, bool kPersist, bool kFixed>
-__global__ void __launch_bounds__(kThreads, KIND == 0 ? NMHD_BATCH_MIN_BLOCKS_0
-                                                      : (KIND == 1 ? NMHD_BATCH_MIN_BLOCKS_1 : NMHD_BATCH_MIN_BLOCKS_2))
+__global__ void __launch_bounds__(kThreads, KIND == 0   ? NMHD_BATCH_MIN_BLOCKS_0
+                                            : KIND == 1 ? (kFixed ? NMHD_BATCH_MIN_BLOCKS_1 + 1 : NMHD_BATCH_MIN_BLOCKS_1)
+                                                        : NMHD_BATCH_MIN_BLOCKS_2)
     k_batch_stage(const __grid_constant__ BatchGroup p, int tb, int te, int in_sel, int out_sel, int half,
                   int final_stage) {
   __shared__ float red[kThreads / 32];
