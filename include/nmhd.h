@@ -245,6 +245,8 @@ nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *gene
  * (semantics of nmhd_proceed, per box; a box that reached the goal waits).
  * *steps_done: steps taken by the box that took most. */
 nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
+/* Stream of the batch's work, as nmhd_set_stream (NULL: a stream of its own). */
+nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream);
 /* Tile of box `box` in the batched kernels: tile_x x tile_y x tile_z cells (256
  * threads), chosen per box to launch the fewest padded cells, at least 8 wide
  * in x; ties keep 32 x 4 x 2. */

@@ -86,6 +86,11 @@ class BatchSolver:
         self.proceed(math.inf, nsteps)
         return self.last_steps
 
+    def set_stream(self, cuda_stream):
+        """Run the batch's work on ``cuda_stream`` (a cudaStream_t as int, e.g.
+        torch.cuda.Stream().cuda_stream); None: a stream of its own."""
+        self._check(self._L.nmhd_batch_set_stream(self._h, ctypes.c_void_p(cuda_stream or None)))
+
     def tile_shape(self, i):
         """Tile of box i in the batched kernels: (x, y, z) cells."""
         v = [ctypes.c_int() for _ in range(3)]

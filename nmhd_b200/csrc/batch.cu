@@ -253,6 +253,7 @@ struct nmhd_batch {
   int ctas[3] = {0, 0, 0};                  // resident CTAs of each persistent stage kernel
   int device = 0;
   cudaStream_t stream = nullptr;
+  bool own_stream = true;
   bool cfl_ready = false;
   std::map<int, cudaGraphExec_t> graphs;
   std::string err;
@@ -478,7 +479,7 @@ void nmhd_batch_destroy(nmhd_batch *b) {
   cudaFree(b->hist);
   cudaFree(b->ctls);
   cudaFree(b->d_boxes);
-  if (b->stream) cudaStreamDestroy(b->stream);
+  if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
 }
 
@@ -604,6 +605,19 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
     *steps_done = gen1 - gen0;
   }
   return result;
+}
+
+nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream) {
+  if (!b) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "NULL batch");
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
+  for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
+  b->graphs.clear();
+  if (b->own_stream) cudaStreamDestroy(b->stream);
+  b->stream = nullptr;
+  b->own_stream = cuda_stream == nullptr;
+  if (b->own_stream) BATCH_CUDA(b, cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+  else b->stream = (cudaStream_t)cuda_stream;
+  return NMHD_OK;
 }
 
 nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int *tile_y, int *tile_z) {

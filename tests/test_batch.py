@@ -80,10 +80,14 @@ def test_batch_boxes_equal_single_box_runs(gpu, schedule):
 
 @pytest.mark.gpu
 def test_batch_goal_time_per_box(gpu):
+    """Per-box goal times, with the batch on a caller's stream."""
+    import torch
     from nmhd_b200.batch import BatchSolver
     from nmhd_b200.solver import MHDSolver
     boxes, _ = small_ensemble(n=4, seed=8)
+    stream = torch.cuda.Stream(device=gpu)
     with BatchSolver([c for c, _ in boxes]) as batch:
+        batch.set_stream(stream.cuda_stream)
         for i, (c, s) in enumerate(boxes):
             batch.set_state(i, s)
         assert batch.proceed(0.05)
@@ -150,3 +154,4 @@ def test_batch_schedule_arguments_are_checked_on_cpu():
     L = _lib.lib()
     assert L.nmhd_batch_set_schedule(None, 0, 0, 1) == -1
     assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
+    assert L.nmhd_batch_set_stream(None, None) == -1
