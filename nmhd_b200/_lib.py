@@ -85,6 +85,8 @@ _SIGS = [
                                           ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_set_schedule", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nmhd_batch_set_stream", ctypes.c_int, [_P, _P]),
+    ("nmhd_batch_tile_rule", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                            ctypes.POINTER(ctypes.c_int)]),
     ("nmhd_batch_tile_shape", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int),
                                              ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int)]),
     ("nmhd_batch_autotune", ctypes.c_int, [_P, ctypes.c_int, _P, ctypes.c_int]),

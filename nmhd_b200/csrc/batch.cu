@@ -607,6 +607,16 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
   return result;
 }
 
+nmhd_status nmhd_batch_tile_rule(const nmhd_config *box, int *tile_x, int *tile_y, int *tile_z) {
+  if (!box || box->size_x < 1 || box->size_y < 1 || box->size_z < 1) return NMHD_ERR_INVALID_ARGUMENT;
+  int lx, ly, lz;
+  pick_tile(nmhd::derive_grid(*box), lx, ly, lz);
+  if (tile_x) *tile_x = 1 << lx;
+  if (tile_y) *tile_y = 1 << ly;
+  if (tile_z) *tile_z = 1 << lz;
+  return NMHD_OK;
+}
+
 nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream) {
   if (!b) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "NULL batch");
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));

@@ -155,3 +155,37 @@ def test_batch_schedule_arguments_are_checked_on_cpu():
     assert L.nmhd_batch_set_schedule(None, 0, 0, 1) == -1
     assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
     assert L.nmhd_batch_set_stream(None, None) == -1
+
+
+def test_batch_tile_rule_launches_the_fewest_padded_cells_on_cpu():
+    """nmhd_batch_tile_rule (the tile of a box in the batched kernels): 256
+    threads as 2^a x 2^b x 2^c cells with x at least 8 wide, the fewest padded
+    cells; among equals the widest x, then the shape nearest 32 x 4 x 2, then
+    the taller y.  Checked against a brute force over seeded box sizes."""
+    L = _lib.lib()
+    rng = np.random.default_rng(7)
+
+    def padded(n, e):
+        return -(-n // (1 << e)) << e
+
+    def brute(sx, sy, sz):
+        shapes = [(a, b, 8 - a - b) for a in (5, 4, 3) for b in range(0, 9 - a)]
+        key = lambda s: (padded(sx, s[0]) * padded(sy, s[1]) * padded(sz, s[2]), -s[0],
+                         abs(s[1] - 2) + abs(s[2] - 1), -s[1])
+        best = min(shapes, key=key)
+        if key(best) == key((5, 2, 1)):
+            best = (5, 2, 1)
+        return tuple(1 << e for e in best)
+
+    cfg, _ = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8)
+    sizes = [(16, 16, 16), (48, 24, 16), (40, 24, 1), (256, 136, 64), (1, 1, 1), (24, 20, 12)]
+    sizes += [tuple(int(v) for v in rng.integers(1, 200, size=3)) for _ in range(300)]
+    for sx, sy, sz in sizes:
+        c = SolverConfig(**{**cfg.__dict__, "size_x": sx, "size_y": sy, "size_z": sz, "margin_y": 0,
+                            "problem": "none"})
+        v = [ctypes.c_int() for _ in range(3)]
+        assert L.nmhd_batch_tile_rule(ctypes.byref(c.to_ctypes()), *[ctypes.byref(x) for x in v]) == 0
+        got = tuple(x.value for x in v)
+        assert got == brute(sx, sy, sz), (sx, sy, sz, got)
+        assert got[0] * got[1] * got[2] == 256 and got[0] >= 8
+    assert L.nmhd_batch_tile_rule(None, None, None, None) == -1
