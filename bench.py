@@ -448,6 +448,33 @@ def run_ensemble_arm(args):
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         ms = float(t.item())
     value = total_interior * args.steps / (ms * 1e-3) / 1e6
+    launches = batch.launches_per_step() * args.steps
+    # end to end through the public API: every box's state in from pinned host
+    # memory, the same steps, every box's state out to pinned host memory
+    pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory().numpy()
+    host_in = [pinned(s) for _, s in boxes]
+    host_out = [pinned(np.empty_like(s, dtype=np.float32)) for _, s in boxes]
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    e0.record(stream)
+    for i, h in enumerate(host_in):
+        batch.set_state(i, h)
+    batch.step(args.steps)
+    for i, h in enumerate(host_out):
+        batch.get_state(i, out=h)
+    e1.record(stream)
+    torch.cuda.synchronize(dev)
+    e2e_ms = e0.elapsed_time(e1)
+    if dist:
+        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_ms = float(t.item())
+    state_bytes = sum(h.nbytes for h in host_in)
+    e2e = {"value": total_interior * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
+           "note": "set_state of every box (pinned host) + proceed(K steps) + get_state of every box "
+                   "(pinned host), per step"}
     # plain: each box through its own single-box solver, one after another
     plain_steps = 0 if args.no_plain else max(3, args.steps // 4)
     solvers = []
@@ -489,6 +516,7 @@ def run_ensemble_arm(args):
             "plain_per_box": {"value": plain, "unit": "Mcell-updates/s", "steps": plain_steps,
                               "note": "same boxes, one single-box solver each, stepped one after another"},
             "batch_speedup": value / plain if plain else None,
+            "e2e": e2e, "gpu_launches": launches,
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

@@ -251,6 +251,8 @@ nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream);
  * threads), chosen per box to launch the fewest padded cells, at least 8 wide
  * in x; ties keep 32 x 4 x 2. */
 nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int *tile_y, int *tile_z);
+/* Kernel launches of one batched time step with the current schedules. */
+int nmhd_batch_launches_per_step(const nmhd_batch *b);
 /* The same rule for a box configuration, without a batch (host only). */
 nmhd_status nmhd_batch_tile_rule(const nmhd_config *box, int *tile_x, int *tile_y, int *tile_z);
 /* Schedule of stage kernel `kernel` (0 face fluxes, 1 constrained transport,

@@ -85,6 +85,7 @@ _SIGS = [
                                           ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_set_schedule", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nmhd_batch_set_stream", ctypes.c_int, [_P, _P]),
+    ("nmhd_batch_launches_per_step", ctypes.c_int, [_P]),
     ("nmhd_batch_tile_rule", ctypes.c_int, [_P, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                             ctypes.POINTER(ctypes.c_int)]),
     ("nmhd_batch_tile_shape", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_int),

@@ -64,8 +64,14 @@ class BatchSolver:
             raise ValueError(f"box {i}: state shape {st.shape} != {(8,) + self.configs[i].shape}")
         self._check(self._L.nmhd_batch_set_state(self._h, i, self._ptrs(i, st), 0))
 
-    def get_state(self, i):
-        out = np.empty((8,) + self.configs[i].shape, dtype=np.float32)
+    def get_state(self, i, out=None):
+        """State of box i (8 fields, .bin order); into ``out`` (a C-contiguous
+        float32 host array of that shape, e.g. pinned) when given."""
+        shape = (8,) + self.configs[i].shape
+        if out is None:
+            out = np.empty(shape, dtype=np.float32)
+        elif out.shape != shape or out.dtype != np.float32 or not out.flags.c_contiguous:
+            raise ValueError(f"box {i}: out must be a C-contiguous float32 array of shape {shape}")
         self._check(self._L.nmhd_batch_get_state(self._h, i, self._ptrs(i, out), 0))
         return out
 
@@ -90,6 +96,10 @@ class BatchSolver:
         """Run the batch's work on ``cuda_stream`` (a cudaStream_t as int, e.g.
         torch.cuda.Stream().cuda_stream); None: a stream of its own."""
         self._check(self._L.nmhd_batch_set_stream(self._h, ctypes.c_void_p(cuda_stream or None)))
+
+    def launches_per_step(self):
+        """Kernel launches of one batched step with the current schedules."""
+        return self._check(self._L.nmhd_batch_launches_per_step(self._h))
 
     def tile_shape(self, i):
         """Tile of box i in the batched kernels: (x, y, z) cells."""

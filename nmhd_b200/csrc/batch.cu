@@ -607,6 +607,15 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
   return result;
 }
 
+int nmhd_batch_launches_per_step(const nmhd_batch *b) {
+  if (!b) return NMHD_ERR_INVALID_ARGUMENT;
+  int n = (b->total_fill > 0) + (b->total_mcfl > 0);
+  for (int kind = 0; kind < 3; ++kind)
+    for (const BatchGroup &p : b->groups)
+      n += 2 * (b->split[kind] ? (p.fixed_tiles > 0) + (p.total_tiles > p.fixed_tiles) : 1);
+  return n;
+}
+
 nmhd_status nmhd_batch_tile_rule(const nmhd_config *box, int *tile_x, int *tile_y, int *tile_z) {
   if (!box || box->size_x < 1 || box->size_y < 1 || box->size_z < 1) return NMHD_ERR_INVALID_ARGUMENT;
   int lx, ly, lz;

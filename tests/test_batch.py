@@ -97,7 +97,9 @@ def test_batch_goal_time_per_box(gpu):
                 assert one.proceed(0.05)
                 t, g = batch.clock(i)
                 assert t == float(np.float32(0.05)) and g == one.generation()
-                assert np.array_equal(batch.get_state(i), one.get_state())
+                out = np.empty((8,) + c.shape, dtype=np.float32)
+                assert batch.get_state(i, out=out) is out
+                assert np.array_equal(out, one.get_state())
 
 
 @pytest.mark.gpu
@@ -155,6 +157,7 @@ def test_batch_schedule_arguments_are_checked_on_cpu():
     assert L.nmhd_batch_set_schedule(None, 0, 0, 1) == -1
     assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
     assert L.nmhd_batch_set_stream(None, None) == -1
+    assert L.nmhd_batch_launches_per_step(None) == -1
 
 
 def test_batch_tile_rule_launches_the_fewest_padded_cells_on_cpu():
