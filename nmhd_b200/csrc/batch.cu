@@ -87,10 +87,6 @@ __device__ __forceinline__ int group_box(const BatchGroup &p, int t) {
   return lo;
 }
 
-#ifndef NMHD_BATCH_CT_INNER
-#define NMHD_BATCH_CT_INNER 1
-#endif
-
 // One tile of one stage kernel: the box's 2^lx x 2^ly x 2^lz cells on the
 // CTA's 256 threads (a 1-D block).  KIND 0: face fluxes, 1: constrained
 // transport, 2: conserved update + primitive recovery (+ CFL and clock in the
@@ -119,7 +115,7 @@ __device__ __forceinline__ void batch_tile(const BoxDesc &d, int t, int in_sel, 
       const int o = (z * g.sy + y) * g.sx + x;
       // tiles whose cells and their +-1 neighbours all lie inside the box
       // address the neighbours without the periodic wrap
-      const bool inner = NMHD_BATCH_CT_INNER && bx0 >= 1 && bx0 + (1 << lx) < g.sx && by0 >= 1 &&
+      const bool inner = bx0 >= 1 && bx0 + (1 << lx) < g.sx && by0 >= 1 &&
                          by0 + (1 << ly) < g.sy && bz0 >= 1 && bz0 + (1 << lz) < g.sz;
       // always the division form: with power-of-two spacings x / d equals
       // the product form x * (1 / d) bitwise, and one form instead of two

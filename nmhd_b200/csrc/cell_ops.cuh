@@ -337,18 +337,6 @@ __device__ __forceinline__ void ct_core(const GridParams &g, const Src &S, const
   wo[7 * N + o] = wb[7 * N + o] + dt * pb;
 }
 
-// ct_core reading HBM directly (kLean: through CtGlobalLean).
-template <bool kPow2, bool kLean = false>
-__device__ __forceinline__ void ct_cell(const GridParams &g, const float *__restrict__ win,
-                                        const float *__restrict__ wb, float *__restrict__ wo,
-                                        const float *__restrict__ flux, int x, int y, int z, float dt) {
-  const int o = (z * g.sy + y) * g.sx + x;
-  if (kLean)
-    ct_core<kPow2>(g, ct_global_lean(g, win, flux, x, y, z), wb, wo, o, dt);
-  else
-    ct_core<kPow2>(g, ct_global(g, win, flux, x, y, z), wb, wo, o, dt);
-}
-
 // Rest of the stage for cell (x, y, z): flux divergence of rho, m, E
 // (mhd_solver.inlrb:689-693), conserved state before the stage (to_conserved
 // :762-777), update (add_pace/update :797-835), primitive recovery with the new
