@@ -458,11 +458,9 @@ def run_ensemble_arm(args):
     if dist:
         dist.barrier()
     e0.record(stream)
-    for i, h in enumerate(host_in):
-        batch.set_state(i, h)
+    batch.set_states(host_in)
     batch.step(args.steps)
-    for i, h in enumerate(host_out):
-        batch.get_state(i, out=h)
+    batch.get_states(out=host_out)
     e1.record(stream)
     torch.cuda.synchronize(dev)
     e2e_ms = e0.elapsed_time(e1)
@@ -473,8 +471,8 @@ def run_ensemble_arm(args):
     state_bytes = sum(h.nbytes for h in host_in)
     e2e = {"value": total_interior * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
            "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
-           "note": "set_state of every box (pinned host) + proceed(K steps) + get_state of every box "
-                   "(pinned host), per step"}
+           "note": "set_states (every box, pinned host) + proceed(K steps) + get_states (every box, "
+                   "pinned host), per step"}
     # plain: each box through its own single-box solver, one after another
     plain_steps = 0 if args.no_plain else max(3, args.steps // 4)
     solvers = []

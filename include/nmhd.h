@@ -239,6 +239,11 @@ int nmhd_batch_size(const nmhd_batch *b);
 /* State of box `box`, as nmhd_set_state/nmhd_get_state. */
 nmhd_status nmhd_batch_set_state(nmhd_batch *b, int box, const float *const fields[8], int on_device);
 nmhd_status nmhd_batch_get_state(nmhd_batch *b, int box, float *const fields[8], int on_device);
+/* Every box's state at once: fields holds 8 pointers per box, box after box
+ * (8 * nmhd_batch_size pointers); one round trip to the boxes' control blocks
+ * instead of one per box. */
+nmhd_status nmhd_batch_set_states(nmhd_batch *b, const float *const *fields, int on_device);
+nmhd_status nmhd_batch_get_states(nmhd_batch *b, float *const *fields, int on_device);
 /* Clock of box `box` (current_time, generation). */
 nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *generation);
 /* Advances every box until all reach goal_time or max_steps steps are done

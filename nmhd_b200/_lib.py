@@ -79,6 +79,8 @@ _SIGS = [
     ("nmhd_batch_size", ctypes.c_int, [_P]),
     ("nmhd_batch_set_state", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), ctypes.c_int]),
     ("nmhd_batch_get_state", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_batch_set_states", ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.c_int]),
+    ("nmhd_batch_get_states", ctypes.c_int, [_P, ctypes.POINTER(_P), ctypes.c_int]),
     ("nmhd_batch_clock", ctypes.c_int, [_P, ctypes.c_int, ctypes.POINTER(ctypes.c_double),
                                         ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64,

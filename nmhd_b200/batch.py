@@ -75,6 +75,30 @@ class BatchSolver:
         self._check(self._L.nmhd_batch_get_state(self._h, i, self._ptrs(i, out), 0))
         return out
 
+    def set_states(self, states):
+        """Every box's state at once (a sequence of arrays, box order)."""
+        if len(states) != len(self.configs):
+            raise ValueError(f"{len(states)} states for {len(self.configs)} boxes")
+        arrs = [np.ascontiguousarray(s, dtype=np.float32) for s in states]
+        for i, a in enumerate(arrs):
+            if a.shape != (8,) + self.configs[i].shape:
+                raise ValueError(f"box {i}: state shape {a.shape} != {(8,) + self.configs[i].shape}")
+        ptrs = (ctypes.c_void_p * (8 * len(arrs)))(*[p for i, a in enumerate(arrs) for p in self._ptrs(i, a)])
+        self._check(self._L.nmhd_batch_set_states(self._h, ptrs, 0))
+
+    def get_states(self, out=None):
+        """Every box's state at once, into ``out`` (C-contiguous float32 host
+        arrays, box order) when given."""
+        if out is None:
+            out = [np.empty((8,) + c.shape, dtype=np.float32) for c in self.configs]
+        for i, a in enumerate(out):
+            if a.shape != (8,) + self.configs[i].shape or a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError(f"box {i}: out must be a C-contiguous float32 array of shape "
+                                 f"{(8,) + self.configs[i].shape}")
+        ptrs = (ctypes.c_void_p * (8 * len(out)))(*[p for i, a in enumerate(out) for p in self._ptrs(i, a)])
+        self._check(self._L.nmhd_batch_get_states(self._h, ptrs, 0))
+        return out
+
     def clock(self, i):
         t = ctypes.c_double()
         g = ctypes.c_int64()

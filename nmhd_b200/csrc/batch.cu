@@ -481,41 +481,77 @@ void nmhd_batch_destroy(nmhd_batch *b) {
 
 int nmhd_batch_size(const nmhd_batch *b) { return b ? b->n : 0; }
 
-nmhd_status nmhd_batch_set_state(nmhd_batch *b, int box, const float *const fields[8], int on_device) {
-  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
-  std::vector<StepCtl> h;
-  nmhd_status st = read_ctls(b, h);
-  if (st != NMHD_OK) return st;
+}  // extern "C"
+
+namespace {
+
+// Copies of one box's 8 fields into (to_box) or out of its current buffer,
+// whose parity the control block h says.
+nmhd_status box_copy(nmhd_batch *b, const StepCtl &h, int box, float *const *fields, int on_device, bool to_box) {
   const BoxDesc &d = b->boxes[box];
-  float *cur = h[box].parity ? d.w1 : d.w0;
+  float *cur = h.parity ? d.w1 : d.w0;
   const size_t bytes = sizeof(float) * (size_t)d.g.n;
   for (int v = 0; v < 8; ++v) {
     if (!fields[v]) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
-    BATCH_CUDA(b, cudaMemcpyAsync(cur + (size_t)v * d.g.n, fields[v], bytes,
-                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, b->stream));
+    float *dev = cur + (size_t)v * d.g.n;
+    const cudaMemcpyKind kind = on_device ? cudaMemcpyDeviceToDevice
+                                          : (to_box ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost);
+    BATCH_CUDA(b, cudaMemcpyAsync(to_box ? dev : fields[v], to_box ? fields[v] : dev, bytes, kind, b->stream));
   }
-  h[box].status = 0;
-  h[box].done = 0;
-  h[box].cfl_cur = h[box].cfl_next = 0x7f800000u;
+  return NMHD_OK;
+}
+
+// States of boxes [b0, b1) in (fields box-major, 8 per box): one round trip
+// to the control blocks for all of them.
+nmhd_status set_states(nmhd_batch *b, int b0, int b1, const float *const *fields, int on_device) {
+  std::vector<StepCtl> h;
+  nmhd_status st = read_ctls(b, h);
+  if (st != NMHD_OK) return st;
+  for (int box = b0; box < b1; ++box) {
+    st = box_copy(b, h[box], box, const_cast<float *const *>(fields + 8 * (box - b0)), on_device, true);
+    if (st != NMHD_OK) return st;
+    h[box].status = 0;
+    h[box].done = 0;
+    h[box].cfl_cur = h[box].cfl_next = 0x7f800000u;
+  }
   b->cfl_ready = false;
   return write_ctls(b, h);
 }
 
-nmhd_status nmhd_batch_get_state(nmhd_batch *b, int box, float *const fields[8], int on_device) {
-  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+nmhd_status get_states(nmhd_batch *b, int b0, int b1, float *const *fields, int on_device) {
   std::vector<StepCtl> h;
   nmhd_status st = read_ctls(b, h);
   if (st != NMHD_OK) return st;
-  const BoxDesc &d = b->boxes[box];
-  const float *cur = h[box].parity ? d.w1 : d.w0;
-  const size_t bytes = sizeof(float) * (size_t)d.g.n;
-  for (int v = 0; v < 8; ++v) {
-    if (!fields[v]) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "field pointer is NULL");
-    BATCH_CUDA(b, cudaMemcpyAsync(fields[v], cur + (size_t)v * d.g.n, bytes,
-                                  on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, b->stream));
+  for (int box = b0; box < b1; ++box) {
+    st = box_copy(b, h[box], box, fields + 8 * (box - b0), on_device, false);
+    if (st != NMHD_OK) return st;
   }
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
   return NMHD_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+nmhd_status nmhd_batch_set_state(nmhd_batch *b, int box, const float *const fields[8], int on_device) {
+  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  return set_states(b, box, box + 1, fields, on_device);
+}
+
+nmhd_status nmhd_batch_get_state(nmhd_batch *b, int box, float *const fields[8], int on_device) {
+  if (!b || !fields || box < 0 || box >= b->n) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  return get_states(b, box, box + 1, fields, on_device);
+}
+
+nmhd_status nmhd_batch_set_states(nmhd_batch *b, const float *const *fields, int on_device) {
+  if (!b || !fields) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  return set_states(b, 0, b->n, fields, on_device);
+}
+
+nmhd_status nmhd_batch_get_states(nmhd_batch *b, float *const *fields, int on_device) {
+  if (!b || !fields) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "bad argument");
+  return get_states(b, 0, b->n, fields, on_device);
 }
 
 nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *generation) {

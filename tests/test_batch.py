@@ -88,8 +88,7 @@ def test_batch_goal_time_per_box(gpu):
     stream = torch.cuda.Stream(device=gpu)
     with BatchSolver([c for c, _ in boxes]) as batch:
         batch.set_stream(stream.cuda_stream)
-        for i, (c, s) in enumerate(boxes):
-            batch.set_state(i, s)
+        batch.set_states([s for _, s in boxes])  # all boxes in one call
         assert batch.proceed(0.05)
         for i, (c, s) in enumerate(boxes):
             with MHDSolver(c) as one:
@@ -100,6 +99,7 @@ def test_batch_goal_time_per_box(gpu):
                 out = np.empty((8,) + c.shape, dtype=np.float32)
                 assert batch.get_state(i, out=out) is out
                 assert np.array_equal(out, one.get_state())
+                assert np.array_equal(batch.get_states()[i], out)
 
 
 @pytest.mark.gpu
@@ -158,6 +158,7 @@ def test_batch_schedule_arguments_are_checked_on_cpu():
     assert L.nmhd_batch_autotune(None, 3, None, 0) == -1
     assert L.nmhd_batch_set_stream(None, None) == -1
     assert L.nmhd_batch_launches_per_step(None) == -1
+    assert L.nmhd_batch_set_states(None, None, 0) == -1 and L.nmhd_batch_get_states(None, None, 0) == -1
 
 
 def test_batch_tile_rule_launches_the_fewest_padded_cells_on_cpu():
