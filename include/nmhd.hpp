@@ -317,6 +317,24 @@ class Batch {
     check(nmhd_batch_get_state(b_, box, f, 0));
     return all;
   }
+  // Every box's state at once (one host round trip to the control blocks).
+  void initialize_states(const std::vector<std::vector<float>> &all) {
+    if ((int)all.size() != size()) throw Error(NMHD_ERR_INVALID_ARGUMENT, "one state per box expected");
+    std::vector<const float *> f(8 * all.size());
+    for (size_t i = 0; i < all.size(); ++i)
+      for (int v = 0; v < 8; ++v) f[8 * i + v] = all[i].data() + v * cells((int)i);
+    check(nmhd_batch_set_states(b_, f.data(), 0));
+  }
+  std::vector<std::vector<float>> states() {
+    std::vector<std::vector<float>> all(size());
+    std::vector<float *> f(8 * all.size());
+    for (size_t i = 0; i < all.size(); ++i) {
+      all[i].resize(8 * cells((int)i));
+      for (int v = 0; v < 8; ++v) f[8 * i + v] = all[i].data() + v * cells((int)i);
+    }
+    check(nmhd_batch_get_states(b_, f.data(), 0));
+    return all;
+  }
   // Every box until goal_time (or max_steps steps): true when all reached it.
   bool proceed(float goal_time, long long max_steps = 0) {
     int64_t done = 0;

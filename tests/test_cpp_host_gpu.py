@@ -90,8 +90,10 @@ int main(int argc, char **argv) {
   }
   batch.autotune(2);
   const bool reached = batch.proceed(1e30f, 7);
+  const std::vector<std::vector<float>> all = batch.states();
   for (int i = 0; i < 2; ++i) {
     const std::vector<float> s = batch.state(i);
+    if (s != all[i]) return 5;
     FILE *fp = std::fopen(argv[1 + i], "wb");
     if (!fp || std::fwrite(s.data(), 4, s.size(), fp) != s.size()) return 4;
     std::fclose(fp);
