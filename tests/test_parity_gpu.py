@@ -385,3 +385,38 @@ def test_profile_counts_kernel_launches(gpu, variant, zc, mz, expect):
         assert all(ms >= 0 for ms, _ in prof.values())
         assert sol.generation() == 3
         assert_same(sol.get_state(), o["state"])
+
+
+def test_full_size_runs_keep_the_conservation_properties(gpu):
+    """Size-independent properties at the benchmarks' full sizes, where the
+    oracle would take too long: the 256^3 Orszag-Tang box (fully periodic, no
+    source) conserves mass, momentum and total energy to roundoff over 100
+    steps (the scheme updates them in flux form) with div B at roundoff; the
+    128 x 256 x 64 MRI box runs the benchmark's 1000 steps with div B at
+    roundoff and a valid state."""
+    cfg, s = orszag_tang_3d(256)
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        del s
+        d0 = sol.diagnostics()
+        sol.step(100)
+        assert sol.generation() == 100
+        d1 = sol.diagnostics()
+    b0 = 1.0 / math.sqrt(4.0 * math.pi)
+    assert abs(d1["mass"] - d0["mass"]) < 1e-5 * d0["mass"]
+    assert abs(d1["total_energy"] - d0["total_energy"]) < 1e-5 * d0["total_energy"]
+    for a, b in zip(d0["momentum"], d1["momentum"]):
+        assert abs(b - a) < 1e-5 * d0["mass"]
+    assert d1["max_div_b"] < 1e-4 * b0 * 256
+
+    cfg, s = shearing_box()
+    with MHDSolver(cfg) as sol:
+        sol.set_state(s)
+        d0 = sol.diagnostics()
+        sol.step(1000)
+        assert sol.generation() == 1000
+        st = sol.get_state()
+        d1 = sol.diagnostics()
+    assert np.isfinite(st).all() and (st[0] > 0).all() and (st[4] > 0).all()
+    assert d1["max_div_b"] < 1e-4 * math.sqrt(2 / 400) * 128
+    assert abs(d1["mass"] - d0["mass"]) < 1e-6 * d0["mass"]
