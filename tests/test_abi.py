@@ -108,3 +108,37 @@ def test_cpp_mirror_compiles_and_links(tmp_path):
     lib = os.path.join(root, "nmhd_b200")
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(root, "include"), str(src),
                     "-L" + lib, "-lnmhd", "-Wl,-rpath," + lib, "-o", str(tmp_path / "m")], check=True)
+
+
+@pytest.mark.parametrize("change,code,text", [
+    (dict(size_y=0), -1, b"sizes"),
+    (dict(size_x=2048, size_y=1024, size_z=1024), -1, b"too large"),
+    (dict(margin_y=-1), -1, b"margins"),
+    (dict(size_y=10, margin_y=4), -1, b"interior Y rows"),
+    (dict(size_z=5, margin_z=2), -1, b"interior Z planes"),
+    (dict(extent_y=0.0), -1, b"extents"),
+    (dict(gamma=1.0), -1, b"gamma"),
+    (dict(cfl=0.0), -1, b"cfl"),
+    (dict(raw_problem=7), -1, b"unknown problem"),
+    (dict(space_order=3), -1, b"space_order"),
+    (dict(time_order=0), -1, b"time_order"),
+    (dict(parallel_size_y=-1), -1, b"parallel_size_y"),
+    (dict(flags=4), -1, b"unknown flags"),
+    (dict(flags=1, parallel_size_y=2), -7, b"whole boxes"),
+    (dict(parallel_size_y=2, margin_y=0, size_y=16), -1, b"margin_y >= 1"),
+])
+def test_create_validates_every_config_rule_on_cpu(change, code, text):
+    """nmhd_create refuses each invalid configuration with its status and a
+    message before any device work (the reference's compile-time config has
+    no such checks; these are the runtime config's rules)."""
+    L = _lib.lib()
+    base = dict(size_x=16, size_y=16 + 8, size_z=8, margin_y=4, extent_x=2.0)
+    change = dict(change)
+    raw = change.pop("raw_problem", None)
+    c = SolverConfig(**{**base, **change}).to_ctypes()
+    if raw is not None:
+        c.problem = raw
+    h = ctypes.c_void_p()
+    assert L.nmhd_create(ctypes.byref(c), ctypes.byref(h)) == code
+    assert text in L.nmhd_last_error(None), L.nmhd_last_error(None)
+    assert not h.value
