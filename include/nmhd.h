@@ -229,9 +229,8 @@ const char *nmhd_noalloc_last_error(void);
  * over all boxes (per group of 128 boxes, whose descriptors travel in the
  * launch's parameter block), either persistent (a resident grid walking tile
  * ranges) or one tile per CTA, as nmhd_batch_autotune picks; each box has its
- * own tile shape (nmhd_batch_tile_shape);
- * batches of steps are one CUDA graph.  Batched boxes use time_order 2 and no
- * Z margins. */
+ * own tile shape (nmhd_batch_tile_shape); batches of steps are one CUDA graph.
+ * Batched boxes use time_order 2 and no Z margins. */
 typedef struct nmhd_batch nmhd_batch;
 nmhd_status nmhd_batch_create(const nmhd_config *boxes, int n, nmhd_batch **out);
 void nmhd_batch_destroy(nmhd_batch *b);
@@ -256,10 +255,10 @@ nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream);
  * threads), chosen per box to launch the fewest padded cells, at least 8 wide
  * in x; ties keep 32 x 4 x 2. */
 nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int *tile_y, int *tile_z);
-/* Kernel launches of one batched time step with the current schedules. */
-int nmhd_batch_launches_per_step(const nmhd_batch *b);
 /* The same rule for a box configuration, without a batch (host only). */
 nmhd_status nmhd_batch_tile_rule(const nmhd_config *box, int *tile_x, int *tile_y, int *tile_z);
+/* Kernel launches of one batched time step with the current schedules. */
+int nmhd_batch_launches_per_step(const nmhd_batch *b);
 /* Schedule of stage kernel `kernel` (0 face fluxes, 1 constrained transport,
  * 2 conserved update): persistent = 1 for the resident grid walking tile
  * ranges, 0 for one tile per CTA (the default); split = 1 (the default) runs
