@@ -195,14 +195,16 @@ const char *nmhd_kernel_name(int i);
 
 /* Allocation-free time stepping.  No counterpart in the reference (whose
  * MHDSolver owns Thrust vectors, src/library/mhd_solver.hrb:150-184).  For
- * callers that cannot allocate device memory: code running inside someone
- * else's CUDA-graph capture, hosts whose allocator owns all device memory, or
- * real-time loops where an allocation and its implicit synchronisation are not
- * allowed.  Advances a caller-owned box by up to nsteps steps (stopping at
- * goal_time, rounded to float) with the same kernels and bitwise the same
- * result as nmhd_proceed, keeping every intermediate in one static device
- * array of this library sized for NMHD_NOALLOC_MAX_CELLS cells (about 28 MB,
- * held by every GPU that loads the library until the process exits).
+ * callers that cannot allocate device memory: a host framework whose caching
+ * allocator has reserved the device's memory, or a real-time loop where a
+ * device allocation and the synchronisation it can bring are not allowed.
+ * Advances a caller-owned box by up to nsteps steps (stopping at goal_time,
+ * rounded to float) with the tiled kernels (kernel variant 0), which give
+ * bitwise the same result as nmhd_proceed, keeping every intermediate in one
+ * static device array of this library sized for NMHD_NOALLOC_MAX_CELLS cells
+ * (about 28 MB, held by every GPU that loads the library until the process
+ * exits).
+ *   cfg        nmhd_create's rules, plus a whole box: parallel_size_y <= 1, flags 0
  *   state_in   device pointer, 8 x Sx*Sy*Sz floats (.bin field order); read only
  *   state_out  device pointer, same size, must not alias state_in; receives the result
  *   time, generation  in: the clock of state_in; out: the clock of the result
@@ -211,9 +213,12 @@ const char *nmhd_kernel_name(int i);
  * a device looks up the array's device address (set-up); make that first
  * call before any stream capture.  All calls share the array and it keeps the
  * last call's contents: calls that overlap on the GPU race.  Runs on
- * `cuda_stream` (NULL: the default stream) and returns when done.
- * Returns NMHD_GOAL_REACHED, NMHD_STEP_LIMIT or an error; nmhd_noalloc_last_error()
- * describes the last error. */
+ * `cuda_stream` (NULL: the default stream), reads the control block back
+ * every 16 steps (stopping once the goal is reached or the state is bad) and
+ * returns when done.  A CUDA error pending from earlier work is reported as
+ * NMHD_ERR_CUDA without launching anything.  Returns NMHD_GOAL_REACHED,
+ * NMHD_STEP_LIMIT or an error; nmhd_noalloc_last_error() describes the last
+ * error. */
 #define NMHD_NOALLOC_MAX_CELLS 262144
 nmhd_status nmhd_advance_noalloc(const nmhd_config *cfg, const float *state_in, float *state_out,
                                  double *time, int64_t *generation, double goal_time, int64_t nsteps,

@@ -370,10 +370,14 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
   for (int i = 0; i < n; ++i) {
     const nmhd_config &c = cfgs[i];
     const long long cells = (long long)c.size_x * c.size_y * c.size_z;
-    if (c.size_x < 1 || c.size_y < 1 || c.size_z < 1 || cells * 21 >= (1LL << 31) || c.margin_z != 0 ||
-        c.margin_y < 0 || c.size_y - 2 * c.margin_y < c.margin_y || !(c.gamma > 1.0f) || !(c.cfl > 0.0f) ||
-        (c.space_order != 1 && c.space_order != 2) || c.time_order != 2 || c.parallel_size_y > 1 || c.flags != 0 ||
-        (c.problem != NMHD_PROBLEM_NONE && c.problem != NMHD_PROBLEM_SHEARING_BOX)) {
+    std::string why;
+    const nmhd_status vs = nmhd::validate_config(&c, why);
+    if (vs != NMHD_OK) {
+      delete b;
+      return bfail(nullptr, vs, "box " + std::to_string(i) + ": " + why);
+    }
+    if (cells * 21 >= (1LL << 31) || c.margin_z != 0 || c.time_order != 2 || c.parallel_size_y > 1 ||
+        c.flags != 0) {
       delete b;
       return bfail(nullptr, NMHD_ERR_INVALID_ARGUMENT,
                    "box " + std::to_string(i) + ": invalid configuration (batched boxes are whole boxes with "

@@ -100,9 +100,7 @@ GridParams nmhd::derive_grid(const nmhd_config &c) {
   return g;
 }
 
-namespace {
-
-nmhd_status validate(const nmhd_config *c, std::string &why) {
+nmhd_status nmhd::validate_config(const nmhd_config *c, std::string &why) {
   if (!c) { why = "config is NULL"; return NMHD_ERR_INVALID_ARGUMENT; }
   if (c->size_x < 1 || c->size_y < 1 || c->size_z < 1) { why = "sizes must be >= 1"; return NMHD_ERR_INVALID_ARGUMENT; }
   const long long n = (long long)c->size_x * c->size_y * c->size_z;
@@ -131,6 +129,8 @@ nmhd_status validate(const nmhd_config *c, std::string &why) {
   }
   return NMHD_OK;
 }
+
+namespace {
 
 nmhd_status read_ctl(nmhd_solver *s, StepCtl &h) {
   NMHD_CUDA(s, cudaMemcpyAsync(&h, s->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
@@ -239,7 +239,7 @@ nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
   if (!out) return fail(nullptr, NMHD_ERR_INVALID_ARGUMENT, "out is NULL");
   *out = nullptr;
   std::string why;
-  nmhd_status st = validate(cfg, why);
+  nmhd_status st = nmhd::validate_config(cfg, why);
   if (st != NMHD_OK) return fail(nullptr, st, why);
   nmhd_solver *s = new nmhd_solver();
   s->cfg = *cfg;

@@ -3,6 +3,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <string>
+
 #include "../../include/nmhd.h"
 
 namespace nmhd {
@@ -50,6 +52,9 @@ enum : int { kStatusNumerical = 1, kStatusBadDt = 2 };
 
 // Box constants from a configuration, with the reference's float chains.
 GridParams derive_grid(const nmhd_config &c);
+// The runtime configuration's rules (nmhd_create's checks, shared by every
+// entry point that takes an nmhd_config): NMHD_OK, or a status and `why`.
+nmhd_status validate_config(const nmhd_config *c, std::string &why);
 constexpr int kDtHistCap = 4096;
 constexpr int kFluxFields = 21;  // 3 face directions x 7 flux components
 

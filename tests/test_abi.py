@@ -142,3 +142,40 @@ def test_create_validates_every_config_rule_on_cpu(change, code, text):
     assert L.nmhd_create(ctypes.byref(c), ctypes.byref(h)) == code
     assert text in L.nmhd_last_error(None), L.nmhd_last_error(None)
     assert not h.value
+
+
+@pytest.mark.parametrize("change,text", [
+    (dict(extent_x=0.0), b"extents"),
+    (dict(extent_z=-1.0), b"extents"),
+    (dict(parallel_size_y=-1), b"parallel_size_y"),
+    (dict(parallel_size_y=2), b"whole box"),
+    (dict(flags=1), b"whole box"),
+    (dict(gamma=0.5), b"gamma"),
+    (dict(size_x=65, size_y=72, size_z=64), b"at most 262144"),
+])
+def test_noalloc_validates_like_create_on_cpu(change, text):
+    """nmhd_advance_noalloc checks nmhd_create's configuration rules (the
+    same validator) plus its whole-box rules and size limit before any device
+    work; the state pointers are never dereferenced on this path."""
+    L = _lib.lib()
+    base = dict(size_x=16, size_y=16 + 8, size_z=8, margin_y=4, extent_x=2.0)
+    c = SolverConfig(**{**base, **change}).to_ctypes()
+    t, g, done = ctypes.c_double(0.0), ctypes.c_int64(0), ctypes.c_int64(0)
+    code = L.nmhd_advance_noalloc(ctypes.byref(c), ctypes.c_void_p(0x1000), ctypes.c_void_p(0x2000),
+                                  ctypes.byref(t), ctypes.byref(g), 1.0, 1, ctypes.byref(done), None)
+    assert code in (-1, -7)
+    assert text in L.nmhd_noalloc_last_error(), L.nmhd_noalloc_last_error()
+
+
+def test_batch_create_validates_like_create_on_cpu():
+    """nmhd_batch_create applies nmhd_create's rules to every box (extents
+    included) before any device work."""
+    L = _lib.lib()
+    good = SolverConfig(size_x=16, size_y=24, size_z=8, margin_y=4, extent_x=2.0, problem="shearing_box")
+    bad = SolverConfig(size_x=16, size_y=24, size_z=8, margin_y=4, extent_x=2.0, extent_y=0.0,
+                       problem="shearing_box")
+    arr = (NmhdConfig * 2)(good.to_ctypes(), bad.to_ctypes())
+    h = ctypes.c_void_p()
+    assert L.nmhd_batch_create(arr, 2, ctypes.byref(h)) == -1
+    assert b"box 1" in L.nmhd_batch_last_error(None) and b"extents" in L.nmhd_batch_last_error(None)
+    assert not h.value

@@ -1,9 +1,10 @@
 """The allocation-free entry point, nmhd_advance_noalloc, called through the C ABI.
 
-It is for callers that cannot allocate device memory (inside another
-library's CUDA-graph capture, under a host allocator that owns all device
-memory, in real-time loops).  This file is named so pytest collects it last;
-it passes alone in a fresh process and after the other tests.
+It is for callers that cannot allocate device memory: a host framework whose
+caching allocator has reserved the device's memory, or a real-time loop where
+a device allocation and the synchronisation it can bring are not allowed.
+This file is named so pytest collects it last; it passes alone in a fresh
+process and after the other tests.
 
 Tolerance: bitwise equality with the existing entry point (nmhd_create +
 nmhd_proceed), the same bar as every other parity test here.
@@ -33,13 +34,20 @@ def noalloc(cfg, dev_in, dev_out, time, generation, steps, goal=math.inf):
     return code, t.value, g.value, done.value
 
 
-@pytest.mark.parametrize("case", ["orszag_tang", "shearing_box"])
+@pytest.mark.parametrize("case", ["orszag_tang", "shearing_box", "euler", "z_margins"])
 def test_noalloc_matches_existing_entry_point_twice(gpu, case):
     import torch
     if case == "orszag_tang":
         cfg, s = orszag_tang_3d(24, ny=20, nz=12)
-    else:
+    elif case == "shearing_box":
         cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=21)
+    elif case == "euler":  # time_order 1
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=22)
+        cfg.time_order = 1
+    else:  # Z margins filled by copy, as the reference's kMarginSizeZ
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=23)
+        cfg.margin_z, cfg.size_z = 4, 16
+        s = np.ascontiguousarray(np.concatenate([s[:, -4:], s, s[:, :4]], axis=1))
     steps = 7
     # existing entry point: the same box after `steps` and after 2*`steps` steps
     with MHDSolver(cfg) as sol:
@@ -81,3 +89,19 @@ def test_noalloc_goal_time_and_size_limit(gpu):
     code, _, _, _ = noalloc(big, a, b, 0.0, 0, 1)
     assert code == -1
     assert b"at most 262144" in _lib.lib().nmhd_noalloc_last_error()
+
+
+def test_noalloc_stops_at_the_goal_within_a_large_step_cap(gpu):
+    """nsteps is a cap: with a goal a few steps away and a cap of 10^12 the
+    call returns once the goal step is done (the control block is read back
+    every 16 steps)."""
+    import time as _time
+    import torch
+    cfg, s = orszag_tang_3d(16)
+    a = torch.from_numpy(s).to(gpu)
+    b = torch.empty_like(a)
+    t0 = _time.perf_counter()
+    code, t, g, done = noalloc(cfg, a, b, 0.0, 0, 10 ** 12, goal=0.01)
+    assert code == _lib.GOAL_REACHED
+    assert t == float(np.float32(0.01)) and done == g
+    assert _time.perf_counter() - t0 < 60
