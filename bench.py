@@ -92,27 +92,78 @@ def load_peaks():
 
 
 class ClockSampler:
-    """nvidia-smi samples of SM clock and throttle reasons while running."""
+    """SM clock and clock-event (throttle) reasons sampled while running.
+
+    NVML is polled every 2 ms from a thread (read-only queries), so that a
+    timed region of a few milliseconds still carries its own clock record;
+    without NVML, nvidia-smi samples every 200 ms."""
 
     Q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
          "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
          "clocks_event_reasons.sw_power_cap")
+    NAMES = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
 
-    def __init__(self, index):
+    def __init__(self, index, period_s=0.002):
         self.index = index
+        self.period = period_s
         self.proc = None
         self.out = None
+        self.thread = None
+        self.samples = []
+        self.max_mhz = None
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        pynvml.nvmlInit()
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.index).uuid)
+            return pynvml, pynvml.nvmlDeviceGetHandleByUUID(uuid if uuid.startswith("GPU-") else "GPU-" + uuid)
+        except Exception:
+            vis = os.environ.get("CUDA_VISIBLE_DEVICES", "")
+            ids = [v for v in vis.split(",") if v.strip()]
+            idx = int(ids[self.index]) if self.index < len(ids) and ids[self.index].strip().isdigit() else self.index
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(idx)
+
+    def _poll(self, nv, h):
+        bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+        while not self.stop.is_set():
+            try:
+                mhz = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+            except Exception:
+                break
+            self.samples.append((float(mhz), [k for k, b in bits.items() if r & b]))
+            self.stop.wait(self.period)
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self.thread = threading.Thread(target=self._poll, args=(nv, h), daemon=True)
+            self.thread.start()
+            self.source = "nvml, %g ms period" % (1e3 * self.period)
+            return self
+        except Exception:
+            self.thread = None
         if shutil.which("nvidia-smi"):
             self.out = tempfile.TemporaryFile(mode="w+")
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
                  "--format=csv,noheader,nounits", "-lms", "200"],
                 stdout=self.out, stderr=subprocess.DEVNULL)
+            self.source = "nvidia-smi, 200 ms period"
         return self
 
     def __exit__(self, *exc):
+        if self.thread:
+            self.stop.set()
+            self.thread.join(timeout=5)
         if self.proc:
             self.proc.terminate()
             try:
@@ -121,27 +172,29 @@ class ClockSampler:
                 self.proc.kill()
 
     def summary(self):
-        if not self.out:
-            return None
-        self.out.seek(0)
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.out:
-            f = [t.strip() for t in line.split(",")]
-            if len(f) < 7:
-                continue
-            try:
-                sm.append(float(f[0]))
-                mx = float(f[1])
-            except ValueError:
-                continue
-            for name, val in zip(names, f[3:7]):
-                if val.lower() == "active":
-                    reasons.add(name)
+        sm, mx, reasons = [], self.max_mhz, set()
+        if self.thread is not None:
+            for mhz, rs in self.samples:
+                sm.append(mhz)
+                reasons.update(rs)
+        elif self.out:
+            self.out.seek(0)
+            for line in self.out:
+                f = [t.strip() for t in line.split(",")]
+                if len(f) < 7:
+                    continue
+                try:
+                    sm.append(float(f[0]))
+                    mx = float(f[1])
+                except ValueError:
+                    continue
+                for name, val in zip(self.NAMES, f[3:7]):
+                    if val.lower() == "active":
+                        reasons.add(name)
         if not sm:
             return None
         return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": self.source}
 
 
 def cpu_reference_run(workload, steps, threads=None):
@@ -253,6 +306,8 @@ def run_gpu_arm(args):
         tuning = sol.autotune(steps=5)
         best = min(tuning, key=lambda t: t[3])
         choice = {"variant": best[0], "tile_rows": best[1], "z_chunk": best[2], "source": "autotune"}
+    # the timed region launches only graphs built here, before it starts
+    sol.prepare(args.steps)
     sol.step(args.warmup)
     torch.cuda.synchronize(dev)
 
@@ -306,6 +361,7 @@ def run_gpu_arm(args):
         fdev = max(float(np.abs(a[g_].astype(np.float64) - b[g_]).max() / max(np.abs(b[g_]).max(), 1e-30))
                    for g_ in ([0], [1, 2, 3], [4], [5, 6, 7]))
         ref_sol.close()
+        fs.prepare(args.steps)
         fs.step(args.warmup)
         torch.cuda.synchronize(dev)
         barrier()
@@ -394,61 +450,82 @@ def run_gpu_arm(args):
             line["autotune_ms_per_step"] = {f"v{a}_r{b}_z{c}": round(d, 4) for a, b, c, d in tuning}
         if world == 1 and not args.no_cpu:
             line["cpu_baseline"] = cpu_sample(wl)
-        print(json.dumps(line), flush=True)
     sol.close()
+    # the other two parts of the metric (plain vs batched; adjoint/forward),
+    # measured in the same run on one GPU: the 64-box ensemble batched and
+    # through per-box plain launches, and the adjoint of the 64^3 box with
+    # the whole tape kept and with the last segment only
+    if world == 1 and not args.no_extras:
+        ens = ensemble_measure("mri_ensemble_64", max(args.steps, 16), args.warmup, dev)
+        line["ensemble_64"] = {k: ens[k] for k in ("value", "unit", "steps", "ms_per_step", "boxes",
+                                                   "cells_interior", "plain_per_box", "batch_speedup",
+                                                   "e2e", "gpu_launches", "schedule", "clocks")}
+        line["ensemble_64"]["metric"] = "Mcell-updates/s, 64 uneven boxes batched (plain_per_box: same boxes, one solver each)"
+        adj = {}
+        for name, budget in (("whole_tape", -1), ("last_segment_only", 0)):
+            m = adjoint_measure("mri_adjoint_64", dev, tape_budget=budget, warmup=1, reps=3)
+            adj[name] = {k: m[k] for k in ("value", "forward_ms", "adjoint_total_ms", "adjoint_reverse_ms",
+                                           "segments_kept_on_tape", "segments", "phases_ms")}
+        line["adjoint_64"] = {"metric": "adjoint/forward time ratio, 64^3 shearing box, 200 steps, "
+                                        "checkpoints every 20",
+                              "unit": "x", "higher_is_better": False, **adj}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 
 
-def run_ensemble_arm(args):
-    """Batched ensemble (64 uneven shearing boxes): aggregate interior
-    cell-updates/s of the batch, and of the same boxes stepped one by one
-    through the single-box path (plain per-box launches)."""
+def ensemble_measure(workload, steps, warmup, dev, rank=0, world=1, dist=None, n_boxes=0, plain=True):
+    """Batched ensemble (e.g. 64 uneven shearing boxes): aggregate interior
+    cell-updates/s of the batch (device-timed, states resident), the same end
+    to end through the public API, and of the same boxes stepped one by one
+    through the single-box path (plain per-box launches).  With world > 1 the
+    boxes are partitioned over the ranks (no data-path collective) and times
+    are the max over ranks."""
     import torch
     from nmhd_b200.batch import BatchSolver
     from nmhd_b200.problems import mri_ensemble
+    from nmhd_b200.shard import my_boxes
     from nmhd_b200.solver import MHDSolver
 
-    from nmhd_b200.shard import my_boxes
-
-    rank, world, local, dist = dist_setup(args.gpus)
-    dev = torch.device("cuda", local)
-    all_boxes, params = mri_ensemble(**ENSEMBLES[args.workload])
-    if args.boxes:  # the first N boxes only (small profiling cases)
-        all_boxes = all_boxes[:args.boxes]
+    all_boxes, params = mri_ensemble(**ENSEMBLES[workload])
+    if n_boxes:  # the first N boxes only (small profiling cases)
+        all_boxes = all_boxes[:n_boxes]
     total_interior = sum(c.interior_cells for c, _ in all_boxes)
-    # N > 1: the ensemble is partitioned over the ranks (boxes never exchange
-    # data); every rank computes the same cost-balanced assignment
     boxes = [all_boxes[i] for i in my_boxes([c for c, _ in all_boxes], rank, world)]
     cfgs = [c for c, _ in boxes]
-    interior = sum(c.interior_cells for c in cfgs)
+
+    def max_over_ranks(x):
+        if not dist:
+            return x
+        tt = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        return float(tt.item())
+
     stream = torch.cuda.Stream(device=dev)
     batch = BatchSolver(cfgs)
     batch.set_stream(stream.cuda_stream)
     for i, (_, s) in enumerate(boxes):
         batch.set_state(i, s)
-    batch.step(args.warmup)
+    batch.step(warmup)
     # schedule of each stage kernel (persistent or one tile per CTA), timed on these boxes
     tuning = batch.autotune(reps=3)
     schedule = {("flux", "ct", "update")[k]: ("persistent" if p else "per_tile") + ("_split" if s else "")
                 for k, p, s, ms in tuning if ms == min(m for kk, _, _, m in tuning if kk == k)}
-    batch.step(args.warmup)
+    batch.prepare(steps)
+    batch.step(warmup)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     torch.cuda.synchronize(dev)
     if dist:
         dist.barrier()
     with ClockSampler(dev.index) as clocks:
         e0.record(stream)
-        batch.step(args.steps)
+        batch.step(steps)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-    ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
-    value = total_interior * args.steps / (ms * 1e-3) / 1e6
-    launches = batch.launches_per_step() * args.steps
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    value = total_interior * steps / (ms * 1e-3) / 1e6
+    launches = batch.launches_per_step() * steps
     # end to end through the public API: every box's state in from pinned host
     # memory, the same steps, every box's state out to pinned host memory
     pinned = lambda a: torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).pin_memory().numpy()
@@ -459,66 +536,78 @@ def run_ensemble_arm(args):
         dist.barrier()
     e0.record(stream)
     batch.set_states(host_in)
-    batch.step(args.steps)
+    batch.step(steps)
     batch.get_states(out=host_out)
     e1.record(stream)
     torch.cuda.synchronize(dev)
-    e2e_ms = e0.elapsed_time(e1)
-    if dist:
-        t = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_ms = float(t.item())
+    e2e_ms = max_over_ranks(e0.elapsed_time(e1))
     state_bytes = sum(h.nbytes for h in host_in)
-    e2e = {"value": total_interior * args.steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
-           "h2d_bytes_per_step": state_bytes / args.steps, "d2h_bytes_per_step": state_bytes / args.steps,
+    e2e = {"value": total_interior * steps / (e2e_ms * 1e-3) / 1e6, "unit": "Mcell-updates/s",
+           "h2d_bytes_per_step": state_bytes / steps, "d2h_bytes_per_step": state_bytes / steps,
            "note": "set_states (every box, pinned host) + proceed(K steps) + get_states (every box, "
                    "pinned host), per step"}
-    # plain: each box through its own single-box solver, one after another
-    plain_steps = 0 if args.no_plain else max(3, args.steps // 4)
+    batch.close()
+    # plain: each box through its own single-box solver, one after another,
+    # graphs built before the timed region
+    plain_steps = max(3, steps // 4) if plain else 0
     solvers = []
     plain_wall = 0.0
     for c, s in boxes if plain_steps else []:
         sol = MHDSolver(c)
         sol.set_stream(stream.cuda_stream)
         sol.set_state(s)
-        sol.step(args.warmup)
+        sol.prepare(plain_steps)
+        sol.step(warmup)
         solvers.append(sol)
     if plain_steps:
         torch.cuda.synchronize(dev)
+        if dist:
+            dist.barrier()
         e0.record(stream)
         for sol in solvers:
             sol.step(plain_steps)
         e1.record(stream)
         torch.cuda.synchronize(dev)
-        plain_wall = e0.elapsed_time(e1) * 1e-3
-        if dist:
-            t = torch.tensor([plain_wall], dtype=torch.float64, device=dev)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            plain_wall = float(t.item())
-    plain = total_interior * plain_steps / plain_wall / 1e6 if plain_steps else None
+        plain_wall = max_over_ranks(e0.elapsed_time(e1)) * 1e-3
+    plain_v = total_interior * plain_steps / plain_wall / 1e6 if plain_steps else None
     for sol in solvers:
         sol.close()
+    return {"value": value, "unit": "Mcell-updates/s", "steps": steps, "ms_per_step": ms / steps,
+            "boxes": len(all_boxes), "cells_interior": total_interior, "schedule": schedule,
+            "autotune_ms_per_launch": {"%s_%s%s" % (("flux", "ct", "update")[k],
+                                                    "persistent" if p else "per_tile",
+                                                    "_split" if s else ""): round(ms_, 4)
+                                       for k, p, s, ms_ in tuning},
+            "plain_per_box": {"value": plain_v, "unit": "Mcell-updates/s", "steps": plain_steps,
+                              "note": "same boxes, one single-box solver each, stepped one after another"},
+            "batch_speedup": value / plain_v if plain_v else None,
+            "e2e": e2e, "gpu_launches": launches, "clocks": clocks.summary()}
+
+
+def run_ensemble_arm(args):
+    """The batched ensemble as the bench line's workload (strong scaling over
+    ranks: the same boxes, partitioned)."""
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    m = ensemble_measure(args.workload, args.steps, args.warmup, dev, rank, world, dist, args.boxes,
+                         plain=not args.no_plain)
     if rank == 0:
         line = {
-            "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+            "metric": "Mcell-updates/s", "value": m["value"], "unit": "Mcell-updates/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": m["ms_per_step"],
             "higher_is_better": True, "scaling": "strong", "vs_baseline": None, "dtype": "f32",
             "data": "synthetic (seeded ensemble of shearing boxes)",
-            "config": {"workload": args.workload, "boxes": len(all_boxes), "cells_interior": total_interior,
+            "config": {"workload": args.workload, "boxes": m["boxes"], "cells_interior": m["cells_interior"],
                        "parallelism": "boxes sharded over %d GPUs" % world if world > 1 else "single",
-                       "timing": "CUDA events on the batch's stream around proceed() (one host sync per "
-                                 "16-step graph inside)",
-                       "schedule": schedule},
-            "autotune_ms_per_launch": {"%s_%s%s" % (("flux", "ct", "update")[k], "persistent" if p else "per_tile",
-                                                    "_split" if s else ""): round(ms, 4) for k, p, s, ms in tuning},
-            "plain_per_box": {"value": plain, "unit": "Mcell-updates/s", "steps": plain_steps,
-                              "note": "same boxes, one single-box solver each, stepped one after another"},
-            "batch_speedup": value / plain if plain else None,
-            "e2e": e2e, "gpu_launches": launches,
-            "clocks": clocks.summary(),
+                       "timing": "CUDA events on the batch's stream around proceed() (graphs built "
+                                 "before the timed region)",
+                       "schedule": m["schedule"]},
+            "autotune_ms_per_launch": m["autotune_ms_per_launch"],
+            "plain_per_box": m["plain_per_box"], "batch_speedup": m["batch_speedup"],
+            "e2e": m["e2e"], "gpu_launches": m["gpu_launches"], "clocks": m["clocks"],
         }
         print(json.dumps(line), flush=True)
-    batch.close()
     if dist:
         dist.destroy_process_group()
 
@@ -605,41 +694,40 @@ def run_slab_arm(args):
     dist.destroy_process_group()
 
 
-def run_adjoint_arm(args):
-    """Adjoint / forward time ratio on the 64^3 shearing box, with the
-    gradient's checks: central differences of the FP32 and FP64 losses along
-    16 seeded initial-velocity directions, the FP64 tangent-linear run along 4
-    of them, and the FP64 adjoint-vs-tangent transpose identity."""
+def adjoint_measure(workload, dev, tape_budget=-1, warmup=3, reps=1, adjoint_steps=0, checks=False):
+    """Adjoint / forward time ratio on the 64^3 shearing box (200 FP32 steps,
+    checkpoints every 20): the forward is the production path (nmhd_proceed,
+    its graphs built before timing), the adjoint run is nmhd_adjoint_run with
+    the given tape budget (-1: as many segments as fit in half the free HBM;
+    0: the last segment only, every other segment recomputed from its
+    checkpoint).  Median over `reps` runs of each."""
     import torch
     from nmhd_b200.problems import shearing_box
     from nmhd_b200.solver import MHDSolver
 
-    rank, world, local, dist = dist_setup(args.gpus)
-    dev = torch.device("cuda", local)
-    spec = ADJOINTS[args.workload]
+    spec = ADJOINTS[workload]
     n = spec["n"]
     cfg, s = shearing_box(n_radial=n, n_azimuthal=n, n_vertical=n, l_radial=1.0, l_azimuthal=1.0,
                           l_vertical=1.0, seed=spec["seed"])
     steps, window, K = spec["steps"], spec["window"], spec["ckpt"]
-    if args.adjoint_steps:  # shorter runs (profiling): the window keeps its length, at the end
-        steps = args.adjoint_steps
+    if adjoint_steps:  # shorter runs (profiling): the window keeps its length, at the end
+        steps = adjoint_steps
         window = (max(0, steps - (window[1] - window[0])), steps)
     stream = torch.cuda.Stream(device=dev)
     sol = MHDSolver(cfg)
     sol.set_stream(stream.cuda_stream)
     sol.set_state(s)
-    sol.set_adjoint_tape_budget(args.tape_budget)
-    for _ in range(args.warmup):
+    sol.set_adjoint_tape_budget(tape_budget)
+    for _ in range(warmup):
         sol.adjoint(steps, window=window, ckpt_every=K)
-    # forward: the production path (nmhd_proceed, CUDA graphs) over the same steps
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     fwd = []
-    reps = max(1, args.steps // 100)
     with ClockSampler(dev.index) as clocks:
         for _ in range(reps):
             sol.set_state(s)
             sol.set_time(0.0, 0)
-            sol.step(3)  # builds this box's graphs, then restart
+            sol.prepare(steps)
+            sol.step(3)  # warm, then restart from the initial state
             sol.set_state(s)
             sol.set_time(0.0, 0)
             torch.cuda.synchronize(dev)
@@ -657,23 +745,44 @@ def run_adjoint_arm(args):
     fwd_ms = statistics.median(fwd)
     tot = statistics.median([a["total"] for a in adj])
     rev = statistics.median([a["recompute"] + a["adjoint"] for a in adj])
-    line = {
-        "metric": "adjoint/forward time ratio", "value": tot / fwd_ms, "unit": "x",
-        "n_gpus": world, "steps": steps, "warmup": args.warmup, "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing box)",
-        "config": {"workload": args.workload, "cells_interior": cfg.interior_cells,
-                   "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
-                   "ckpt_every": K, "tape_budget_bytes": args.tape_budget,
-                   "segments_kept_on_tape": sol.adjoint_kept_segments(),
-                   "segments": -(-steps // K),
-                   "parallelism": "replicas" if world > 1 else "single"},
-        "forward_ms": fwd_ms, "adjoint_total_ms": tot, "adjoint_reverse_ms": rev,
-        "reverse_over_forward": rev / fwd_ms, "phases_ms": adj[-1], "loss": J,
-        "clocks": clocks.summary(),
-    }
-    if not args.no_checks:
-        line["gradient_checks"] = adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg)
+    out = {"value": tot / fwd_ms, "unit": "x", "steps": steps, "cells_interior": cfg.interior_cells,
+           "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
+           "ckpt_every": K, "tape_budget_bytes": tape_budget,
+           "segments_kept_on_tape": sol.adjoint_kept_segments(), "segments": -(-steps // K),
+           "forward_ms": fwd_ms, "adjoint_total_ms": tot, "adjoint_reverse_ms": rev,
+           "reverse_over_forward": rev / fwd_ms, "phases_ms": adj[-1], "loss_value": J,
+           "clocks": clocks.summary()}
+    if checks:
+        out["gradient_checks"] = adjoint_checks(sol, s, g, dts, steps, window, K, spec, cfg)
     sol.close()
+    return out
+
+
+def run_adjoint_arm(args):
+    """Adjoint / forward time ratio on the 64^3 shearing box, with the
+    gradient's checks: central differences of the FP32 and FP64 losses along
+    16 seeded initial-velocity directions, the FP64 tangent-linear run along 4
+    of them, and the FP64 adjoint-vs-tangent transpose identity."""
+    import torch
+    rank, world, local, dist = dist_setup(args.gpus)
+    dev = torch.device("cuda", local)
+    m = adjoint_measure(args.workload, dev, args.tape_budget, args.warmup, max(1, args.steps // 100),
+                        args.adjoint_steps, checks=not args.no_checks)
+    line = {
+        "metric": "adjoint/forward time ratio", "value": m["value"], "unit": "x",
+        "n_gpus": world, "steps": m["steps"], "warmup": args.warmup, "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded shearing box)",
+        "config": {"workload": args.workload, "cells_interior": m["cells_interior"],
+                   "cells_with_margins": m["cells_with_margins"], "loss": m["loss"],
+                   "ckpt_every": m["ckpt_every"], "tape_budget_bytes": args.tape_budget,
+                   "segments_kept_on_tape": m["segments_kept_on_tape"], "segments": m["segments"],
+                   "parallelism": "replicas" if world > 1 else "single"},
+        "forward_ms": m["forward_ms"], "adjoint_total_ms": m["adjoint_total_ms"],
+        "adjoint_reverse_ms": m["adjoint_reverse_ms"], "reverse_over_forward": m["reverse_over_forward"],
+        "phases_ms": m["phases_ms"], "loss": m["loss_value"], "clocks": m["clocks"],
+    }
+    if "gradient_checks" in m:
+        line["gradient_checks"] = m["gradient_checks"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist:
@@ -764,6 +873,8 @@ def main():
                     choices=sorted(WORKLOADS) + sorted(ENSEMBLES) + sorted(ADJOINTS) + sorted(SLABS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--no-fast", action="store_true", help="skip the fast-arithmetic measurement")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="default workload: skip the ensemble and adjoint measurements")
     ap.add_argument("--kernel", default="", help="variant,tile_rows,z_chunk (skip autotuning)")
     ap.add_argument("--no-checks", action="store_true", help="adjoint workload: timing only")
     ap.add_argument("--adjoint-steps", type=int, default=0, help="adjoint workload: steps per run (default 200)")

@@ -137,6 +137,12 @@ nmhd_status nmhd_write(nmhd_solver *s, const char *path);
  * *steps_done (may be NULL) receives the number of steps taken. */
 nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limit,
                          int64_t max_steps, int64_t *steps_done);
+/* Builds, without running them, the CUDA graphs that nmhd_proceed(..., max_steps,
+ * ...) launches (it steps in graphs of 16 steps and one of the remainder;
+ * max_steps <= 0: the 16-step graph), so that a later proceed spends no host
+ * time capturing them.  No counterpart in the reference, which launches every
+ * kernel of every step from the host (mhd_solver.inlrb:850-993). */
+nmhd_status nmhd_prepare(nmhd_solver *s, int64_t max_steps);
 
 /* MHDSolver::current_time(), generation(), and the GlobalSetup fields that
  * load_state() restores. */
@@ -254,6 +260,9 @@ nmhd_status nmhd_batch_clock(nmhd_batch *b, int box, double *time, int64_t *gene
  * (semantics of nmhd_proceed, per box; a box that reached the goal waits).
  * *steps_done: steps taken by the box that took most. */
 nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_steps, int64_t *steps_done);
+/* Builds, without running them, the CUDA graphs nmhd_batch_proceed(..., max_steps,
+ * ...) launches (as nmhd_prepare). */
+nmhd_status nmhd_batch_prepare(nmhd_batch *b, int64_t max_steps);
 /* Stream of the batch's work, as nmhd_set_stream (NULL: a stream of its own). */
 nmhd_status nmhd_batch_set_stream(nmhd_batch *b, void *cuda_stream);
 /* Tile of box `box` in the batched kernels: tile_x x tile_y x tile_z cells (256

@@ -239,6 +239,9 @@ class MHDSolver {
       if (st == NMHD_TIMEOUT) return false;
     }
   }
+  // Builds the CUDA graphs a later proceed(..., max_steps) launches, without
+  // running them (nmhd_prepare).
+  void prepare(long long max_steps = 0) { check(nmhd_prepare(s_, max_steps)); }
   // The application's monitor() (e.g. src/application/kepler_disk_demo/
   // mhd_solver.curb:107-130); an empty function removes it.
   void set_monitor(std::function<int(MHDSolver &)> m) { monitor_ = std::move(m); }

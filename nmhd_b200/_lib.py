@@ -46,6 +46,7 @@ _SIGS = [
     ("nmhd_write", ctypes.c_int, [_P, ctypes.c_char_p]),
     ("nmhd_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_double, ctypes.c_int64,
                                     ctypes.POINTER(ctypes.c_int64)]),
+    ("nmhd_prepare", ctypes.c_int, [_P, ctypes.c_int64]),
     ("nmhd_current_time", ctypes.c_double, [_P]),
     ("nmhd_generation", ctypes.c_int64, [_P]),
     ("nmhd_set_time", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64]),
@@ -85,6 +86,7 @@ _SIGS = [
                                         ctypes.POINTER(ctypes.c_int64)]),
     ("nmhd_batch_proceed", ctypes.c_int, [_P, ctypes.c_double, ctypes.c_int64,
                                           ctypes.POINTER(ctypes.c_int64)]),
+    ("nmhd_batch_prepare", ctypes.c_int, [_P, ctypes.c_int64]),
     ("nmhd_batch_set_schedule", ctypes.c_int, [_P, ctypes.c_int, ctypes.c_int, ctypes.c_int]),
     ("nmhd_batch_set_stream", ctypes.c_int, [_P, _P]),
     ("nmhd_batch_launches_per_step", ctypes.c_int, [_P]),

@@ -116,6 +116,11 @@ class BatchSolver:
         self.proceed(math.inf, nsteps)
         return self.last_steps
 
+    def prepare(self, max_steps=0):
+        """Build the CUDA graphs a later proceed(..., max_steps) launches,
+        without running them (nmhd_batch_prepare)."""
+        self._check(self._L.nmhd_batch_prepare(self._h, int(max_steps)))
+
     def set_stream(self, cuda_stream):
         """Run the batch's work on ``cuda_stream`` (a cudaStream_t as int, e.g.
         torch.cuda.Stream().cuda_stream); None: a stream of its own."""

@@ -252,6 +252,10 @@ struct nmhd_batch {
   bool own_stream = true;
   bool cfl_ready = false;
   std::map<int, cudaGraphExec_t> graphs;
+  // Pinned copies of every box's control block after each of the (at most
+  // two) step batches in flight in nmhd_batch_proceed, and their events.
+  StepCtl *hctl = nullptr;
+  cudaEvent_t batch_done[2] = {nullptr, nullptr};
   std::string err;
 };
 
@@ -341,6 +345,29 @@ void enqueue_batch_step(nmhd_batch *b) {
   stage(2, 1, 0, 1);
 }
 
+// Steps per CUDA graph of nmhd_batch_proceed.
+constexpr int kBatchSteps = 16;
+
+// The graph of k batched steps (captured on first use).
+nmhd_status batch_graph(nmhd_batch *b, int k, cudaGraphExec_t *out) {
+  auto it = b->graphs.find(k);
+  if (it != b->graphs.end()) {
+    *out = it->second;
+    return NMHD_OK;
+  }
+  cudaGraph_t graph;
+  cudaGraphExec_t ge;
+  BATCH_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+  for (int i = 0; i < k; ++i) enqueue_batch_step(b);
+  BATCH_CUDA(b, cudaStreamEndCapture(b->stream, &graph));
+  cudaError_t e = cudaGraphInstantiate(&ge, graph, 0);
+  cudaGraphDestroy(graph);
+  if (e != cudaSuccess) return bfail(b, NMHD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+  b->graphs[k] = ge;
+  *out = ge;
+  return NMHD_OK;
+}
+
 nmhd_status read_ctls(nmhd_batch *b, std::vector<StepCtl> &h) {
   h.resize(b->n);
   BATCH_CUDA(b, cudaMemcpyAsync(h.data(), b->ctls, sizeof(StepCtl) * b->n, cudaMemcpyDeviceToHost, b->stream));
@@ -392,6 +419,9 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
   if (e == cudaSuccess) e = cudaMalloc(&b->hist, sizeof(float) * nmhd::kDtHistCap * n);
   if (e == cudaSuccess) e = cudaMalloc(&b->ctls, sizeof(StepCtl) * n);
   if (e == cudaSuccess) e = cudaMalloc(&b->d_boxes, sizeof(BoxDesc) * n);
+  if (e == cudaSuccess) e = cudaMallocHost(&b->hctl, 2 * sizeof(StepCtl) * n);
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&b->batch_done[i], cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMemsetAsync(b->pool, 0, sizeof(float) * pool_floats, b->stream);
   if (e != cudaSuccess) {
     nmhd_batch_destroy(b);
@@ -479,6 +509,9 @@ void nmhd_batch_destroy(nmhd_batch *b) {
   cudaFree(b->hist);
   cudaFree(b->ctls);
   cudaFree(b->d_boxes);
+  if (b->hctl) cudaFreeHost(b->hctl);
+  for (cudaEvent_t ev : b->batch_done)
+    if (ev) cudaEventDestroy(ev);
   if (b->stream && b->own_stream) cudaStreamDestroy(b->stream);
   delete b;
 }
@@ -596,33 +629,36 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
     BATCH_CUDA(b, cudaGetLastError());
     b->cfl_ready = true;
   }
-  const int kBatch = 16;
+  // As nmhd_proceed: batches of kBatchSteps steps, one graph each, the next
+  // launched before the previous one's control blocks are read (a batch
+  // after every box's goal step returns at once on the device).
   long long left = max_steps > 0 ? max_steps : -1;
-  long long launched = 0;
+  int queue[2], queued = 0, head = 0, next_slot = 0;
+  const size_t nctl = (size_t)b->n;
   nmhd_status result = NMHD_OK;
   for (;;) {
-    int k = kBatch;
-    if (left >= 0 && left < k) k = (int)left;
-    if (k == 0) { result = NMHD_STEP_LIMIT; break; }
-    cudaGraphExec_t ge;
-    auto it = b->graphs.find(k);
-    if (it == b->graphs.end()) {
-      cudaGraph_t graph;
-      BATCH_CUDA(b, cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
-      for (int i = 0; i < k; ++i) enqueue_batch_step(b);
-      BATCH_CUDA(b, cudaStreamEndCapture(b->stream, &graph));
-      cudaError_t e = cudaGraphInstantiate(&ge, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess) return bfail(b, NMHD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      b->graphs[k] = ge;
-    } else {
-      ge = it->second;
+    while (queued < 2 && left != 0) {
+      int k = kBatchSteps;
+      if (left >= 0 && left < k) k = (int)left;
+      cudaGraphExec_t ge;
+      st = batch_graph(b, k, &ge);
+      if (st != NMHD_OK) return st;
+      const int slot = next_slot;
+      next_slot ^= 1;
+      BATCH_CUDA(b, cudaGraphLaunch(ge, b->stream));
+      BATCH_CUDA(b, cudaMemcpyAsync(b->hctl + slot * nctl, b->ctls, sizeof(StepCtl) * nctl,
+                                    cudaMemcpyDeviceToHost, b->stream));
+      BATCH_CUDA(b, cudaEventRecord(b->batch_done[slot], b->stream));
+      queue[(head + queued) % 2] = slot;
+      ++queued;
+      if (left > 0) left -= k;
     }
-    BATCH_CUDA(b, cudaGraphLaunch(ge, b->stream));
-    st = read_ctls(b, h);
-    if (st != NMHD_OK) return st;
-    launched += k;
-    if (left > 0) left -= k;
+    if (queued == 0) { result = NMHD_STEP_LIMIT; break; }
+    const int slot = queue[head];
+    head = (head + 1) % 2;
+    --queued;
+    BATCH_CUDA(b, cudaEventSynchronize(b->batch_done[slot]));
+    h.assign(b->hctl + slot * nctl, b->hctl + (slot + 1) * nctl);
     int bad = -1, done = 0;
     for (int i = 0; i < b->n; ++i) {
       if (h[i].status && bad < 0) bad = i;
@@ -635,12 +671,23 @@ nmhd_status nmhd_batch_proceed(nmhd_batch *b, double goal_time, int64_t max_step
     }
     if (done == b->n) { result = NMHD_GOAL_REACHED; break; }
   }
+  BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
   if (steps_done) {
     long long gen1 = 0;
     for (int i = 0; i < b->n; ++i) gen1 = std::max(gen1, h[i].generation);
     *steps_done = gen1 - gen0;
   }
   return result;
+}
+
+nmhd_status nmhd_batch_prepare(nmhd_batch *b, int64_t max_steps) {
+  if (!b) return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "NULL batch");
+  cudaGraphExec_t ge;
+  const int first = max_steps > 0 && max_steps < kBatchSteps ? (int)max_steps : kBatchSteps;
+  nmhd_status st = batch_graph(b, first, &ge);
+  if (st == NMHD_OK && max_steps > kBatchSteps && max_steps % kBatchSteps)
+    st = batch_graph(b, (int)(max_steps % kBatchSteps), &ge);
+  return st;
 }
 
 int nmhd_batch_launches_per_step(const nmhd_batch *b) {

@@ -146,6 +146,9 @@ nmhd_status write_ctl(nmhd_solver *s, const StepCtl &h) {
 
 float *current_buffer(nmhd_solver *s, const StepCtl &h) { return h.parity ? s->w1 : s->w0; }
 
+// Steps per CUDA graph of nmhd_proceed.
+constexpr int kStepBatch = 16;
+
 // One RK stage with the selected kernel variant.
 void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
   const GridParams &g = s->g;
@@ -255,6 +258,9 @@ nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
   if (e == cudaSuccess) e = cudaMalloc(&s->dt_hist, sizeof(float) * nmhd::kDtHistCap);
   if (e == cudaSuccess) e = cudaMalloc(&s->ctl, sizeof(StepCtl));
   if (e == cudaSuccess) e = cudaMalloc(&s->diag, sizeof(double) * nmhd::kDiagFields);
+  if (e == cudaSuccess) e = cudaMallocHost(&s->hctl, 2 * sizeof(StepCtl));
+  for (int i = 0; i < 2 && e == cudaSuccess; ++i)
+    e = cudaEventCreateWithFlags(&s->batch_done[i], cudaEventDisableTiming);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->w0, 0, sizeof(float) * 8 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->w1, 0, sizeof(float) * 8 * n, s->stream);
   if (e == cudaSuccess) e = cudaMemsetAsync(s->wp, 0, sizeof(float) * 8 * n, s->stream);
@@ -292,6 +298,9 @@ void nmhd_destroy(nmhd_solver *s) {
   cudaFree(s->dt_hist);
   cudaFree(s->ctl);
   cudaFree(s->diag);
+  if (s->hctl) cudaFreeHost(s->hctl);
+  for (cudaEvent_t ev : s->batch_done)
+    if (ev) cudaEventDestroy(ev);
   if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
   delete s;
 }
@@ -389,20 +398,39 @@ nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limi
     NMHD_CUDA(s, cudaGetLastError());
     s->cfl_ready = true;
   }
-  const int kBatch = 16;
+  // Batches of kStepBatch steps, each one CUDA graph followed by a copy of the
+  // control block to pinned host memory.  Without a wallclock limit the next
+  // batch is launched before the previous one's control block is read, so the
+  // GPU does not idle while the host checks it; a batch launched after the
+  // goal step returns at once on the device (every kernel tests `done`).
+  // With a wallclock limit one batch at a time is in flight, so the limit
+  // stops the run within one batch, as before.
   long long left = max_steps > 0 ? max_steps : -1;
+  const int depth = wallclock_limit > 0 ? 1 : 2;
+  int queue[2], queued = 0, head = 0, next_slot = 0;
   nmhd_status result = NMHD_OK;
   for (;;) {
-    int batch = kBatch;
-    if (left >= 0 && left < batch) batch = (int)left;
-    if (batch == 0) { result = NMHD_STEP_LIMIT; break; }
-    cudaGraphExec_t ge;
-    st = graph_for(s, batch, &ge);
-    if (st != NMHD_OK) return st;
-    NMHD_CUDA(s, cudaGraphLaunch(ge, s->stream));
-    st = read_ctl(s, h);
-    if (st != NMHD_OK) return st;
-    if (left > 0) left -= batch;
+    while (queued < depth && left != 0) {
+      int batch = kStepBatch;
+      if (left >= 0 && left < batch) batch = (int)left;
+      cudaGraphExec_t ge;
+      st = graph_for(s, batch, &ge);
+      if (st != NMHD_OK) return st;
+      const int slot = next_slot;
+      next_slot ^= 1;
+      NMHD_CUDA(s, cudaGraphLaunch(ge, s->stream));
+      NMHD_CUDA(s, cudaMemcpyAsync(&s->hctl[slot], s->ctl, sizeof(StepCtl), cudaMemcpyDeviceToHost, s->stream));
+      NMHD_CUDA(s, cudaEventRecord(s->batch_done[slot], s->stream));
+      queue[(head + queued) % 2] = slot;
+      ++queued;
+      if (left > 0) left -= batch;
+    }
+    if (queued == 0) { result = NMHD_STEP_LIMIT; break; }
+    const int slot = queue[head];
+    head = (head + 1) % 2;
+    --queued;
+    NMHD_CUDA(s, cudaEventSynchronize(s->batch_done[slot]));
+    h = s->hctl[slot];
     if (h.status) {
       result = fail(s, NMHD_ERR_NUMERICAL,
                     (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
@@ -415,8 +443,23 @@ nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limi
       if (el > wallclock_limit) { result = NMHD_TIMEOUT; break; }
     }
   }
+  // a batch still in flight ran after the goal or the error: its kernels
+  // returned at once and the clock read above is final
+  NMHD_CUDA(s, cudaStreamSynchronize(s->stream));
   if (steps_done) *steps_done = h.generation - gen0;
   return result;
+}
+
+nmhd_status nmhd_prepare(nmhd_solver *s, int64_t max_steps) {
+  if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
+  if (s->cfg.parallel_size_y > 1)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "a radial slab steps through nmhd_halo_pack/unpack and nmhd_step_stages");
+  cudaGraphExec_t ge;
+  const int first = max_steps > 0 && max_steps < kStepBatch ? (int)max_steps : kStepBatch;
+  nmhd_status st = graph_for(s, first, &ge);
+  if (st == NMHD_OK && max_steps > kStepBatch && max_steps % kStepBatch)
+    st = graph_for(s, (int)(max_steps % kStepBatch), &ge);
+  return st;
 }
 
 double nmhd_current_time(const nmhd_solver *s) {

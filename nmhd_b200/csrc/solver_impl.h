@@ -23,6 +23,10 @@ struct nmhd_solver {
   int variant = 2;         // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks
   nmhd::TileShape shape = {8, 16};
   std::map<int, cudaGraphExec_t> graphs;
+  // Pinned copies of the control block after each of the (at most two) step
+  // batches in flight in nmhd_proceed, and the events that mark them.
+  nmhd::StepCtl *hctl = nullptr;
+  cudaEvent_t batch_done[2] = {nullptr, nullptr};
   std::string err;
   void *adjoint = nullptr;  // differentiation workspace (adjoint.cu), allocated on first use
 };

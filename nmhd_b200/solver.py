@@ -187,6 +187,11 @@ class MHDSolver:
         _check(self._L, self._h, code)
         return code == _lib.GOAL_REACHED
 
+    def prepare(self, max_steps=0):
+        """Build the CUDA graphs a later proceed(..., max_steps) launches,
+        without running them (nmhd_prepare)."""
+        _check(self._L, self._h, self._L.nmhd_prepare(self._h, int(max_steps)))
+
     def step(self, nsteps):
         """Advance exactly ``nsteps`` steps (no goal time); returns steps done."""
         self.proceed(math.inf, -1.0, nsteps)

@@ -112,3 +112,19 @@ def test_hlld_consistency_and_mirror():
         fb = oracle.hlld(g, -bx, m2).astype(np.float64)
         sign = np.array([-1, 1, -1, -1, -1, -1, -1])
         assert np.allclose(fa, sign * fb, rtol=1e-4, atol=1e-5)
+
+
+@pytest.mark.parametrize("name,nr,k,nz,q,beta", [("shear64x32x32_q12", 32, 2, 32, 1.2, 1e2),
+                                                 ("shear144x48x32_q18", 48, 3, 32, 1.8, 1e4)])
+def test_oracle_matches_reference_at_ensemble_q_extremes(name, nr, k, nz, q, beta):
+    """The reference built with kDifferentialRotationIndex 1.2 and 1.8 (the
+    ends of the batched ensemble's q range) equals the restatement with that
+    q, at the ends of the ensemble's beta range."""
+    if oracle.ref_binary(name) is None:
+        pytest.skip(f"reference binary ref_{name} not built")
+    cfg, s = shearing_box(n_radial=nr, n_azimuthal=k * nr, n_vertical=nz, l_radial=1.0,
+                          l_azimuthal=float(k), l_vertical=1.0, q=q, beta=beta, seed=77)
+    ref, times, _ = oracle.run_ref(name, s, 15)
+    r = oracle.proceed(cfg, s, 15)
+    assert np.array_equal(ref, r["state"])
+    assert np.array_equal(times, r["times"])
