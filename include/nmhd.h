@@ -179,8 +179,11 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * default): per-cell kernels on 32x4x2 blocks; variant 3: the variant-2
  * kernels as a pipeline over chunks of z_chunk planes, so each chunk's face
  * fluxes are read back from L2 (nmhd_profile then times each whole stage as
- * its flux class).  tile_rows is used by variant 0 only, z_chunk by variants
- * 0 and 3.  Every variant gives bitwise identical results. */
+ * its flux class); variant 4: the variant-2 flux kernel, then constrained
+ * transport and the conserved update fused in one kernel per stage (corner
+ * EMFs and new face B of a 32x4x2 tile in shared memory).  tile_rows is used
+ * by variant 0 only, z_chunk by variants 0 and 3.  Every variant gives
+ * bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);
 /* The solver's kernel selection (any pointer may be NULL). */
 nmhd_status nmhd_get_kernel(const nmhd_solver *s, int *variant, int *tile_rows, int *z_chunk);

@@ -10,8 +10,11 @@
 //               (:762-835), primitive recovery (:779-795), the Kepler kick
 //               (:837-848), and in the final stage the CFL reduction and clock
 //               update (:496-521, 870-901, 981).
+//  k_cell_epilogue  (variant 4) k_cell_ct and k_cell_prim fused: one pass per
+//               tile with the corner EMFs and new face B in shared memory
+//               (cell_epilogue.cuh).
 // The per-cell work lives in cell_ops.cuh, shared with the batch kernels.
-#include "cell_ops.cuh"
+#include "cell_epilogue.cuh"
 
 // Resident CTAs per SM asked of the compiler (register budget) for the two
 // update kernels, both bound by memory latency: measured on the 128x256x64
@@ -30,6 +33,10 @@
 #endif
 #ifndef NMHD_PRIM_MIN_BLOCKS
 #define NMHD_PRIM_MIN_BLOCKS (kPow2 ? 6 : 4)
+#endif
+// The fused epilogue holds 38.7 KB of shared memory per CTA (5 CTAs/SM).
+#ifndef NMHD_EPI_MIN_BLOCKS
+#define NMHD_EPI_MIN_BLOCKS 5
 #endif
 
 namespace nmhd {
@@ -102,6 +109,25 @@ __global__ void __launch_bounds__(kThreads, NMHD_PRIM_MIN_BLOCKS) k_cell_prim(Gr
   if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, red);
 }
 
+// Constrained transport and conserved update of one stage in one pass
+// (variant 4); ntiles: the CTAs of this launch (the last one to finish the
+// final stage advances the clock).
+template <bool kPow2>
+__global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
+    k_cell_epilogue(GridParams g, StepCtl *ctl, float *w0, float *w1, float *wp, const float *__restrict__ flux,
+                    float *dt_hist, int in_sel, int out_sel, int half, int final_stage, unsigned ntiles) {
+  __shared__ epi::Smem s;
+  if (ctl->done) return;
+  float dt = step_dt(ctl, nullptr);
+  if (half) dt = dt / 2.0f;
+  const float *win = pick(ctl, in_sel, w0, w1, wp), *wb = pick(ctl, 0, w0, w1, wp);
+  float *wo = const_cast<float *>(pick(ctl, out_sel, w0, w1, wp));
+  int bad = 0;
+  const float tcfl = epi::tile_epilogue<kPow2>(s, g, win, wb, wo, flux, blockIdx.x * BX, blockIdx.y * BY,
+                                               blockIdx.z * BZ, dt, final_stage != 0, &bad);
+  if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, s.red);
+}
+
 dim3 cell_grid(const GridParams &g, int nz) {
   return dim3((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (nz + BZ - 1) / BZ);
 }
@@ -134,6 +160,18 @@ void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1,
   else
     update_range<false>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, 0, g.sz, ntiles,
                         true, true, st);
+}
+
+void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                              float *dt_hist, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
+  const dim3 grid = cell_grid(g, g.sz), blk(BX, BY, BZ);
+  const unsigned ntiles = grid.x * grid.y * grid.z;
+  if (g.pow2_spacing)
+    k_cell_epilogue<true><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
+                                                final_stage, ntiles);
+  else
+    k_cell_epilogue<false><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
+                                                 final_stage, ntiles);
 }
 
 // One RK stage as a z-chunked pipeline (variant 3): chunk c of zc planes is

@@ -17,13 +17,13 @@
 namespace nmhd {
 
 // Minbee limiter: src/library/mhd_solver.inlrb:140-145.
-__device__ __forceinline__ float absolute_smaller(float a, float b) {
+__host__ __device__ __forceinline__ float absolute_smaller(float a, float b) {
   return a * b <= 0.0f ? 0.0f : (fabsf(a) < fabsf(b) ? a : b);
 }
 
 // 4-cell MUSCL reconstruction at the face between x1 and x2:
 // src/library/mhd_solver.inlrb:147-155.
-__device__ __forceinline__ void reconstruct4(float x0, float x1, float x2, float x3, float &left,
+__host__ __device__ __forceinline__ void reconstruct4(float x0, float x1, float x2, float x3, float &left,
                                              float &right) {
   const float d01 = x1 - x0;
   const float d12 = x2 - x1;
@@ -48,7 +48,7 @@ struct HlldIn {
   float dl, dr, ul, ur, vl, vr, wl, wr, pl, pr, byl, byr, bzl, bzr;
 };
 
-__device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, const HlldIn &s,
+__host__ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, const HlldIn &s,
                                           float f[7]) {
   const float TINY = 1.0e-10f;
   const float dens_L = s.dl, dens_R = s.dr, velx_L = s.ul, velx_R = s.ur;
@@ -112,29 +112,13 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
 #endif
 
   const float sLm = S_L - S_M, sRm = S_R - S_M;
-  const float dens_L_s = dens_L * sLv / sLm;
-  const float dnL = dens_L * sLv * sLm - B2x + TINY;
-  const float vely_L_s = vely_L - Bx * By_L * (S_M - velx_L) / dnL;
-  const float velz_L_s = velz_L - Bx * Bz_L * (S_M - velx_L) / dnL;
-  const float qL = dens_L * (sLv * sLv) - B2x;
-  const float By_L_s = By_L * qL / dnL;
-  const float Bz_L_s = Bz_L * qL / dnL;
-
-  const float dens_R_s = dens_R * sRv / sRm;
-  const float dnR = dens_R * sRv * sRm - B2x + TINY;
-  const float vely_R_s = vely_R - Bx * By_R * (S_M - velx_R) / dnR;
-  const float velz_R_s = velz_R - Bx * Bz_R * (S_M - velx_R) / dnR;
-  const float qR = dens_R * (sRv * sRv) - B2x;
-  const float By_R_s = By_R * qR / dnR;
-  const float Bz_R_s = Bz_R * qR / dnR;
-
-  const float vB_L = velx_L * Bx + vely_L * By_L + velz_L * Bz_L;
-  const float vB_L_s = S_M * Bx + vely_L_s * By_L_s + velz_L_s * Bz_L_s;
-  const float etot_L_s = (sLv * etot_L - pT_L * velx_L + pT_s * S_M + Bx * (vB_L - vB_L_s)) / sLm;
-  const float vB_R = velx_R * Bx + vely_R * By_R + velz_R * Bz_R;
-  const float vB_R_s = S_M * Bx + vely_R_s * By_R_s + velz_R_s * Bz_R_s;
-  const float etot_R_s = (sRv * etot_R - pT_R * velx_R + pT_s * S_M + Bx * (vB_R - vB_R_s)) / sRm;
-
+  // Single-star densities of both sides fix the Alfven speeds S_L*, S_R*
+  // and with them the fan region; everything else of the star states is
+  // computed below only for the side(s) the region's formula reads.
+  const float dsL = dens_L * sLv;
+  const float dsR = dens_R * sRv;
+  const float dens_L_s = dsL / sLm;
+  const float dens_R_s = dsR / sRm;
   const float sdL = sqrtf(dens_L_s), sdR = sqrtf(dens_R_s);
   const float S_L_s = S_M - fabsf(Bx) / sdL;
   const float S_R_s = S_M + fabsf(Bx) / sdR;
@@ -158,10 +142,10 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
   const float bz_ = left ? Bz_L : Bz_R;
   const float e_ = left ? etot_L : etot_R;
   const float pT_ = left ? pT_L : pT_R;
-  const float vB_ = left ? vB_L : vB_R;
   const float mx_ = left ? momx_L : momx_R;
   const float my_ = left ? momy_L : momy_R;
   const float mz_ = left ? momz_L : momz_R;
+  const float vB_ = u_ * Bx + v_ * by_ + w_ * bz_;
 
   const float F0 = d_ * u_;
   const float F1 = mx_ * u_ + pT_ - B2x;
@@ -174,13 +158,20 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
     f[0] = F0; f[1] = F1; f[2] = F2; f[3] = F3; f[4] = F4; f[5] = F5; f[6] = F6;
     return;
   }
+  // single-star state of the selected side (hlld.inl:146-164, the same
+  // expressions for L and R)
   const float S_ = left ? S_L : S_R;
+  const float sv_ = left ? sLv : sRv;
+  const float sm_ = left ? sLm : sRm;
   const float ds_ = left ? dens_L_s : dens_R_s;
-  const float vs_ = left ? vely_L_s : vely_R_s;
-  const float ws_ = left ? velz_L_s : velz_R_s;
-  const float bys_ = left ? By_L_s : By_R_s;
-  const float bzs_ = left ? Bz_L_s : Bz_R_s;
-  const float es_ = left ? etot_L_s : etot_R_s;
+  const float dn_ = (left ? dsL : dsR) * sm_ - B2x + TINY;
+  const float vs_ = v_ - Bx * by_ * (S_M - u_) / dn_;
+  const float ws_ = w_ - Bx * bz_ * (S_M - u_) / dn_;
+  const float q_ = d_ * (sv_ * sv_) - B2x;
+  const float bys_ = by_ * q_ / dn_;
+  const float bzs_ = bz_ * q_ / dn_;
+  const float vBs_ = S_M * Bx + vs_ * bys_ + ws_ * bzs_;
+  const float es_ = (sv_ * e_ - pT_ * u_ + pT_s * S_M + Bx * (vB_ - vBs_)) / sm_;
   // U* of the selected side
   const float Us1 = ds_ * S_M, Us2 = ds_ * vs_, Us3 = ds_ * ws_;
   if (region == 1 || region == 4) {
@@ -193,7 +184,21 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
     f[6] = F6 + S_ * bzs_ - S_ * bz_;
     return;
   }
-  // double-star states (regions 2 and 3)
+  // regions 2 and 3: the other side's transverse star state too
+  const float uo = left ? velx_R : velx_L;
+  const float dno = (left ? dsR : dsL) * (left ? sRm : sLm) - B2x + TINY;
+  const float svo = left ? sRv : sLv;
+  const float qo = (left ? dens_R : dens_L) * (svo * svo) - B2x;
+  const float byo = left ? By_R : By_L, bzo = left ? Bz_R : Bz_L;
+  const float vso = (left ? vely_R : vely_L) - Bx * byo * (S_M - uo) / dno;
+  const float wso = (left ? velz_R : velz_L) - Bx * bzo * (S_M - uo) / dno;
+  const float byso = byo * qo / dno;
+  const float bzso = bzo * qo / dno;
+  const float vely_L_s = left ? vs_ : vso, vely_R_s = left ? vso : vs_;
+  const float velz_L_s = left ? ws_ : wso, velz_R_s = left ? wso : ws_;
+  const float By_L_s = left ? bys_ : byso, By_R_s = left ? byso : bys_;
+  const float Bz_L_s = left ? bzs_ : bzso, Bz_R_s = left ? bzso : bzs_;
+  // double-star states (hlld.inl:172-193)
   const float fr = 1.0f / (sdL + sdR);
   const float vely_ss = fr * (sdL * vely_L_s + sdR * vely_R_s + (By_R_s - By_L_s) * signBx);
   const float velz_ss = fr * (sdL * velz_L_s + sdR * velz_R_s + (Bz_R_s - Bz_L_s) * signBx);
@@ -202,8 +207,7 @@ __device__ __forceinline__ void hlld_flux(const float gamma, const float Bx, con
   const float Bz_ss = fr * (sdL * Bz_R_s + sdR * Bz_L_s + sdLR * (velz_R_s - velz_L_s) * signBx);
   const float vB_ss = S_M * Bx + vely_ss * By_ss + velz_ss * Bz_ss;
   const float Sss = left ? S_L_s : S_R_s;
-  const float ess = left ? (etot_L_s - sdL * (vB_L_s - vB_ss) * signBx)
-                         : (etot_R_s + sdR * (vB_R_s - vB_ss) * signBx);
+  const float ess = left ? (es_ - sdL * (vBs_ - vB_ss) * signBx) : (es_ + sdR * (vBs_ - vB_ss) * signBx);
   const float Sd = Sss - S_;
   f[0] = F0 + Sss * ds_ - Sd * ds_ - S_ * d_;
   f[1] = F1 + Sss * Us1 - Sd * Us1 - S_ * mx_;

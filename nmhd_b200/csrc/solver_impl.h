@@ -20,7 +20,9 @@ struct nmhd_solver {
   nmhd::StepCtl *ctl = nullptr;
   double *diag = nullptr;
   bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
-  int variant = 2;         // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks
+  // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks,
+  // 3: variant 2 as a z-chunk pipeline, 4: variant 2 with the fused epilogue
+  int variant = 2;
   nmhd::TileShape shape = {8, 16};
   std::map<int, cudaGraphExec_t> graphs;
   // Pinned copies of the control block after each of the (at most two) step

@@ -109,6 +109,11 @@ void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, f
 void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                         float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
                         cudaStream_t stream);
+// The update of a stage in one kernel (variant 4): constrained transport and
+// conserved update fused, corner EMFs and new face B in shared memory.
+void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                              float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                              cudaStream_t stream);
 // One RK stage with the per-cell kernels as a pipeline over chunks of z_chunk
 // planes (variant 3), so each chunk's face fluxes are consumed from L2.
 void launch_cell_stage_chunked(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,

@@ -116,7 +116,7 @@ def test_gpu_large_box_matches_oracle_and_keeps_div_b(gpu):
 
 
 @pytest.mark.parametrize("case", ["ot_m2", "shear_m2", "shear_m4_mz2"])
-@pytest.mark.parametrize("variant", [2, 0])
+@pytest.mark.parametrize("variant", [2, 0, 4])
 def test_per_stage_margin_fill_matches_oracle(gpu, case, variant):
     """NMHD_FLAG_HALO_PER_STAGE: the predictor's margins refilled before the
     second stage; bitwise the oracle's mode, for the default and the tiled
@@ -262,21 +262,45 @@ def test_goal_time_semantics(gpu):
 
 @pytest.mark.parametrize("variant,rows,zc", [(2, 8, 0), (1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5),
                                              (0, 8, 3), (3, 8, 1), (3, 8, 2), (3, 8, 3), (3, 8, 4),
-                                             (3, 8, 64)])
+                                             (3, 8, 64), (4, 8, 0)])
 @pytest.mark.parametrize("case", ["ot_ragged", "shear_ragged", "shear_mz"])
 def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
     """Every kernel variant and tile shape, on boxes whose sizes are not
     multiples of the tile (partial tiles in x, y and z)."""
+    _variant_case(variant, rows, zc, case)
+
+
+@pytest.mark.parametrize("variant", [2, 4])
+@pytest.mark.parametrize("case", ["tiny", "ot_2d", "euler_order1"])
+def test_cell_kernels_on_tiny_flat_and_first_order_boxes(gpu, variant, case):
+    """The per-cell kernels and the fused epilogue (whose shared-memory tile
+    with its halo is larger than these boxes: every halo entry wraps
+    periodically) on a 5 x 9 x 1 box, a single-plane box, and Euler stepping
+    with piecewise-constant reconstruction."""
+    _variant_case(variant, 8, 0, case)
+
+
+def _variant_case(variant, rows, zc, case):
     if case == "ot_ragged":
         cfg, s = orszag_tang_3d(40, ny=20, nz=13)
         steps = 12
     elif case == "shear_ragged":
         cfg, s = shearing_box(n_radial=12, n_azimuthal=48, n_vertical=7, l_azimuthal=2.0, seed=5)
         steps = 12
-    else:
+    elif case == "shear_mz":
         cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=6)
         cfg.margin_z, cfg.size_z = 4, 16
         s = np.concatenate([s[:, -4:], s, s[:, :4]], axis=1)
+        steps = 10
+    elif case == "tiny":  # boxes smaller than a tile and its halo in every axis
+        cfg, s = shearing_box(n_radial=3, n_azimuthal=5, n_vertical=1, l_azimuthal=2.0, seed=8, margin=3)
+        steps = 8
+    elif case == "ot_2d":
+        cfg, s = orszag_tang_3d(40, ny=24, nz=1)
+        steps = 10
+    else:  # Euler stepping with piecewise-constant reconstruction
+        cfg, s = shearing_box(n_radial=12, n_azimuthal=40, n_vertical=5, l_azimuthal=2.0, seed=10)
+        cfg.time_order, cfg.space_order = 1, 1
         steps = 10
     o = oracle.proceed(cfg, s, steps)
     with MHDSolver(cfg) as sol:
@@ -367,7 +391,8 @@ def test_monitor_hook_runs_before_every_step(gpu):
         assert sol.calls == sol.generation()
 
 
-@pytest.mark.parametrize("variant,zc,mz,expect", [(2, 0, 0, 8), (2, 0, 2, 9), (0, 0, 0, 6), (3, 4, 0, 2 + 2 * 3 * 2)])
+@pytest.mark.parametrize("variant,zc,mz,expect", [(2, 0, 0, 8), (2, 0, 2, 9), (0, 0, 0, 6), (3, 4, 0, 2 + 2 * 3 * 2),
+                                                 (4, 0, 0, 6), (4, 0, 2, 7)])
 def test_profile_counts_kernel_launches(gpu, variant, zc, mz, expect):
     """nmhd_profile reports each class's kernel launches per step (the bench's
     gpu_launches): fill (Y, Z), margin CFL, flux and update of each stage;
