@@ -407,12 +407,19 @@ def run_gpu_arm(args):
         peak, peak_kind = load_peaks()
         # the RK2 step is the unit: 160 algorithmic bytes per cell-update
         achieved = BYTES_PER_CELL_UPDATE * cells / (kernel_ms_step * 1e-3) / 1e9
-        traffic, winst = None, None
+        # DRAM bytes and warp instructions per step of the chosen kernel
+        # variant, from an ncu capture of the same box (not measured in this
+        # run; the file says which launches)
+        traffic, winst, tsrc = None, None, None
         tf = os.path.join(ROOT, "profiles", "traffic_" + wl + ".json")
         if os.path.exists(tf):
             tj = json.load(open(tf))
-            traffic = tj.get("dram_bytes_per_step")
-            winst = tj.get("warp_instructions_per_step")
+            tv = tj.get("by_variant", {}).get(str(choice["variant"]))
+            if tv:
+                traffic = tv.get("dram_bytes_per_step")
+                winst = tv.get("warp_instructions_per_step")
+                tsrc = "profiles/traffic_%s.json (ncu capture of kernel variant %s): %s" % (
+                    wl, choice["variant"], tj.get("source", ""))
         launches_per_step = sum(k for _, k in prof.values())
         line = {
             "metric": "Mcell-updates/s", "value": value, "unit": "Mcell-updates/s",
@@ -425,7 +432,7 @@ def run_gpu_arm(args):
                        "kernel": choice},
             "e2e": e2e,
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": traffic,
+                         "frac": achieved / peak, "traffic": traffic, "traffic_source": tsrc,
                          "peak_kind": peak_kind,
                          "unit_of_work": "one RK2 step (all kernels); 160 B per cell-update",
                          "kernels_ms_per_step": {k: round(t, 5) for k, (t, _) in prof.items()}},

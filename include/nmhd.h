@@ -175,13 +175,14 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * src/application/optimize_mhd, kernel_call() in src/library/mhd_solver.inlrb:24-33).
  * variant 0: z-marching tiled kernels (32 x tile_rows cells per CTA,
  * tile_rows in {4, 8, 16}, z_chunk planes per CTA, 0 = whole height);
- * variant 1: per-cell flux and update kernels on 1-D blocks; variant 2 (the
- * default): per-cell kernels on 32x4x2 blocks; variant 3: the variant-2
+ * variant 1: per-cell flux and update kernels on 1-D blocks; variant 2:
+ * per-cell kernels on 32x4x2 blocks; variant 3: the variant-2
  * kernels as a pipeline over chunks of z_chunk planes, so each chunk's face
  * fluxes are read back from L2 (nmhd_profile then times each whole stage as
- * its flux class); variant 4: the variant-2 flux kernel, then constrained
- * transport and the conserved update fused in one kernel per stage (corner
- * EMFs and new face B of a 32x4x2 tile in shared memory).  tile_rows is used
+ * its flux class); variant 4 (the default): the variant-2 flux kernel, then
+ * constrained transport and the conserved update fused in one kernel per
+ * stage (corner EMFs and new face B of a 32x4x2 tile in shared memory, its
+ * inputs staged by tensor copies).  tile_rows is used
  * by variant 0 only, z_chunk by variants 0 and 3.  Every variant gives
  * bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);

@@ -285,12 +285,12 @@ void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl)
   }
   if (s->cfg.time_order == 1) {
     nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, st);
-    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, nullptr, st);
   } else {
     nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, st);
-    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, nullptr, st);
     nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, st);
-    nmhd::launch_cell_update(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, nullptr, st);
   }
   w.parity ^= 1;
 }

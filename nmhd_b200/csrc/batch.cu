@@ -364,6 +364,7 @@ nmhd_status batch_graph(nmhd_batch *b, int k, cudaGraphExec_t *out) {
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return bfail(b, NMHD_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
   b->graphs[k] = ge;
+  BATCH_CUDA(b, cudaGraphUpload(ge, b->stream));  // the first launch then pays no upload
   *out = ge;
   return NMHD_OK;
 }

@@ -18,6 +18,8 @@
 // per-axis offset tables, so partial tiles and tiny boxes need no special
 // path (halo entries beyond a partial tile are computed and not used).
 #pragma once
+#include <cuda.h>
+
 #include "cell_ops.cuh"
 
 namespace nmhd {
@@ -67,25 +69,44 @@ using BZs = Staged<32, 4, 3, 0, 0, 0>;
 // Shared memory of one tile.  The velocity region holds the new face B once
 // the corner EMFs are computed; wbf holds the face B of the step's state at
 // the same faces.
-struct __align__(16) Smem {
-  int gx[34], gy[6], gz[4];  // wrapped global offsets of x0-1+i, (y0-1+j)*Sx, (z0-1+k)*Sx*Sy
-  float vel[3 * VelBox::N];
-  float bf[XYF::N + YXF::N + XZF::N + ZXF::N + YZF::N + ZYF::N];
-  float edge[2 * ZEdge::N + 2 * YEdge::N + 2 * XEdge::N];
-  float wbf[BXs::N + BYs::N + BZs::N];
-  float red[kThreads / 32];
-};
-static_assert(3 * VelBox::N >= BXs::N + BYs::N + BZs::N, "face B region");
-static_assert(sizeof(int) * 44 % 16 == 0 && VelBox::N % 4 == 0 && XYF::N % 4 == 0 && YXF::N % 4 == 0 &&
-                  XZF::N % 4 == 0 && ZXF::N % 4 == 0 && YZF::N % 4 == 0 && ZYF::N % 4 == 0 &&
-                  (2 * ZEdge::N + 2 * YEdge::N + 2 * XEdge::N) % 4 == 0 && BXs::N % 4 == 0 && BYs::N % 4 == 0,
-              "16-byte aligned staged rows");
-
-constexpr int kXY = 0, kYX = kXY + XYF::N, kXZ = kYX + YXF::N, kZX = kXZ + XZF::N, kYZ = kZX + ZXF::N,
-              kZY = kYZ + YZF::N;
+// Staged and computed boxes in shared memory, each region starting on a
+// 128-byte boundary (the tensor-memory-access copies below write whole boxes
+// there).
+constexpr int r32(int n) { return (n + 31) / 32 * 32; }
+constexpr int kXY = 0, kYX = kXY + r32(XYF::N), kXZ = kYX + r32(YXF::N), kZX = kXZ + r32(XZF::N),
+              kYZ = kZX + r32(ZXF::N), kZY = kYZ + r32(YZF::N), kBF = kZY + r32(ZYF::N);
 constexpr int eXY = 0, eYX = ZEdge::N, eXZ = 2 * ZEdge::N, eZX = eXZ + YEdge::N, eYZ = eZX + YEdge::N,
-              eZY = eYZ + XEdge::N;
-constexpr int fBX = 0, fBY = BXs::N, fBZ = BXs::N + BYs::N;
+              eZY = eYZ + XEdge::N, kEdge = r32(eZY + XEdge::N);
+constexpr int fBX = 0, fBY = r32(BXs::N), fBZ = fBY + r32(BYs::N), kWB = fBZ + r32(BZs::N);
+
+// Shared memory of one tile.  The velocity region holds the new face B once
+// the corner EMFs are computed; wbf holds the face B of the step's state at
+// the same faces.
+struct __align__(128) Smem {
+  float vel[3 * VelBox::N];
+  float bf[kBF];
+  float edge[kEdge];
+  float wbf[kWB];
+  int gx[34], gy[6], gz[4];  // wrapped global offsets of x0-1+i, (y0-1+j)*Sx, (z0-1+k)*Sx*Sy
+  float red[kThreads / 32];
+  unsigned long long mbar;   // completion of the tile's tensor copies
+};
+static_assert(3 * VelBox::N >= kWB, "face B region");
+static_assert((3 * VelBox::N) % 32 == 0 && kBF % 32 == 0 && kEdge % 32 == 0, "128-byte aligned regions");
+// bytes the tensor copies of one tile deliver
+constexpr unsigned kTileTxBytes =
+    4u * (3 * VelBox::N + XYF::N + YXF::N + XZF::N + ZXF::N + YZF::N + ZYF::N + BXs::N + BYs::N + BZs::N);
+
+// Tensor maps (cuTensorMapEncodeTiled, 4-D: x, y, z, field) of the staged
+// boxes: per state buffer (0 w0, 1 w1, 2 predictor) the velocity box over
+// fields 1-3 and the three face-B boxes; the six B-flux boxes of the flux
+// scratch.  `enabled` is 0 where they cannot be made (rows not 16-byte
+// multiples); tiles then stage with cp.async.
+struct EpiMaps {
+  CUtensorMap vel[3], bx[3], by[3], bz[3];
+  CUtensorMap xy, yx, xz, zx, yz, zy;
+  int enabled;
+};
 
 // Global offset of tile-local cell (a, b, c) through the wrapped tables.
 __device__ __forceinline__ int goff(const Smem &s, int a, int b, int c) {
@@ -102,6 +123,40 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // 16-byte asynchronous copy (both addresses 16-byte aligned), cached in L2 only.
 __device__ __forceinline__ void cp_async16(unsigned dst, const float *src) {
   asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(dst), "l"(src) : "memory");
+}
+
+// Tensor copy of box B at tile origin (x0, y0, z0), fields f0.., into shared
+// address dst, completing on the tile's mbarrier (cp.async.bulk.tensor; the
+// x coordinate x0 + OI - XO is a multiple of 4 floats, 16 bytes).
+template <class B>
+__device__ __forceinline__ void tma_box(unsigned dst, const CUtensorMap *map, int x0, int y0, int z0, int f0,
+                                        unsigned mbar) {
+  asm volatile(
+      "cp.async.bulk.tensor.4d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3, %4, "
+      "%5}], [%6];" ::"r"(dst),
+      "l"(reinterpret_cast<unsigned long long>(map)), "r"(x0 + B::OI - B::XO), "r"(y0 + B::OJ), "r"(z0 + B::OK),
+      "r"(f0), "r"(mbar)
+      : "memory");
+}
+
+__device__ __forceinline__ bool mbar_try_wait(unsigned mbar, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+      : "=r"(ok)
+      : "r"(mbar), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+
+// Bounded wait for phase 0 of the tile's mbarrier: true when the copies
+// landed within kTmaWaitTries polls (each poll may itself suspend the thread
+// for a while).
+constexpr int kTmaWaitTries = 1 << 20;
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned mbar) {
+  for (int i = 0; i < kTmaWaitTries; ++i)
+    if (mbar_try_wait(mbar, 0)) return true;
+  return false;
 }
 
 // Copy box B of global field src (and, for F > 1 fields, the fields at
@@ -360,10 +415,11 @@ __device__ __forceinline__ float finish_cell(const Smem &s, const GridParams &g,
 // calls it.  win: stage input (velocities), wb: state at the start of the
 // step, wo: stage output.  Returns the thread's CFL time (inf if none).
 template <bool kPow2>
-__device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, const float *__restrict__ win,
+__device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, const EpiMaps &maps, int in_buf,
+                                               int base_buf, const float *__restrict__ win,
                                                const float *__restrict__ wb, float *__restrict__ wo,
                                                const float *__restrict__ flux, int x0, int y0, int z0, float dt,
-                                               bool final_stage, int *bad) {
+                                               bool final_stage, int *bad, int *timed_out) {
   const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
   const size_t N = (size_t)g.n;
   {
@@ -378,28 +434,72 @@ __device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, con
       asm volatile("prefetch.global.L2 [%0];" ::"l"(p));
     }
   }
-  if (tid < 34) s.gx[tid] = wrap_any(x0 - 1 + tid, g.sx);
-  else if (tid < 40) s.gy[tid - 34] = wrap_any(y0 - 1 + (tid - 34), g.sy) * g.sx;
-  else if (tid < 44) s.gz[tid - 40] = wrap_any(z0 - 1 + (tid - 40), g.sz) * g.sx * g.sy;
+  const unsigned vs = (unsigned)__cvta_generic_to_shared(s.vel), bs = (unsigned)__cvta_generic_to_shared(s.bf),
+                 ws = (unsigned)__cvta_generic_to_shared(s.wbf),
+                 mb = (unsigned)__cvta_generic_to_shared(&s.mbar);
+  // Tiles whose staged boxes (x0-4..x0+35, y0-1..y0+4, z0-1..z0+2) lie inside
+  // the box need no periodic wrap: one thread stages all of them with ten
+  // tensor copies.  The others stage entry by entry through the wrapped
+  // offset tables (16-byte row chunks when only y or z wraps).
+  const bool tma = maps.enabled && x0 >= 4 && x0 + 36 <= g.sx && y0 >= 1 && y0 + 5 <= g.sy && z0 >= 1 &&
+                   z0 + 3 <= g.sz;
+  if (tma) {
+    if (tid == 0) {
+      asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(mb) : "memory");
+      asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+      asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+      asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(kTileTxBytes)
+                   : "memory");
+      tma_box<VelBox>(vs, &maps.vel[in_buf], x0, y0, z0, 1, mb);
+      tma_box<XYF>(bs + 4 * kXY, &maps.xy, x0, y0, z0, 5, mb);
+      tma_box<YXF>(bs + 4 * kYX, &maps.yx, x0, y0, z0, 13, mb);
+      tma_box<XZF>(bs + 4 * kXZ, &maps.xz, x0, y0, z0, 6, mb);
+      tma_box<ZXF>(bs + 4 * kZX, &maps.zx, x0, y0, z0, 19, mb);
+      tma_box<YZF>(bs + 4 * kYZ, &maps.yz, x0, y0, z0, 12, mb);
+      tma_box<ZYF>(bs + 4 * kZY, &maps.zy, x0, y0, z0, 20, mb);
+      tma_box<BXs>(ws + 4 * fBX, &maps.bx[base_buf], x0, y0, z0, 5, mb);
+      tma_box<BYs>(ws + 4 * fBY, &maps.by[base_buf], x0, y0, z0, 6, mb);
+      tma_box<BZs>(ws + 4 * fBZ, &maps.bz[base_buf], x0, y0, z0, 7, mb);
+    }
+  } else {
+    if (tid < 34) s.gx[tid] = wrap_any(x0 - 1 + tid, g.sx);
+    else if (tid < 40) s.gy[tid - 34] = wrap_any(y0 - 1 + (tid - 34), g.sy) * g.sx;
+    else if (tid < 44) s.gz[tid - 40] = wrap_any(z0 - 1 + (tid - 40), g.sz) * g.sx * g.sy;
+  }
   __syncthreads();
   const int warp = tid >> 5, lane = tid & 31;
-  // whole 16-byte row chunks: no periodic wrap in x (the padded rows span
-  // x0 - 4 .. x0 + 35) and 16-byte aligned rows
-  const bool vec = x0 >= 1 && x0 + 32 < g.sx && (g.sx & 3) == 0;
-  const unsigned vs = (unsigned)__cvta_generic_to_shared(s.vel), bs = (unsigned)__cvta_generic_to_shared(s.bf),
-                 ws = (unsigned)__cvta_generic_to_shared(s.wbf);
-  load_box<VelBox, 3>(s, vs, win + N, N, x0, vec, tid);
-  load_box<XYF, 1>(s, bs + 4 * kXY, flux + 5 * N, N, x0, vec, tid);
-  load_box<YXF, 1>(s, bs + 4 * kYX, flux + 13 * N, N, x0, vec, tid);
-  load_box<XZF, 1>(s, bs + 4 * kXZ, flux + 6 * N, N, x0, vec, tid);
-  load_box<ZXF, 1>(s, bs + 4 * kZX, flux + 19 * N, N, x0, vec, tid);
-  load_box<YZF, 1>(s, bs + 4 * kYZ, flux + 12 * N, N, x0, vec, tid);
-  load_box<ZYF, 1>(s, bs + 4 * kZY, flux + 20 * N, N, x0, vec, tid);
-  load_box<BXs, 1>(s, ws + 4 * fBX, wb + 5 * N, N, x0, vec, tid);
-  load_box<BYs, 1>(s, ws + 4 * fBY, wb + 6 * N, N, x0, vec, tid);
-  load_box<BZs, 1>(s, ws + 4 * fBZ, wb + 7 * N, N, x0, vec, tid);
-  cp_async_wait_all();
-  __syncthreads();
+  if (tma) {
+    // every thread waits for the copies (bounded); the outcome is made
+    // uniform over the CTA
+    const bool ok = __syncthreads_and(mbar_wait_bounded(mb));
+    if (!ok) {
+      // the copies did not land in time: flag it and wait once more (bounded)
+      // so that none is still writing when the CTA exits
+      *timed_out = 1;
+      mbar_wait_bounded(mb);
+      __syncthreads();
+      if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
+      return __uint_as_float(0x7f800000u);
+    }
+    // every thread has passed the wait: the barrier's word is released
+    if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
+  } else {
+    // whole 16-byte row chunks: no periodic wrap in x (the padded rows span
+    // x0 - 4 .. x0 + 35) and 16-byte aligned rows
+    const bool vec = x0 >= 1 && x0 + 32 < g.sx && (g.sx & 3) == 0;
+    load_box<VelBox, 3>(s, vs, win + N, N, x0, vec, tid);
+    load_box<XYF, 1>(s, bs + 4 * kXY, flux + 5 * N, N, x0, vec, tid);
+    load_box<YXF, 1>(s, bs + 4 * kYX, flux + 13 * N, N, x0, vec, tid);
+    load_box<XZF, 1>(s, bs + 4 * kXZ, flux + 6 * N, N, x0, vec, tid);
+    load_box<ZXF, 1>(s, bs + 4 * kZX, flux + 19 * N, N, x0, vec, tid);
+    load_box<YZF, 1>(s, bs + 4 * kYZ, flux + 12 * N, N, x0, vec, tid);
+    load_box<ZYF, 1>(s, bs + 4 * kZY, flux + 20 * N, N, x0, vec, tid);
+    load_box<BXs, 1>(s, ws + 4 * fBX, wb + 5 * N, N, x0, vec, tid);
+    load_box<BYs, 1>(s, ws + 4 * fBY, wb + 6 * N, N, x0, vec, tid);
+    load_box<BZs, 1>(s, ws + 4 * fBZ, wb + 7 * N, N, x0, vec, tid);
+    cp_async_wait_all();
+    __syncthreads();
+  }
   corner_emfs(s, threadIdx.x, threadIdx.y, threadIdx.z, warp, lane, tid);
   __syncthreads();
   face_b<kPow2>(s, g, threadIdx.x, threadIdx.y, threadIdx.z, warp, lane, dt);

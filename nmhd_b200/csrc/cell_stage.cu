@@ -14,6 +14,11 @@
 //               tile with the corner EMFs and new face B in shared memory
 //               (cell_epilogue.cuh).
 // The per-cell work lives in cell_ops.cuh, shared with the batch kernels.
+#include <cudaTypedefs.h>
+
+#include <cstring>
+#include <mutex>
+
 #include "cell_epilogue.cuh"
 
 // Resident CTAs per SM asked of the compiler (register budget) for the two
@@ -112,19 +117,29 @@ __global__ void __launch_bounds__(kThreads, NMHD_PRIM_MIN_BLOCKS) k_cell_prim(Gr
 // Constrained transport and conserved update of one stage in one pass
 // (variant 4); ntiles: the CTAs of this launch (the last one to finish the
 // final stage advances the clock).
+// Buffer index (0 w0, 1 w1, 2 predictor) that pick() selects.
+__device__ __forceinline__ int pick_index(const StepCtl *c, int sel) {
+  if (sel == 2) return 2;
+  return (sel == 0) == (c->parity == 0) ? 0 : 1;
+}
+
 template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
-    k_cell_epilogue(GridParams g, StepCtl *ctl, float *w0, float *w1, float *wp, const float *__restrict__ flux,
-                    float *dt_hist, int in_sel, int out_sel, int half, int final_stage, unsigned ntiles) {
+    k_cell_epilogue(const __grid_constant__ epi::EpiMaps maps, GridParams g, StepCtl *ctl, float *w0, float *w1,
+                    float *wp, const float *__restrict__ flux, float *dt_hist, int in_sel, int out_sel, int half,
+                    int final_stage, unsigned ntiles) {
   __shared__ epi::Smem s;
   if (ctl->done) return;
   float dt = step_dt(ctl, nullptr);
   if (half) dt = dt / 2.0f;
   const float *win = pick(ctl, in_sel, w0, w1, wp), *wb = pick(ctl, 0, w0, w1, wp);
   float *wo = const_cast<float *>(pick(ctl, out_sel, w0, w1, wp));
-  int bad = 0;
-  const float tcfl = epi::tile_epilogue<kPow2>(s, g, win, wb, wo, flux, blockIdx.x * BX, blockIdx.y * BY,
-                                               blockIdx.z * BZ, dt, final_stage != 0, &bad);
+  int bad = 0, timed_out = 0;
+  const float tcfl = epi::tile_epilogue<kPow2>(s, g, maps, pick_index(ctl, in_sel), pick_index(ctl, 0), win, wb, wo,
+                                               flux, blockIdx.x * BX, blockIdx.y * BY, blockIdx.z * BZ, dt,
+                                               final_stage != 0, &bad, &timed_out);
+  if (timed_out && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
+    atomicOr(&ctl->status, kStatusTimeout);
   if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, s.red);
 }
 
@@ -162,15 +177,78 @@ void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1,
                         true, true, st);
 }
 
+struct EpilogueMaps {
+  epi::EpiMaps m;
+};
+
+// Tensor maps of the fused epilogue's staged boxes for one solver's buffers
+// (cuTensorMapEncodeTiled through the runtime's driver entry point): 4-D
+// (x, y, z, field) over the 8 state fields or the 21 flux fields, box
+// extents the padded shared boxes'.  NULL where the rows are not 16-byte
+// multiples (Sx % 4 != 0) or the driver offers no encoder; the kernel then
+// stages every tile with cp.async.
+EpilogueMaps *make_epilogue_maps(const GridParams &g, float *w0, float *w1, float *wp, float *flux) {
+  if (g.sx % 4 != 0) return nullptr;
+  static PFN_cuTensorMapEncodeTiled_v12000 encode = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuTensorMapEncodeTiled", &fn, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      encode = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(fn);
+  });
+  if (!encode) return nullptr;
+  EpilogueMaps *out = new EpilogueMaps();
+  std::memset(out, 0, sizeof(*out));
+  const cuuint64_t sx = g.sx, sy = g.sy, sz = g.sz, n = (cuuint64_t)g.n;
+  bool ok = true;
+  auto make = [&](CUtensorMap *map, float *base, int nfields, int bx, int by, int bz, int bf) {
+    const cuuint64_t dims[4] = {sx, sy, sz, (cuuint64_t)nfields};
+    const cuuint64_t strides[3] = {sx * 4, sx * sy * 4, n * 4};
+    const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, (cuuint32_t)bf};
+    const cuuint32_t es[4] = {1, 1, 1, 1};
+    ok = ok && encode(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 4, base, dims, strides, box, es,
+                      CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+                      CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
+  };
+  using namespace epi;
+  float *w[3] = {w0, w1, wp};
+  for (int b = 0; b < 3; ++b) {
+    make(&out->m.vel[b], w[b], 8, VelBox::P, VelBox::NJ, VelBox::NK, 3);
+    make(&out->m.bx[b], w[b], 8, BXs::P, BXs::NJ, BXs::NK, 1);
+    make(&out->m.by[b], w[b], 8, BYs::P, BYs::NJ, BYs::NK, 1);
+    make(&out->m.bz[b], w[b], 8, BZs::P, BZs::NJ, BZs::NK, 1);
+  }
+  make(&out->m.xy, flux, kFluxFields, XYF::P, XYF::NJ, XYF::NK, 1);
+  make(&out->m.yx, flux, kFluxFields, YXF::P, YXF::NJ, YXF::NK, 1);
+  make(&out->m.xz, flux, kFluxFields, XZF::P, XZF::NJ, XZF::NK, 1);
+  make(&out->m.zx, flux, kFluxFields, ZXF::P, ZXF::NJ, ZXF::NK, 1);
+  make(&out->m.yz, flux, kFluxFields, YZF::P, YZF::NJ, YZF::NK, 1);
+  make(&out->m.zy, flux, kFluxFields, ZYF::P, ZYF::NJ, ZYF::NK, 1);
+  if (!ok) {
+    delete out;
+    return nullptr;
+  }
+  out->m.enabled = 1;
+  return out;
+}
+
+void free_epilogue_maps(EpilogueMaps *m) { delete m; }
+
 void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
-                              float *dt_hist, int in_sel, int out_sel, int half, int final_stage, cudaStream_t st) {
+                              float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
+                              const EpilogueMaps *maps, cudaStream_t st) {
   const dim3 grid = cell_grid(g, g.sz), blk(BX, BY, BZ);
   const unsigned ntiles = grid.x * grid.y * grid.z;
+  static const EpilogueMaps kNone = {};  // enabled = 0: cp.async staging only
+  const epi::EpiMaps &m = maps ? maps->m : kNone.m;
   if (g.pow2_spacing)
-    k_cell_epilogue<true><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
+    k_cell_epilogue<true><<<grid, blk, 0, st>>>(m, g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
                                                 final_stage, ntiles);
   else
-    k_cell_epilogue<false><<<grid, blk, 0, st>>>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
+    k_cell_epilogue<false><<<grid, blk, 0, st>>>(m, g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half,
                                                  final_stage, ntiles);
 }
 

@@ -163,7 +163,7 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
       nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
     if (s->variant == 4)
       nmhd::launch_cell_update_fused(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
-                                     final_stage, st);
+                                     final_stage, s->epi_maps, st);
     else
       nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                                final_stage, st);
@@ -205,6 +205,8 @@ nmhd_status graph_for(nmhd_solver *s, int steps, cudaGraphExec_t *out) {
   cudaGraphDestroy(graph);
   if (e != cudaSuccess) return cuda_fail(s, e, "cudaGraphInstantiate");
   s->graphs[steps] = exec;
+  // upload now, so that the first launch does not pay for it
+  NMHD_CUDA(s, cudaGraphUpload(exec, s->stream));
   *out = exec;
   return NMHD_OK;
 }
@@ -285,6 +287,7 @@ nmhd_status nmhd_create(const nmhd_config *cfg, nmhd_solver **out) {
     nmhd_destroy(s);
     return st;
   }
+  s->epi_maps = nmhd::make_epilogue_maps(s->g, s->w0, s->w1, s->wp, s->flux);
   apply_tuned(s);
   *out = s;
   return NMHD_OK;
@@ -295,6 +298,7 @@ void nmhd_destroy(nmhd_solver *s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   drop_graphs(s);
   nmhd_adjoint_release(s);
+  nmhd::free_epilogue_maps(s->epi_maps);
   cudaFree(s->w0);
   cudaFree(s->w1);
   cudaFree(s->wp);
@@ -437,8 +441,9 @@ nmhd_status nmhd_proceed(nmhd_solver *s, double goal_time, double wallclock_limi
     h = s->hctl[slot];
     if (h.status) {
       result = fail(s, NMHD_ERR_NUMERICAL,
-                    (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
-                                                    : "non-finite state, density <= 0 or pressure <= 0");
+                    (h.status & nmhd::kStatusTimeout) ? "a kernel's bounded wait for its tensor copies gave up"
+                    : (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
+                                                      : "non-finite state, density <= 0 or pressure <= 0");
       break;
     }
     if (h.done) { result = NMHD_GOAL_REACHED; break; }
@@ -601,7 +606,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
                                  half, fin, q);
       else if (s->variant == 4)
         nmhd::launch_cell_update_fused(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel,
-                                       half, fin, q);
+                                       half, fin, s->epi_maps, q);
       else
         nmhd::launch_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                             fin, q);
@@ -921,8 +926,9 @@ nmhd_status nmhd_slab_poll(nmhd_solver *s, int64_t *generation, double *time) {
   if (time) *time = h.time;
   if (h.status)
     return fail(s, NMHD_ERR_NUMERICAL,
-                (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
-                                                : "non-finite state, density <= 0 or pressure <= 0");
+                (h.status & nmhd::kStatusTimeout) ? "a kernel's bounded wait for its tensor copies gave up"
+                : (h.status & nmhd::kStatusBadDt) ? "time step is negative or not finite"
+                                                  : "non-finite state, density <= 0 or pressure <= 0");
   return h.done ? NMHD_GOAL_REACHED : NMHD_OK;
 }
 

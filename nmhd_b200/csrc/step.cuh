@@ -48,7 +48,9 @@ struct StepCtl {
   long long dt_seq_base;
 };
 
-enum : int { kStatusNumerical = 1, kStatusBadDt = 2 };
+// kStatusTimeout: a bounded wait inside a kernel (for its tensor copies) gave
+// up; the kernel stopped without writing its results.
+enum : int { kStatusNumerical = 1, kStatusBadDt = 2, kStatusTimeout = 4 };
 
 // Box constants from a configuration, with the reference's float chains.
 GridParams derive_grid(const nmhd_config &c);
@@ -111,9 +113,14 @@ void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1,
                         cudaStream_t stream);
 // The update of a stage in one kernel (variant 4): constrained transport and
 // conserved update fused, corner EMFs and new face B in shared memory.
+// `maps` (make_epilogue_maps, for these w0, w1, wp and flux buffers) lets
+// interior tiles stage their inputs with tensor copies; NULL: cp.async only.
+struct EpilogueMaps;
+EpilogueMaps *make_epilogue_maps(const GridParams &g, float *w0, float *w1, float *wp, float *flux);
+void free_epilogue_maps(EpilogueMaps *m);
 void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                               float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
-                              cudaStream_t stream);
+                              const EpilogueMaps *maps, cudaStream_t stream);
 // One RK stage with the per-cell kernels as a pipeline over chunks of z_chunk
 // planes (variant 3), so each chunk's face fluxes are consumed from L2.
 void launch_cell_stage_chunked(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,

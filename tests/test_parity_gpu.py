@@ -334,7 +334,7 @@ def test_autotune_restores_state_and_keeps_results_bitwise(gpu):
         assert again.kernel() == best[:3]
     other, _ = shearing_box(n_radial=16, n_azimuthal=64, n_vertical=12, l_azimuthal=4.0, seed=13)
     with MHDSolver(other) as fresh:
-        assert fresh.kernel()[0] == 2
+        assert fresh.kernel()[0] == 4
 
 
 @pytest.mark.parametrize("zc", [1, 2, 5])
