@@ -6,7 +6,7 @@ seeded inputs and stores its outputs.  The reference ships no golden vectors
 of its own, so these fixtures pin both the oracle (tests/test_oracle_pin.py)
 and, through it, the CUDA path.
 
-Usage:  python tests/golden/make_golden.py
+Usage:  python tests/golden/make_golden.py [NAME ...]   (default: every case)
 """
 from __future__ import annotations
 
@@ -24,6 +24,13 @@ from oracle import oracle  # noqa: E402
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 
+def scheme(built, space=2, time=2):
+    """A problem with generate_config.rb's scheme options (-s space, -t time)."""
+    cfg, state = built
+    cfg.space_order, cfg.time_order = space, time
+    return cfg, state
+
+
 # name -> (reference binary, problem builder, steps, goal_time, store input)
 CASES = {
     "ot16": ("ot16", lambda: orszag_tang_3d(16), 10, 1.0e30, True),
@@ -35,6 +42,16 @@ CASES = {
     "shear48x20x12": ("shear48x20x12",
                       lambda: shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12, l_azimuthal=2.0),
                       8, 1.0e30, False),
+    # the reference's piecewiseconst1 / euler1 schemes (oracle/expand_variant.py)
+    "ot24x20x12_s1": ("ot24x20x12_s1", lambda: scheme(orszag_tang_3d(24, ny=20, nz=12), space=1),
+                      15, 1.0e30, False),
+    "shear32x16x8_t1": ("shear32x16x8_t1",
+                        lambda: scheme(shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8,
+                                                    l_azimuthal=4.0, seed=4), time=1), 15, 1.0e30, False),
+    "shear48x20x12_s1t1": ("shear48x20x12_s1t1",
+                           lambda: scheme(shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12,
+                                                       l_azimuthal=2.0, seed=5), space=1, time=1),
+                           15, 1.0e30, False),
 }
 
 
@@ -69,7 +86,10 @@ def digest(a):
 
 
 def main():
+    only = set(sys.argv[1:])
     for name, (binary, make, steps, goal, keep_input) in CASES.items():
+        if only and name not in only:
+            continue
         cfg, state = make()
         out, times, info = oracle.run_ref(binary, state, steps, goal_time=goal)
         payload = {"output": out, "times": times, "steps": np.int64(info["steps"]),
@@ -80,6 +100,8 @@ def main():
         np.savez_compressed(os.path.join(HERE, name + ".npz"), **payload)
         print(name, info)
     for name, (binary, make, steps, keep) in SLAB_CASES.items():
+        if only and name not in only:
+            continue
         cfg, states = make()
         outs, times, infos = oracle.run_ref_slabs(binary, states, steps)
         payload = {"times": times, "steps": np.int64(infos[0]["steps"]),

@@ -102,3 +102,35 @@ def test_batched_ensemble_extremes_match_reference(gpu):
             got, t, gen = gpu_run(cfg, s, steps)
             assert b.clock(len(corners) + j) == (t, gen)
             assert_same(b.get_state(len(corners) + j), got)
+
+
+# The reference's other scheme choices (generate_config.rb -s 1 / -t 1),
+# host-compiled from its shipped expansion through oracle/expand_variant.py:
+# (binary, problem, space order, time order)
+SCHEMES = [
+    ("ot24x20x12_s1", lambda: orszag_tang_3d(24, ny=20, nz=12), 1, 2),
+    ("shear32x16x8_t1", lambda: shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0,
+                                             seed=11), 2, 1),
+    ("shear48x20x12_s1t1", lambda: shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12, l_azimuthal=2.0,
+                                                seed=12), 1, 1),
+]
+
+
+@pytest.mark.parametrize("variant", [4, 2])
+@pytest.mark.parametrize("case", range(len(SCHEMES)))
+def test_scheme_variants_match_the_reference_expansions(gpu, case, variant):
+    """Piecewise-constant reconstruction and Euler stepping, 60 steps, against
+    the reference's own piecewiseconst1 / euler1 code (its template's rules
+    applied to the shipped expansion), for the default and the three-kernel
+    variant."""
+    name, make, so, to = SCHEMES[case]
+    needs_ref(name)
+    cfg, s = make()
+    cfg.space_order, cfg.time_order = so, to
+    ref, times, info = oracle.run_ref(name, s, 60)
+    with MHDSolver(cfg) as sol:
+        sol.set_kernel(variant, 8, 0)
+        sol.set_state(s)
+        sol.step(60)
+        assert sol.current_time() == times[-1]
+        assert_same(sol.get_state(), ref)

@@ -15,12 +15,25 @@ import pytest
 from nmhd_b200.problems import orszag_tang_3d, shearing_box
 from oracle import oracle
 
+def scheme(built, space=2, time=2):
+    """A problem with generate_config.rb's scheme options (-s space, -t time)."""
+    cfg, state = built
+    cfg.space_order, cfg.time_order = space, time
+    return cfg, state
+
+
 GOLDEN = {
     "ot16": lambda: orszag_tang_3d(16),
     "ot16_goal": lambda: orszag_tang_3d(16),
     "ot24x20x12": lambda: orszag_tang_3d(24, ny=20, nz=12),
     "shear32x16x8": lambda: shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0),
     "shear48x20x12": lambda: shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12, l_azimuthal=2.0),
+    # the reference's piecewiseconst1 / euler1 expansions (oracle/expand_variant.py)
+    "ot24x20x12_s1": lambda: scheme(orszag_tang_3d(24, ny=20, nz=12), space=1),
+    "shear32x16x8_t1": lambda: scheme(shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8,
+                                                   l_azimuthal=4.0, seed=4), time=1),
+    "shear48x20x12_s1t1": lambda: scheme(shearing_box(n_radial=20, n_azimuthal=48, n_vertical=12,
+                                                      l_azimuthal=2.0, seed=5), space=1, time=1),
 }
 
 
