@@ -35,6 +35,10 @@ typedef struct oracle_config {
   int32_t space_order; /* 2 minbee, 1 piecewise constant */
   int32_t time_order;  /* 2 midpoint, 1 Euler */
   int32_t flags;       /* 1: margins refilled before the second RK2 stage */
+  /* kParallelSizeY: P > 1 makes the state one radial slab of a box split over
+   * P ranks along Y (size_y: the slab's rows and margins; extent_y: the
+   * box's), advanced with the split-phase functions below */
+  int32_t parallel_size_y;
 } oracle_config;
 
 /* float build (the reference's FP32) */
@@ -48,6 +52,21 @@ int oracle_proceed_f32(const oracle_config *cfg, float *state, double *time, int
 void oracle_hlld_f32(float gamma, float bx, const float lr[14], float out[7]);
 float oracle_cfl_f32(const oracle_config *cfg, const float *state, float goal);
 void oracle_shear_fill_f32(const oracle_config *cfg, float *state, double time);
+/* Split-phase step of one rank of a P-rank run (MHDSolver::proceed with
+ * communicate(), src/library/mhd_solver.inlrb:283-493, 850-993):
+ *   halo_pack    the two outgoing Y messages of communicate_gather_kernel_y
+ *                (:184-222) at time t: send_inc (to the rank above) and
+ *                send_dec (to the rank below), each 8 x Sx*My*Sz values
+ *   halo_unpack  communicate_scatter_kernel_y (:224-242) of the received
+ *                messages into the Y margins, then the Z-margin copies
+ *   stages       the RK stages of one step with the common dt (:904-978).
+ * With P = 1 and each message delivered to itself this is oracle_proceed's
+ * step. */
+void oracle_halo_pack_f32(const oracle_config *cfg, const float *state, double time, float *send_inc,
+                          float *send_dec);
+void oracle_halo_unpack_f32(const oracle_config *cfg, float *state, const float *recv_inc,
+                            const float *recv_dec);
+void oracle_stages_f32(const oracle_config *cfg, float *state, float dt);
 
 /* double build (the reference with Real = double) */
 int oracle_proceed_f64(const oracle_config *cfg, double *state, double *time, int64_t *generation,
@@ -56,6 +75,11 @@ int oracle_proceed_f64(const oracle_config *cfg, double *state, double *time, in
 void oracle_hlld_f64(double gamma, double bx, const double lr[14], double out[7]);
 double oracle_cfl_f64(const oracle_config *cfg, const double *state, double goal);
 void oracle_shear_fill_f64(const oracle_config *cfg, double *state, double time);
+void oracle_halo_pack_f64(const oracle_config *cfg, const double *state, double time, double *send_inc,
+                          double *send_dec);
+void oracle_halo_unpack_f64(const oracle_config *cfg, double *state, const double *recv_inc,
+                            const double *recv_dec);
+void oracle_stages_f64(const oracle_config *cfg, double *state, double dt);
 
 #ifdef __cplusplus
 }

@@ -43,13 +43,16 @@ typedef struct FN(consts) {
 
 static void FN(derive)(const oracle_config *c, FN(consts) *k) {
   int s[3] = {c->size_x, c->size_y, c->size_z};
-  int gsz[3] = {c->size_x, c->size_y - 2 * c->margin_y, c->size_z - 2 * c->margin_z};
+  /* kLocalSize (interior of this rank) and kGlobalSize (P ranks along Y) */
+  const int py = c->parallel_size_y > 1 ? c->parallel_size_y : 1;
+  int lsz[3] = {c->size_x, c->size_y - 2 * c->margin_y, c->size_z - 2 * c->margin_z};
+  int gsz[3] = {lsz[0], py * lsz[1], lsz[2]};
   float ext[3] = {c->extent_x, c->extent_y, c->extent_z};
   real comp_ext[3], local_ext[3];
   for (int i = 0; i < 3; ++i) {
     real L = (real)ext[i];
     comp_ext[i] = (real)((real)(L / (real)gsz[i]) * (real)s[i]);
-    local_ext[i] = (real)((real)(L / (real)gsz[i]) * (real)gsz[i]);
+    local_ext[i] = (real)((real)(L / (real)gsz[i]) * (real)lsz[i]);
     k->d[i] = comp_ext[i] / (real)s[i];
   }
   k->extent_x = comp_ext[0];
@@ -451,42 +454,57 @@ static void FN(displacement)(const FN(consts) *k, double t, int *d_int, real *mi
   *minor = (real)(displacement1 / (double)k->d[0] - *d_int);
 }
 
-/* communicate() with one rank (mhd_solver.inlrb:184-242, 283-493): shifted
- * Y-margin fill from the opposite interior rows, then plain Z-margin copies. */
-static void FN(shear_fill_impl)(const oracle_config *cfg, const FN(grid) *g, const FN(consts) *k,
-                                real *w, double t) {
+/* communicate_gather_kernel_y (mhd_solver.inlrb:184-222): the two outgoing
+ * messages of the Y-margin exchange at time t, item (z*M + y)*Sx + x of
+ * field v at v*unit + item: buf_inc (to the rank above) from the top interior
+ * rows shifted by +d_int, v_X - relative_velocity; buf_dec (to the rank below)
+ * from the bottom interior rows shifted by -d_int-1, v_X + relative_velocity.
+ * The interpolation weights both multiply the same sample, as the
+ * reference's do. */
+static void FN(halo_pack)(const oracle_config *cfg, const FN(grid) *g, const FN(consts) *k, const real *w,
+                          double t, real *buf_inc, real *buf_dec) {
+  const int M = cfg->margin_y;
+  const int sx = g->sx, sy = g->sy, sz = g->sz;
+  const size_t n = g->n;
+  int d_int;
+  real f;
+  FN(displacement)(k, t, &d_int, &f);
+  const real rv = (real)k->rel_vel;
+  const size_t unit = (size_t)sx * M * sz;
+  for (int v = 0; v < 8; ++v) {
+    const real *var = w + (size_t)v * n;
+#pragma omp parallel for schedule(static)
+    for (int zz = 0; zz < sz; ++zz)
+      for (int yy = 0; yy < M; ++yy)
+        for (int xx = 0; xx < sx; ++xx) {
+          size_t a = ((size_t)zz * M + yy) * sx + xx;
+          int inc_x0 = (xx + d_int) % sx;
+          int dec_x0 = (xx - d_int - 1 + sx) % sx;
+          real vi = var[((size_t)zz * sy + (sy - 2 * M + yy)) * sx + inc_x0];
+          real vd = var[((size_t)zz * sy + (M + yy)) * sx + dec_x0];
+          real bi = ((real)1 - f) * vi + f * vi;
+          real bd = f * vd + ((real)1 - f) * vd;
+          if (v == F_VX) {
+            bi = bi - rv;
+            bd = bd + rv;
+          }
+          buf_inc[(size_t)v * unit + a] = bi;
+          buf_dec[(size_t)v * unit + a] = bd;
+        }
+  }
+}
+
+/* communicate_scatter_kernel_y (mhd_solver.inlrb:224-242): the message from
+ * the rank below (recv_inc) into the bottom margin, the one from the rank
+ * above (recv_dec) into the top margin except By of its first row; then the
+ * plain Z-margin copies (:384-402, 463-480). */
+static void FN(halo_unpack)(const oracle_config *cfg, const FN(grid) *g, real *w, const real *recv_inc,
+                            const real *recv_dec) {
   const int M = cfg->margin_y, Mz = cfg->margin_z;
   const int sx = g->sx, sy = g->sy, sz = g->sz;
   const size_t n = g->n;
   if (M > 0) {
-    int d_int;
-    real f;
-    FN(displacement)(k, t, &d_int, &f);
-    const real rv = (real)k->rel_vel;
     const size_t unit = (size_t)sx * M * sz;
-    real *buf_inc = (real *)malloc(sizeof(real) * unit * 8);
-    real *buf_dec = (real *)malloc(sizeof(real) * unit * 8);
-    for (int v = 0; v < 8; ++v) {
-      const real *var = w + (size_t)v * n;
-#pragma omp parallel for schedule(static)
-      for (int zz = 0; zz < sz; ++zz)
-        for (int yy = 0; yy < M; ++yy)
-          for (int xx = 0; xx < sx; ++xx) {
-            size_t a = ((size_t)zz * M + yy) * sx + xx;
-            int inc_x0 = (xx + d_int) % sx;
-            int dec_x0 = (xx - d_int - 1 + sx) % sx;
-            real vi = var[((size_t)zz * sy + (sy - 2 * M + yy)) * sx + inc_x0];
-            real vd = var[((size_t)zz * sy + (M + yy)) * sx + dec_x0];
-            real bi = ((real)1 - f) * vi + f * vi;
-            real bd = f * vd + ((real)1 - f) * vd;
-            if (v == F_VX) {
-              bi = bi - rv;
-              bd = bd + rv;
-            }
-            buf_inc[(size_t)v * unit + a] = bi;
-            buf_dec[(size_t)v * unit + a] = bd;
-          }
-    }
     for (int v = 0; v < 8; ++v) {
       real *var = w + (size_t)v * n;
 #pragma omp parallel for schedule(static)
@@ -494,13 +512,11 @@ static void FN(shear_fill_impl)(const oracle_config *cfg, const FN(grid) *g, con
         for (int yy = 0; yy < M; ++yy)
           for (int xx = 0; xx < sx; ++xx) {
             size_t a = ((size_t)zz * M + yy) * sx + xx;
-            var[((size_t)zz * sy + yy) * sx + xx] = buf_inc[(size_t)v * unit + a];
+            var[((size_t)zz * sy + yy) * sx + xx] = recv_inc[(size_t)v * unit + a];
             if (!(v == F_BX + 1 && yy == 0))
-              var[((size_t)zz * sy + (sy - M + yy)) * sx + xx] = buf_dec[(size_t)v * unit + a];
+              var[((size_t)zz * sy + (sy - M + yy)) * sx + xx] = recv_dec[(size_t)v * unit + a];
           }
     }
-    free(buf_inc);
-    free(buf_dec);
   }
   if (Mz > 0) {
     const size_t unit = (size_t)sx * sy * Mz;
@@ -517,6 +533,22 @@ static void FN(shear_fill_impl)(const oracle_config *cfg, const FN(grid) *g, con
   }
 }
 
+/* communicate() with one rank (mhd_solver.inlrb:283-493): each message
+ * delivered to the rank itself (the single box's shear-periodic boundary). */
+static void FN(shear_fill_impl)(const oracle_config *cfg, const FN(grid) *g, const FN(consts) *k,
+                                real *w, double t) {
+  const size_t unit = (size_t)g->sx * cfg->margin_y * g->sz;
+  real *buf_inc = NULL, *buf_dec = NULL;
+  if (cfg->margin_y > 0) {
+    buf_inc = (real *)malloc(sizeof(real) * unit * 8);
+    buf_dec = (real *)malloc(sizeof(real) * unit * 8);
+    FN(halo_pack)(cfg, g, k, w, t, buf_inc, buf_dec);
+  }
+  FN(halo_unpack)(cfg, g, w, buf_inc, buf_dec);
+  free(buf_inc);
+  free(buf_dec);
+}
+
 /* one integrator stage (mhd_solver.inlrb:908-962):
  * fluxes from w_in (wind = its velocity), U from w_bef, result in w_out */
 static void FN(stage)(FN(solver) *s, real dt, real *w_in, real *w_bef, real *w_out) {
@@ -530,6 +562,19 @@ static void FN(stage)(FN(solver) *s, real dt, real *w_in, real *w_bef, real *w_o
   FN(add_pace)(s, dt, w_bef, w_out);
   FN(to_primitive)(s, w_out);
   if (s->cfg.problem == 1) FN(kick)(s, dt, w_out);
+}
+
+/* The RK stages of one step with time step dt from time t (mhd_solver.inlrb:966-975) */
+static void FN(run_stages)(FN(solver) *s, real dt, double t) {
+  if (s->cfg.time_order == 1) {
+    FN(stage)(s, dt, s->w, s->w, s->w);
+  } else {
+    FN(stage)(s, dt / 2, s->w, s->w, s->wp);
+    /* nmhd_config flag HALO_PER_STAGE (no reference counterpart): the
+       predictor's margins refilled at its time t + dt/2 */
+    if (s->cfg.flags & 1) FN(shear_fill_impl)(&s->cfg, &s->g, &s->k, s->wp, t + (double)(dt / 2));
+    FN(stage)(s, dt, s->wp, s->w, s->w);
+  }
 }
 
 /* MHDSolver::proceed (mhd_solver.inlrb:850-993) for at most max_steps steps */
@@ -564,15 +609,7 @@ int FN(oracle_proceed)(const oracle_config *cfg, real *state, double *time, int6
       done = 1;
     }
     if (dt_out) dt_out[steps] = dt;
-    if (cfg->time_order == 1) {
-      FN(stage)(&s, dt, s.w, s.w, s.w);
-    } else {
-      FN(stage)(&s, dt / 2, s.w, s.w, s.wp);
-      /* nmhd_config flag HALO_PER_STAGE (no reference counterpart): the
-         predictor's margins refilled at its time t + dt/2 */
-      if (cfg->flags & 1) FN(shear_fill_impl)(cfg, &s.g, &s.k, s.wp, *time + (double)(dt / 2));
-      FN(stage)(&s, dt, s.wp, s.w, s.w);
-    }
+    FN(run_stages)(&s, dt, *time);
     *time += (double)dt;
     *generation += 1;
     ++steps;
@@ -607,4 +644,40 @@ void FN(oracle_shear_fill)(const oracle_config *cfg, real *state, double time) {
   FN(consts) k;
   FN(setup)(cfg, &g, &k);
   FN(shear_fill_impl)(cfg, &g, &k, state, time);
+}
+
+void FN(oracle_halo_pack)(const oracle_config *cfg, const real *state, double time, real *send_inc,
+                          real *send_dec) {
+  FN(grid) g;
+  FN(consts) k;
+  FN(setup)(cfg, &g, &k);
+  if (cfg->margin_y > 0) FN(halo_pack)(cfg, &g, &k, state, time, send_inc, send_dec);
+}
+
+void FN(oracle_halo_unpack)(const oracle_config *cfg, real *state, const real *recv_inc,
+                            const real *recv_dec) {
+  FN(grid) g;
+  FN(consts) k;
+  FN(setup)(cfg, &g, &k);
+  FN(halo_unpack)(cfg, &g, state, recv_inc, recv_dec);
+}
+
+void FN(oracle_stages)(const oracle_config *cfg, real *state, real dt) {
+  FN(solver) s;
+  s.cfg = *cfg;
+  s.cfg.flags &= ~1;  /* a slab has no per-stage margin refill (nmhd_create refuses it) */
+  FN(setup)(cfg, &s.g, &s.k);
+  const size_t n = s.g.n;
+  s.w = state;
+  s.wp = (real *)calloc(8 * n, sizeof(real));
+  s.mom = (real *)calloc(3 * n, sizeof(real));
+  s.ene = (real *)calloc(n, sizeof(real));
+  s.pace = (real *)calloc(8 * n, sizeof(real));
+  s.flux = (real *)calloc(7 * n, sizeof(real));
+  FN(run_stages)(&s, dt, 0.0);
+  free(s.wp);
+  free(s.mom);
+  free(s.ene);
+  free(s.pace);
+  free(s.flux);
 }

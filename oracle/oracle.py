@@ -46,6 +46,15 @@ def lib():
             fn = getattr(L, "oracle_shear_fill_" + suf)
             fn.restype = None
             fn.argtypes = [ctypes.c_void_p, rp, ctypes.c_double]
+            fn = getattr(L, "oracle_halo_pack_" + suf)
+            fn.restype = None
+            fn.argtypes = [ctypes.c_void_p, rp, ctypes.c_double, rp, rp]
+            fn = getattr(L, "oracle_halo_unpack_" + suf)
+            fn.restype = None
+            fn.argtypes = [ctypes.c_void_p, rp, rp, rp]
+            fn = getattr(L, "oracle_stages_" + suf)
+            fn.restype = None
+            fn.argtypes = [ctypes.c_void_p, rp, ctypes.c_float if suf == "f32" else ctypes.c_double]
         L.oracle_hlld_f32.restype = None
         L.oracle_hlld_f32.argtypes = [ctypes.c_float, ctypes.c_float, f32p, f32p]
         L.oracle_hlld_f64.restype = None
@@ -94,6 +103,39 @@ def shear_fill(cfg, state, time, dtype=np.float32):
     c = cfg.to_ctypes()
     getattr(lib(), "oracle_shear_fill_" + suf)(ctypes.byref(c), st, time)
     return st
+
+
+def halo_count(cfg):
+    """Values in one Y-halo message: 8 fields x Sx x margin_y x Sz."""
+    return 8 * cfg.size_x * cfg.margin_y * cfg.size_z
+
+
+def halo_pack(cfg, state, time, dtype=np.float32):
+    """The two outgoing Y messages of a radial slab at ``time``: (to the rank
+    above, to the rank below)."""
+    suf = "f32" if dtype == np.float32 else "f64"
+    st = np.ascontiguousarray(state, dtype=dtype)
+    inc = np.zeros(max(1, halo_count(cfg)), dtype)
+    dec = np.zeros_like(inc)
+    c = cfg.to_ctypes()
+    getattr(lib(), "oracle_halo_pack_" + suf)(ctypes.byref(c), st, time, inc, dec)
+    return inc, dec
+
+
+def halo_unpack(cfg, state, recv_inc, recv_dec, dtype=np.float32):
+    """Scatter the received messages into the Y margins and copy the Z
+    margins, in place (``state`` must be C-contiguous of ``dtype``)."""
+    suf = "f32" if dtype == np.float32 else "f64"
+    c = cfg.to_ctypes()
+    getattr(lib(), "oracle_halo_unpack_" + suf)(ctypes.byref(c), state, np.ascontiguousarray(recv_inc, dtype),
+                                                np.ascontiguousarray(recv_dec, dtype))
+
+
+def stages(cfg, state, dt, dtype=np.float32):
+    """The RK stages of one step with time step ``dt``, in place."""
+    suf = "f32" if dtype == np.float32 else "f64"
+    c = cfg.to_ctypes()
+    getattr(lib(), "oracle_stages_" + suf)(ctypes.byref(c), state, dt)
 
 
 def ref_binary(name):

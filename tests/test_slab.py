@@ -244,6 +244,64 @@ def _t(a):
     return torch.from_numpy(np.ascontiguousarray(a))
 
 
+class OracleSlabBackend:
+    """One radial slab of the MHD step on the host, through the oracle's
+    split-phase functions (the reference's communicate() halves, its slab CFL
+    time and its RK stages): the same interface as SolverBackend, so
+    DistributedSlab drives the real step over gloo.  Clock and goal clamp as
+    MHDSolver::proceed (mhd_solver.inlrb:870-901): dt = the all-reduced
+    minimum of every rank's min(goal, CFL time); past the goal, dt = goal -
+    time and the run ends."""
+
+    def __init__(self, cfg, state):
+        import torch
+        self.cfg = cfg
+        self.w = np.ascontiguousarray(state, np.float32).copy()
+        self.gen = 0
+        self.time = 0.0
+        self.goal = np.float32(np.inf)
+        self.done = False
+        self._slot = torch.full((1,), np.inf, dtype=torch.float32)
+        self.device = "cpu"
+
+    def halo_count(self):
+        return oracle.halo_count(self.cfg)
+
+    def begin(self, goal):
+        self.goal = np.float32(goal)
+        self.done = False
+
+    def pack(self, send_inc, send_dec):
+        if self.done:
+            return
+        inc, dec = oracle.halo_pack(self.cfg, self.w, self.time)
+        send_inc.copy_(_t(inc))
+        send_dec.copy_(_t(dec))
+
+    def unpack(self, recv_inc, recv_dec):
+        if self.done:
+            return
+        oracle.halo_unpack(self.cfg, self.w, recv_inc.numpy(), recv_dec.numpy())
+        self._slot[0] = oracle.cfl(self.cfg, self.w, float(self.goal))
+
+    def cfl_slot(self):
+        return self._slot
+
+    def stages(self):
+        if self.done:
+            return
+        dt = np.float32(self._slot[0].item())
+        if self.time + float(dt) > float(self.goal):
+            dt = np.float32(float(self.goal) - self.time)
+            self.done = True
+        oracle.stages(self.cfg, self.w, dt)
+        self.time += float(dt)
+        self.gen += 1
+
+    def poll(self):
+        return self.done, None, self.gen, self.time
+
+
 def _global_reference(u0, steps, goal=np.inf):
     """The same scheme on the whole periodic array (the answer the ranks must
     reproduce): margins are periodic copies, dt the global CFL minimum."""
@@ -272,8 +330,17 @@ def _worker(rank, world, port, q, mode):
     from nmhd_b200.slab import DistributedSlab
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
+    os.environ["OMP_NUM_THREADS"] = "1"
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
+        if mode in SLAB_CASES:  # the MHD step of a reference P-rank case
+            make, steps = SLAB_CASES[mode]
+            cfg, states = make()
+            b = OracleSlabBackend(cfg, states[rank])
+            slab = DistributedSlab(b, None)
+            reached = slab.proceed(np.inf, max_steps=steps)
+            q.put((rank, {"w": b.w, "gen": b.gen, "time": b.time, "reached": reached}))
+            return
         u0 = np.sin(np.linspace(0, 2 * np.pi, 12 * world, endpoint=False)).astype(np.float32) + 1.5
         part = u0[12 * rank:12 * (rank + 1)]
         fail_at = 5 if (mode == "error" and rank == world - 1) else None
@@ -339,3 +406,23 @@ def test_distributed_timeout_and_error_stop_every_rank():
     assert res[0]["gen"] == res[1]["gen"] == 16  # one batch, on both ranks
     res = _run(3, "error")
     assert all(r["raised"] for r in res)
+
+
+@pytest.mark.parametrize("name", sorted(SLAB_CASES))
+def test_distributed_mhd_step_equals_reference_ranks(name):
+    """The real MHD step through DistributedSlab on as many gloo ranks as the
+    reference case has (2, 3, 4; shear-periodic radial wrap, Z margins), each
+    rank's slab advanced by the oracle's split-phase functions: every rank's
+    state is bitwise the reference's own P-rank run (tests/golden/<name>.npz,
+    written by its communicate() and MPI_Allreduce through the file-mailbox
+    MPI of oracle/refshim), and every rank has the reference's clock."""
+    make, steps = SLAB_CASES[name]
+    cfg, states = make()
+    fx = np.load(os.path.join(GOLDEN, name + ".npz"))
+    assert [str(h) for h in fx["input_sha256"]] == [_digest(s) for s in states]
+    res = _run(len(states), name)
+    assert [_digest(r["w"]) for r in res] == [str(h) for h in fx["output_sha256"]]
+    if "output" in fx:
+        for r, ref in zip(res, fx["output"]):
+            assert np.array_equal(r["w"], ref)
+    assert all(r["gen"] == steps and r["time"] == fx["times"][-1] and r["reached"] is False for r in res)
