@@ -751,7 +751,7 @@ def adjoint_measure(workload, dev, tape_budget=-1, warmup=3, reps=1, adjoint_ste
             adj.append(sol.adjoint_timing())
     fwd_ms = statistics.median(fwd)
     tot = statistics.median([a["total"] for a in adj])
-    rev = statistics.median([a["recompute"] + a["adjoint"] for a in adj])
+    rev = statistics.median([a["adjoint"] for a in adj])  # reverse sweep, recomputation overlapped
     out = {"value": tot / fwd_ms, "unit": "x", "steps": steps, "cells_interior": cfg.interior_cells,
            "cells_with_margins": cfg.cells, "loss": "Maxwell stress -<BxBy>, states %d..%d" % window,
            "ckpt_every": K, "tape_budget_bytes": tape_budget,

@@ -352,13 +352,18 @@ nmhd_status nmhd_tlm_run(nmhd_solver *s, int32_t nsteps, const nmhd_loss_spec *l
  * segments whose tapes were not kept.  bytes = -1 (default): as many segments
  * as fit in half of the device memory free at the run; 0: the last segment
  * only (least memory); > 0: that many bytes for further segments.  The
- * gradient does not depend on it (bitwise).  nmhd_adjoint_kept_segments: how
- * many segments the last run kept. */
+ * gradient does not depend on it (bitwise).  When segments are recomputed, one
+ * more segment's tape is held for the recomputation that overlaps the
+ * reverse sweep.  nmhd_adjoint_kept_segments: how many segments the last
+ * run's forward kept. */
 nmhd_status nmhd_adjoint_set_tape_budget(nmhd_solver *s, int64_t bytes);
 int32_t nmhd_adjoint_kept_segments(const nmhd_solver *s);
 /* Device time of the last nmhd_adjoint_run / nmhd_adjoint_run_f64 in ms:
- * [0] forward run with checkpoints, [1] segment recomputation, [2] adjoint
- * kernels, [3] the whole run. */
+ * [0] forward run with checkpoints, [1] segment recomputation (on a stream of
+ * its own, overlapping [2]: the recomputation of a segment runs beside the
+ * adjoint of the segment after it, in a second tape slot), [2] the reverse
+ * sweep (adjoint kernels, waiting for recomputed segments), [3] the whole
+ * run, [0] + [2]. */
 nmhd_status nmhd_adjoint_timing(const nmhd_solver *s, double ms_out[4]);
 
 /* ---- Radial slab decomposition (kParallelSizeY = P ranks along Y) ----

@@ -171,6 +171,13 @@ struct Workspace {
   float *dt_dev = nullptr, *hist_dummy = nullptr;
   double ms[4] = {0, 0, 0, 0};
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // Segment recomputation runs on a stream of its own, beside the reverse
+  // sweep: control blocks are staged in pinned memory (one per segment, so
+  // none is overwritten before its copy runs) and two tape slots alternate,
+  // ordered by "slot recomputed" / "slot swept" events.
+  cudaStream_t stream2 = nullptr;
+  StepCtl *hstage = nullptr;  // pinned, NMHD_ADJOINT_MAX_STEPS entries
+  cudaEvent_t slot_ready[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr}, fwd_done = nullptr;
 };
 
 Workspace &workspace(nmhd_solver *s) {
@@ -211,6 +218,13 @@ nmhd_status reserve(nmhd_solver *s, Workspace &w, size_t bytes) {
     AD_CUDA(cudaMalloc(&w.dt_dev, sizeof(float) * nmhd::kDtHistCap));
     AD_CUDA(cudaMalloc(&w.hist_dummy, sizeof(float) * nmhd::kDtHistCap));
     for (auto &e : w.ev) AD_CUDA(cudaEventCreate(&e));
+    AD_CUDA(cudaStreamCreateWithFlags(&w.stream2, cudaStreamNonBlocking));
+    AD_CUDA(cudaMallocHost(&w.hstage, sizeof(StepCtl) * NMHD_ADJOINT_MAX_STEPS));
+    for (int i = 0; i < 2; ++i) {
+      AD_CUDA(cudaEventCreateWithFlags(&w.slot_ready[i], cudaEventDisableTiming));
+      AD_CUDA(cudaEventCreateWithFlags(&w.slot_free[i], cudaEventDisableTiming));
+    }
+    AD_CUDA(cudaEventCreateWithFlags(&w.fwd_done, cudaEventDisableTiming));
   }
   if (w.bytes >= bytes) return NMHD_OK;
   if (w.mem) {
@@ -269,14 +283,31 @@ nmhd_status write_ctl(nmhd_solver *s, Workspace &w, double time, long long gen, 
   return NMHD_OK;
 }
 
+// The same control block for the recomputation of segment `slot` (an index
+// into the pinned staging array), copied on `stream` without a host wait.
+nmhd_status write_ctl_async(nmhd_solver *s, Workspace &w, double time, long long gen, int slot,
+                            cudaStream_t stream) {
+  StepCtl &h = w.hstage[slot];
+  std::memset(&h, 0, sizeof(h));
+  h.time = time;
+  h.generation = gen;
+  h.cfl_cur = h.cfl_next = 0x7f800000u;
+  h.goal = INFINITY;
+  h.hist_cap = nmhd::kDtHistCap;
+  h.dt_seq = w.dt_dev;
+  h.dt_seq_base = 0;
+  w.parity = 0;
+  AD_CUDA(cudaMemcpyAsync(w.ctl, &h, sizeof(h), cudaMemcpyHostToDevice, stream));
+  return NMHD_OK;
+}
+
 // One FP32 step with the production kernels on explicit buffers: t.wf holds
 // W^n (its margins are filled in place), the raw W^{n+1} goes to t.wo.  The
 // kernels take the current state as buffer `parity` of (w0, w1) and the final
 // stage flips the device parity; the pair is passed in the order that makes
 // t.wf the current buffer, so the parity needs no reset between steps.
-void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl) {
+void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl, cudaStream_t st) {
   const GridParams &g = s->g;
-  cudaStream_t st = s->stream;
   float *hist = cfl ? w.dt_dev : w.hist_dummy;
   float *b0 = w.parity ? t.wo : t.wf, *b1 = w.parity ? t.wf : t.wo;  // buffer 2 = t.ws
   if (g.my > 0 || g.mz > 0) {
@@ -332,10 +363,16 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   // partner, 3 adjoint states, adjoint scratch, reduction partials
   const size_t nb = (n + 255) / 256;
   R *ckpt = nullptr, *tape = nullptr, *fscr = nullptr, *spare = nullptr, *lam = nullptr, *scr = nullptr;
+  R *xslot = nullptr, *fscr2 = nullptr;
   double *partial = nullptr, *acc = nullptr;
   auto carve = [&](Arena &ar) {
     ckpt = want_grad ? ar.take<R>((size_t)nseg * 8 * n) : nullptr;
     tape = ar.take<R>((size_t)kseg * tape_steps * kTapeFields * n);
+    // segments recomputed beside the reverse sweep: a second tape slot and a
+    // flux scratch of their own
+    const bool recompute = want_grad && kseg < nseg;
+    xslot = recompute ? ar.take<R>((size_t)tape_steps * kTapeFields * n) : nullptr;
+    fscr2 = recompute ? ar.take<R>((size_t)kFluxScratchFields * n) : nullptr;
     fscr = ar.take<R>((size_t)kFluxScratchFields * n);
     spare = ar.take<R>(8 * n);
     lam = want_grad ? ar.take<R>(24 * n) : nullptr;
@@ -410,7 +447,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
       if (t.wf != A) AD_CUDA(cudaMemcpyAsync(t.wf, A, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
     }
     if constexpr (Prec<R>::kProduction) {
-      prod_step(s, w, t, !frozen);
+      prod_step(s, w, t, !frozen, q);
     } else {
       tn[i + 1] = tn[i] + (double)dts[i];
       fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
@@ -446,55 +483,100 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
   }
 
   // ---- reverse sweep ---------------------------------------------------------------
+  // Segments [0, nrec) are recomputed from their checkpoints on a second
+  // stream while the reverse sweep runs on the solver's: recomputed segment
+  // j (from the last, nrec-1, down) lands in slot X for even j and in tape
+  // slot 0 for odd j, so the recomputation of a segment overlaps the adjoint
+  // of the one after it.  Slot 0 first holds the earliest kept segment; a
+  // recomputation into a slot waits for the sweep of its previous segment.
   R *lamA = lam, *lamS = lam + 8 * n, *lamF = lam + 16 * n;
   const AdjScratch<R> sc = scratch_at(scr, n);
   ex.zero(lamA, 8 * n);
-  double ms_re = 0.0, ms_adj = 0.0;
-  for (int seg = nseg - 1; seg >= 0; --seg) {
+  const int nrec = kept0 / K;
+  cudaStream_t q2 = w.stream2;
+  GpuExec ex2{q2};
+  R *slots[2] = {xslot, tape};  // [0] slot X, [1] tape slot 0
+  std::vector<cudaEvent_t> rev(2 * (size_t)nrec, nullptr);
+  for (auto &e : rev) AD_CUDA(cudaEventCreate(&e));
+  auto recompute = [&](int seg) -> nmhd_status {
+    const int j = nrec - 1 - seg, si = j % 2;
     const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
-    const bool kept = n0 >= kept0;  // taped by the forward run
-    // a recomputed segment reuses the first segment slot of the tape: every
-    // kept segment comes later in the run and has been swept already
-    R *segtape = kept ? tape + (size_t)(n0 - kept0) * kTapeFields * n : tape;
-    if (Prec<R>::kProduction && !kept) {
-      st = write_ctl(s, w, tn[n0], n0, true);
-      if (st != NMHD_OK) return st;
+    R *segtape = slots[si];
+    AD_CUDA(cudaStreamWaitEvent(q2, w.slot_free[si], 0));
+    AD_CUDA(cudaEventRecord(rev[2 * j], q2));
+    if constexpr (Prec<R>::kProduction) {
+      nmhd_status r = write_ctl_async(s, w, tn[n0], n0, seg, q2);
+      if (r != NMHD_OK) return r;
     }
-    AD_CUDA(cudaEventRecord(w.ev[2], q));
-    if (!kept)
-      AD_CUDA(cudaMemcpyAsync(segtape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
-    for (int i = n0; i < (kept ? n0 : n1); ++i) {
-      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr);
+    AD_CUDA(cudaMemcpyAsync(segtape, ckpt + (size_t)seg * 8 * n, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q2));
+    for (int i = n0; i < n1; ++i) {
+      const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr2);
       if constexpr (Prec<R>::kProduction)
-        prod_step(s, w, t, false);
+        prod_step(s, w, t, false, q2);
       else
-        fwd_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
+        fwd_step(ex2, gg, s->cfg.time_order, tn[i], (R)dts[i], t);
       if (i + 1 < n1) {
-        const StepTape<R> tn1 = tape_at(segtape + (size_t)(i + 1 - n0) * kTapeFields * n, n, fscr);
-        AD_CUDA(cudaMemcpyAsync(tn1.wf, t.wo, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q));
+        const StepTape<R> tn1 = tape_at(segtape + (size_t)(i + 1 - n0) * kTapeFields * n, n, fscr2);
+        AD_CUDA(cudaMemcpyAsync(tn1.wf, t.wo, sizeof(R) * 8 * n, cudaMemcpyDeviceToDevice, q2));
       }
     }
-    AD_CUDA(cudaEventRecord(w.ev[3], q));
+    AD_CUDA(cudaEventRecord(rev[2 * j + 1], q2));
+    AD_CUDA(cudaEventRecord(w.slot_ready[si], q2));
+    return NMHD_OK;
+  };
+  auto sweep = [&](int seg, R *segtape) -> nmhd_status {
+    const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
     for (int i = n1 - 1; i >= n0; --i) {
       const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr);
       if (in_window(L, i + 1)) ex.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
       adj_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
       std::swap(lamA, lamF);
     }
-    AD_CUDA(cudaGetLastError());
-    AD_CUDA(cudaEventRecord(w.ev[1], q));
-    AD_CUDA(cudaEventSynchronize(w.ev[1]));
-    ms_re += elapsed(w.ev[2], w.ev[3]);
-    ms_adj += elapsed(w.ev[3], w.ev[1]);
+    return NMHD_OK;
+  };
+  AD_CUDA(cudaEventRecord(w.ev[2], q));
+  // the recomputation reads the checkpoints and frozen time steps written on q
+  AD_CUDA(cudaEventRecord(w.fwd_done, q));
+  AD_CUDA(cudaStreamWaitEvent(q2, w.fwd_done, 0));
+  // neither slot holds a segment still to be swept yet
+  for (int i = 0; i < 2; ++i) AD_CUDA(cudaEventRecord(w.slot_free[i], q));
+  if (nrec > 0) {
+    st = recompute(nrec - 1);
+    if (st != NMHD_OK) return st;
   }
+  for (int seg = nseg - 1; seg >= 0; --seg) {
+    const int n0 = seg * K;
+    if (n0 >= kept0) {  // taped by the forward run
+      st = sweep(seg, tape + (size_t)(n0 - kept0) * kTapeFields * n);
+      if (st != NMHD_OK) return st;
+      if (n0 == kept0) AD_CUDA(cudaEventRecord(w.slot_free[1], q));  // tape slot 0 swept
+      continue;
+    }
+    const int si = (nrec - 1 - seg) % 2;
+    if (seg > 0) {  // the next recomputation overlaps this segment's sweep
+      st = recompute(seg - 1);
+      if (st != NMHD_OK) return st;
+    }
+    AD_CUDA(cudaStreamWaitEvent(q, w.slot_ready[si], 0));
+    st = sweep(seg, slots[si]);
+    if (st != NMHD_OK) return st;
+    AD_CUDA(cudaEventRecord(w.slot_free[si], q));
+  }
+  AD_CUDA(cudaGetLastError());
+  AD_CUDA(cudaEventRecord(w.ev[3], q));
+  AD_CUDA(cudaEventSynchronize(w.ev[3]));
+  double ms_re = 0.0;
+  for (int j = 0; j < nrec; ++j) ms_re += elapsed(rev[2 * j], rev[2 * j + 1]);
+  for (auto &e : rev) cudaEventDestroy(e);
+  const double ms_rev = elapsed(w.ev[2], w.ev[3]);
   if (in_window(L, 0)) ex.cells(gg, OpAStress<R>{gg, ckpt, lamA, scale});
   for (int v = 0; v < 8; ++v)
     AD_CUDA(cudaMemcpyAsync(grad[v], lamA + (size_t)v * n, sizeof(R) * n,
                             grad_on_device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost, q));
   AD_CUDA(cudaStreamSynchronize(q));
   w.ms[1] = ms_re;
-  w.ms[2] = ms_adj;
-  w.ms[3] = w.ms[0] + ms_re + ms_adj;
+  w.ms[2] = ms_rev;
+  w.ms[3] = w.ms[0] + ms_rev;
   return NMHD_OK;
 }
 
@@ -509,6 +591,16 @@ void nmhd_adjoint_release(nmhd_solver *s) {
   cudaFree(w->hist_dummy);
   for (auto &e : w->ev)
     if (e) cudaEventDestroy(e);
+  if (w->stream2) {
+    cudaStreamSynchronize(w->stream2);
+    cudaStreamDestroy(w->stream2);
+  }
+  if (w->hstage) cudaFreeHost(w->hstage);
+  for (int i = 0; i < 2; ++i) {
+    if (w->slot_ready[i]) cudaEventDestroy(w->slot_ready[i]);
+    if (w->slot_free[i]) cudaEventDestroy(w->slot_free[i]);
+  }
+  if (w->fwd_done) cudaEventDestroy(w->fwd_done);
   delete w;
   s->adjoint = nullptr;
 }

@@ -375,7 +375,10 @@ class MHDSolver:
         return int(self._L.nmhd_adjoint_kept_segments(self._h))
 
     def adjoint_timing(self):
-        """Device ms of the last adjoint run: forward, recompute, adjoint, total."""
+        """Device ms of the last adjoint run: forward (with checkpoints),
+        recompute (segment recomputation on its own stream, overlapping the
+        reverse sweep), adjoint (the reverse sweep), total (forward + reverse
+        sweep)."""
         ms = np.zeros(4, np.float64)
         _check(self._L, self._h, self._L.nmhd_adjoint_timing(self._h, ms.ctypes.data))
         return {"forward": ms[0], "recompute": ms[1], "adjoint": ms[2], "total": ms[3]}
