@@ -517,7 +517,14 @@ def ensemble_measure(workload, steps, warmup, dev, rank=0, world=1, dist=None, n
     batch.step(warmup)
     # schedule of each stage kernel (persistent or one tile per CTA), timed on these boxes
     tuning = batch.autotune(reps=3)
-    schedule = {("flux", "ct", "update")[k]: ("persistent" if p else "per_tile") + ("_split" if s else "")
+    names = ("flux", "ct", "update", "fused")
+
+    def sched(k, p, s):
+        if k == 3:
+            return ("persistent" if p else "per_tile") if s else "off"
+        return ("persistent" if p else "per_tile") + ("_split" if s else "")
+
+    schedule = {names[k]: sched(k, p, s)
                 for k, p, s, ms in tuning if ms == min(m for kk, _, _, m in tuning if kk == k)}
     batch.prepare(steps)
     batch.step(warmup)
@@ -581,9 +588,7 @@ def ensemble_measure(workload, steps, warmup, dev, rank=0, world=1, dist=None, n
         sol.close()
     return {"value": value, "unit": "Mcell-updates/s", "steps": steps, "ms_per_step": ms / steps,
             "boxes": len(all_boxes), "cells_interior": total_interior, "schedule": schedule,
-            "autotune_ms_per_launch": {"%s_%s%s" % (("flux", "ct", "update")[k],
-                                                    "persistent" if p else "per_tile",
-                                                    "_split" if s else ""): round(ms_, 4)
+            "autotune_ms_per_launch": {"%s_%s" % (names[k], sched(k, p, s)): round(ms_, 4)
                                        for k, p, s, ms_ in tuning},
             "plain_per_box": {"value": plain_v, "unit": "Mcell-updates/s", "steps": plain_steps,
                               "note": "same boxes, one single-box solver each, stepped one after another"},

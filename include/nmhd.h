@@ -282,15 +282,22 @@ int nmhd_batch_launches_per_step(const nmhd_batch *b);
  * ranges, 0 for one tile per CTA (the default); split = 1 (the default) runs
  * the boxes with 32 x 4 x 2 tiles in a launch of their own through a kernel
  * compiled for that shape (fewer registers), 0 runs every box in one launch of
- * the general form (half the launches: better for many small boxes). */
+ * the general form (half the launches: better for many small boxes).
+ * kernel = 3 is the fused pass: split = 1 runs constrained transport and the
+ * conserved update of the 32 x 4 x 2 boxes as one kernel (the single-box fused
+ * epilogue; it takes effect while kernels 1 and 2 are split), persistent its
+ * schedule; split = 0 (the default) turns it off. */
 nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split);
 /* Schedule autotuner of the batch (the batched counterpart of nmhd_autotune).
  * Times `reps` launches of each stage kernel (face fluxes, constrained
  * transport, conserved update) in every schedule (persistent or not, split or
  * not) on the boxes' current states with CUDA events, keeps the fastest per
- * kernel, and leaves states and clocks unchanged.  trials_out (may be NULL)
- * receives up to max_trials rows of (kernel, persistent, split, ms per
- * launch).  Returns the number of rows written or a negative nmhd_status.
+ * kernel, then times the stage update (kernels 1 and 2) against the fused
+ * pass, one tile per CTA and persistent, and keeps the fastest; states and
+ * clocks are left unchanged.  trials_out (may be NULL) receives up to
+ * max_trials rows of (kernel, persistent, split, ms per launch), the fused
+ * comparison as rows (3, persistent, fused, ms per stage update).  Returns the
+ * number of rows written or a negative nmhd_status.
  * Every schedule gives bitwise the same result. */
 int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_trials);
 const char *nmhd_batch_last_error(const nmhd_batch *b);

@@ -22,7 +22,7 @@
 #include <vector>
 
 #include "../../include/nmhd.h"
-#include "cell_ops.cuh"
+#include "cell_epilogue.cuh"
 #include "margin_ops.cuh"
 
 namespace nmhd {
@@ -179,6 +179,54 @@ __global__ void __launch_bounds__(kThreads, KIND == 0   ? NMHD_BATCH_MIN_BLOCKS_
   }
 }
 
+// Constrained transport and conserved update of the boxes with 32 x 4 x 2
+// tiles in one pass per tile: the single-box fused epilogue
+// (cell_epilogue.cuh, staging with cp.async), tiles [tb, te) of the group,
+// persistent or one tile per CTA.
+#ifndef NMHD_BATCH_MIN_BLOCKS_EPI
+#define NMHD_BATCH_MIN_BLOCKS_EPI 5
+#endif
+template <bool kPersist>
+__global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_EPI)
+    k_batch_epilogue(const __grid_constant__ BatchGroup p, int tb, int te, int in_sel, int out_sel, int half,
+                     int final_stage) {
+  __shared__ cell::epi::Smem s;
+  auto tile = [&](const BoxDesc &d, int t) {
+    StepCtl *ctl = d.ctl;
+    const int lt = t - d.tile_begin;
+    const int x0 = lt % d.tiles_x << 5, y0 = lt / d.tiles_x % d.tiles_y << 2, z0 = lt / (d.tiles_x * d.tiles_y) << 1;
+    float dt = step_dt(ctl, nullptr);
+    if (half) dt = dt / 2.0f;
+    const float *win = pick(ctl, in_sel, d.w0, d.w1, d.wp), *wb = pick(ctl, 0, d.w0, d.w1, d.wp);
+    float *wo = const_cast<float *>(pick(ctl, out_sel, d.w0, d.w1, d.wp));
+    int bad = 0, timed_out = 0;
+    const float tcfl =
+        d.g.pow2_spacing
+            ? cell::epi::tile_epilogue<true>(s, d.g, nullptr, 0, 0, win, wb, wo, d.flux, x0, y0, z0, dt,
+                                            final_stage != 0, &bad, &timed_out)
+            : cell::epi::tile_epilogue<false>(s, d.g, nullptr, 0, 0, win, wb, wo, d.flux, x0, y0, z0, dt,
+                                             final_stage != 0, &bad, &timed_out);
+    if (final_stage) finish_tile(ctl, (unsigned)(d.tiles_x * d.tiles_y * d.tiles_z), tcfl, bad, d.dt_hist, s.red);
+  };
+  if (!kPersist) {
+    const int t = tb + blockIdx.x;
+    const BoxDesc &d = p.box[group_box(p, t)];
+    if (d.ctl->done) return;
+    tile(d, t);
+    return;
+  }
+  const int t0 = tb + (int)((long long)(te - tb) * blockIdx.x / gridDim.x);
+  const int t1 = tb + (int)((long long)(te - tb) * (blockIdx.x + 1) / gridDim.x);
+  int b = group_box(p, t0);
+  for (int t = t0; t < t1; ++t) {
+    while (t >= p.tile_begin[b + 1]) ++b;
+    const BoxDesc &d = p.box[b];
+    if (d.ctl->done) continue;
+    tile(d, t);
+    __syncthreads();  // the next tile overwrites the shared tile
+  }
+}
+
 // Shearing-periodic Y-margin fill of every box (margin_ops.cuh).
 __global__ void __launch_bounds__(256) k_batch_fill(const BoxDesc *__restrict__ boxes, int nb, long long total) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
@@ -246,7 +294,10 @@ struct nmhd_batch {
   std::vector<nmhd::BatchGroup> groups;  // launch groups of at most kGroupBoxes boxes
   bool persist[3] = {false, false, false};  // schedule of each stage kernel (nmhd_batch_autotune)
   bool split[3] = {true, true, true};       // boxes with 32 x 4 x 2 tiles in a launch of their own
-  int ctas[3] = {0, 0, 0};                  // resident CTAs of each persistent stage kernel
+  // with split constrained transport and update: the 32 x 4 x 2 boxes take
+  // both in one fused pass (k_batch_epilogue), persistent or one tile per CTA
+  bool fuse = false, persist_fused = false;
+  int ctas[4] = {0, 0, 0, 0};               // resident CTAs of each persistent stage kernel ([3]: fused)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
@@ -321,12 +372,47 @@ void launch_stage(const nmhd::BatchGroup &p, bool persist, bool split, int ctas,
   }
 }
 
-// Kernel `kind` of one stage over every group.
+bool fused(const nmhd_batch *b) { return b->fuse && b->split[1] && b->split[2]; }
+
+// Kernel `kind` of one stage over every group.  Fused: kind 1 covers the
+// boxes with general tiles only, kind 2 the fused pass of the 32 x 4 x 2
+// boxes and the update of the others.
 void launch_kind(nmhd_batch *b, int kind, int in_sel, int out_sel, int half, int fin) {
+  const dim3 blk(nmhd::cell::kThreads);
   for (const BatchGroup &p : b->groups) {
-    if (kind == 0) launch_stage<0>(p, b->persist[0], b->split[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
-    else if (kind == 1) launch_stage<1>(p, b->persist[1], b->split[1], b->ctas[1], b->stream, in_sel, out_sel, half, fin);
-    else launch_stage<2>(p, b->persist[2], b->split[2], b->ctas[2], b->stream, in_sel, out_sel, half, fin);
+    if (kind == 0) {
+      launch_stage<0>(p, b->persist[0], b->split[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
+    } else if (fused(b)) {
+      const int tb = p.fixed_tiles, te = p.total_tiles;
+      if (kind == 1 && te > tb) {
+        if (b->persist[1])
+          nmhd::k_batch_stage<1, true, false><<<std::min(b->ctas[1], te - tb), blk, 0, b->stream>>>(
+              p, tb, te, in_sel, out_sel, half, fin);
+        else
+          nmhd::k_batch_stage<1, false, false><<<te - tb, blk, 0, b->stream>>>(p, tb, te, in_sel, out_sel, half, fin);
+      }
+      if (kind == 2) {
+        if (p.fixed_tiles > 0) {
+          if (b->persist_fused)
+            nmhd::k_batch_epilogue<true><<<std::min(b->ctas[3], p.fixed_tiles), blk, 0, b->stream>>>(
+                p, 0, p.fixed_tiles, in_sel, out_sel, half, fin);
+          else
+            nmhd::k_batch_epilogue<false><<<p.fixed_tiles, blk, 0, b->stream>>>(p, 0, p.fixed_tiles, in_sel,
+                                                                                 out_sel, half, fin);
+        }
+        if (te > tb) {
+          if (b->persist[2])
+            nmhd::k_batch_stage<2, true, false><<<std::min(b->ctas[2], te - tb), blk, 0, b->stream>>>(
+                p, tb, te, in_sel, out_sel, half, fin);
+          else
+            nmhd::k_batch_stage<2, false, false><<<te - tb, blk, 0, b->stream>>>(p, tb, te, in_sel, out_sel, half, fin);
+        }
+      }
+    } else if (kind == 1) {
+      launch_stage<1>(p, b->persist[1], b->split[1], b->ctas[1], b->stream, in_sel, out_sel, half, fin);
+    } else {
+      launch_stage<2>(p, b->persist[2], b->split[2], b->ctas[2], b->stream, in_sel, out_sel, half, fin);
+    }
   }
 }
 
@@ -463,11 +549,12 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
   // persistent schedule: as many CTAs as fit on the GPU at once
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  int occ[3] = {1, 1, 1};
+  int occ[4] = {1, 1, 1, 1};
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0, true, false>, nmhd::cell::kThreads, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1, true, false>, nmhd::cell::kThreads, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2, true, false>, nmhd::cell::kThreads, 0);
-  for (int k = 0; k < 3; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], nmhd::k_batch_epilogue<true>, nmhd::cell::kThreads, 0);
+  for (int k = 0; k < 4; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
   // launch groups: consecutive boxes, tiles numbered from 0 within a group,
   // the boxes with 32 x 4 x 2 tiles first
   for (int i0 = 0; i0 < n; i0 += nmhd::kGroupBoxes) {
@@ -694,9 +781,14 @@ nmhd_status nmhd_batch_prepare(nmhd_batch *b, int64_t max_steps) {
 int nmhd_batch_launches_per_step(const nmhd_batch *b) {
   if (!b) return NMHD_ERR_INVALID_ARGUMENT;
   int n = (b->total_fill > 0) + (b->total_mcfl > 0);
-  for (int kind = 0; kind < 3; ++kind)
-    for (const BatchGroup &p : b->groups)
-      n += 2 * (b->split[kind] ? (p.fixed_tiles > 0) + (p.total_tiles > p.fixed_tiles) : 1);
+  for (const BatchGroup &p : b->groups) {
+    const int fixed = p.fixed_tiles > 0, general = p.total_tiles > p.fixed_tiles;
+    n += 2 * (b->split[0] ? fixed + general : 1);
+    if (fused(b))  // per stage: CT of the general boxes, the fused pass, the general update
+      n += 2 * (general + fixed + general);
+    else
+      for (int kind = 1; kind < 3; ++kind) n += 2 * (b->split[kind] ? fixed + general : 1);
+  }
   return n;
 }
 
@@ -733,11 +825,16 @@ nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int
 }
 
 nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split) {
-  if (!b || kernel < 0 || kernel > 2 || (persistent != 0 && persistent != 1) || (split != 0 && split != 1))
-    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..2, persistent and split 0 or 1");
+  if (!b || kernel < 0 || kernel > 3 || (persistent != 0 && persistent != 1) || (split != 0 && split != 1))
+    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..3, persistent and split 0 or 1");
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
-  b->persist[kernel] = persistent != 0;
-  b->split[kernel] = split != 0;
+  if (kernel == 3) {  // the fused pass: on (split = 1) or off, and its schedule
+    b->fuse = split != 0;
+    b->persist_fused = persistent != 0;
+  } else {
+    b->persist[kernel] = persistent != 0;
+    b->split[kernel] = split != 0;
+  }
   for (auto &kv : b->graphs) cudaGraphExecDestroy(kv.second);
   b->graphs.clear();
   return NMHD_OK;
@@ -772,6 +869,8 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
   // and the clocks alone, so each can be launched again and again on it.
   const bool saved[3] = {b->persist[0], b->persist[1], b->persist[2]};
   const bool saved_split[3] = {b->split[0], b->split[1], b->split[2]};
+  const bool saved_fuse = b->fuse, saved_pf = b->persist_fused;
+  b->fuse = false;  // each kernel alone first; the fused pass is compared last
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -809,11 +908,59 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
     b->persist[kind] = choice;
     b->split[kind] = choice_split;
   }
+  // The stage's update (constrained transport, then conserved update) with
+  // the chosen schedules, against the fused pass for the 32 x 4 x 2 boxes
+  // (both kernels split), one tile per CTA or persistent: rows of kernel 3,
+  // (3, persistent, fused, ms per update).
+  {
+    const bool keep_split[2] = {b->split[1], b->split[2]};
+    double best = 1e30;
+    bool best_fuse = false, best_pf = false, any_fixed = false;
+    for (const BatchGroup &p : b->groups) any_fixed = any_fixed || p.fixed_tiles > 0;
+    for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {
+      const int f = trial > 0, pf = trial == 2;
+      if (f && !any_fixed) break;
+      b->fuse = f != 0;
+      b->persist_fused = pf != 0;
+      if (f) b->split[1] = b->split[2] = true;
+      launch_kind(b, 1, 0, 2, 1, 0);  // warm-up
+      launch_kind(b, 2, 0, 2, 1, 0);
+      e = cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) {
+        launch_kind(b, 1, 0, 2, 1, 0);
+        launch_kind(b, 2, 0, 2, 1, 0);
+      }
+      if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      const double per = ms / reps;
+      if (trials_out && written < max_trials) {
+        trials_out[4 * written + 0] = 3;
+        trials_out[4 * written + 1] = pf;
+        trials_out[4 * written + 2] = f;
+        trials_out[4 * written + 3] = per;
+        ++written;
+      }
+      if (per < best) {
+        best = per;
+        best_fuse = f != 0;
+        best_pf = pf != 0;
+      }
+      if (f) b->split[1] = keep_split[0], b->split[2] = keep_split[1];
+    }
+    b->fuse = best_fuse;
+    b->persist_fused = best_pf;
+    if (best_fuse) b->split[1] = b->split[2] = true;
+  }
   if (e0) cudaEventDestroy(e0);
   if (e1) cudaEventDestroy(e1);
   if (e == cudaSuccess) e = cudaGetLastError();
   if (e != cudaSuccess) {
     for (int k = 0; k < 3; ++k) b->persist[k] = saved[k], b->split[k] = saved_split[k];
+    b->fuse = saved_fuse;
+    b->persist_fused = saved_pf;
     return bfail(b, NMHD_ERR_CUDA, std::string("nmhd_batch_autotune: ") + cudaGetErrorString(e));
   }
   // the graphs hold the previous schedules

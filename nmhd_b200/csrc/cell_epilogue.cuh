@@ -163,21 +163,25 @@ __device__ __forceinline__ bool mbar_wait_bounded(unsigned mbar) {
 // strides of N after it) into shared memory at dst (a shared-space address;
 // field f at dst + 4 * f * B::N) with asynchronous copies, so every copy of
 // the tile is issued before the first is waited for.
-//  vec (the tile needs no periodic wrap in x and rows are 16-byte aligned,
-//  Sx % 4 == 0): whole padded rows, x0 + OI - XO .. + P - 1, 16 bytes per
-//  copy, the tile's threads over all (row, 16-byte chunk) pairs;
+//  vec (rows 16-byte aligned, Sx % 4 == 0): whole padded rows, x0 + OI - XO
+//  .. + P - 1, 16 bytes per copy, the tile's threads over all (row, 16-byte
+//  chunk) pairs; a chunk that lies beyond an x edge of the box is the chunk
+//  Sx away (the periodic wrap moves whole, still aligned, 4-float chunks);
 //  otherwise: entry by entry, one row per warp at a time (the row's y and z
 //  offsets warp-uniform, a lane's x offsets from the wrapped table).
 template <class B, int F>
 __device__ __forceinline__ void load_box(const Smem &s, unsigned dst, const float *__restrict__ src, size_t N,
-                                         int x0, bool vec, int tid) {
+                                         int x0, int nx, bool vec, int tid) {
   if (vec) {
     constexpr int PV = B::P / 4, R = B::NJ * B::NK;
-    const float *src0 = src + (x0 + B::OI - B::XO);
+    const int xs = x0 + B::OI - B::XO;
     for (int e = tid; e < R * PV; e += kThreads) {
       const int r = e / PV, v = e - r * PV;
       const int j = r % B::NJ, k = r / B::NJ;
-      const float *p = src0 + (s.gz[k + B::OK + 1] + s.gy[j + B::OJ + 1] + 4 * v);
+      int xw = xs + 4 * v;  // a multiple of 4 in [-4, Sx + 35]: wrap into [0, Sx)
+      if (xw < 0) xw += nx;
+      if (xw >= nx) xw %= nx;
+      const float *p = src + (s.gz[k + B::OK + 1] + s.gy[j + B::OJ + 1] + xw);
       const unsigned d = dst + 16u * (r * PV + v);
 #pragma unroll
       for (int f = 0; f < F; ++f) cp_async16(d + 4u * (f * B::N), p + f * N);
@@ -412,22 +416,28 @@ __device__ __forceinline__ float finish_cell(const Smem &s, const GridParams &g,
 }
 
 // The whole epilogue of one tile at (x0, y0, z0); every thread of the CTA
-// calls it.  win: stage input (velocities), wb: state at the start of the
-// step, wo: stage output.  Returns the thread's CFL time (inf if none).
+// calls it.  maps: the tensor maps of these buffers (interior tiles stage by
+// tensor copies), or NULL (every tile stages with cp.async).  win: stage
+// input (velocities), wb: state at the start of the step, wo: stage output.
+// Returns the thread's CFL time (inf if none).
 template <bool kPow2>
-__device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, const EpiMaps &maps, int in_buf,
+__device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, const EpiMaps *maps, int in_buf,
                                                int base_buf, const float *__restrict__ win,
                                                const float *__restrict__ wb, float *__restrict__ wo,
                                                const float *__restrict__ flux, int x0, int y0, int z0, float dt,
                                                bool final_stage, int *bad, int *timed_out) {
+  // the thread's cell (a, b, c) of the tile, from its linear index: the same
+  // for a 32 x 4 x 2 block (the single-box kernel) and a 1-D block of 256
+  // threads (the batched kernel)
   const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
+  const int a = tid % BX, b = tid / BX % BY, c = tid / (BX * BY);
   const size_t N = (size_t)g.n;
   {
     // L2 prefetch of the lines the cell update reads later: each warp holds
     // one x row of 32 cells (one 128-byte line per field), lanes 0-14 take
     // the 15 mass/momentum/energy face-flux fields, lanes 15-22 the 8 fields
     // of the step's state
-    const int lane = tid & 31, y = y0 + threadIdx.y, z = z0 + threadIdx.z;
+    const int lane = tid & 31, y = y0 + b, z = z0 + c;
     if (lane < 23 && y < g.sy && z < g.sz) {
       const size_t o = (size_t)(z * g.sy + y) * g.sx + x0;
       const float *p = lane < 15 ? flux + (size_t)(lane / 5 * 7 + lane % 5) * N + o : wb + (size_t)(lane - 15) * N + o;
@@ -441,7 +451,7 @@ __device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, con
   // the box need no periodic wrap: one thread stages all of them with ten
   // tensor copies.  The others stage entry by entry through the wrapped
   // offset tables (16-byte row chunks when only y or z wraps).
-  const bool tma = maps.enabled && x0 >= 4 && x0 + 36 <= g.sx && y0 >= 1 && y0 + 5 <= g.sy && z0 >= 1 &&
+  const bool tma = maps && maps->enabled && x0 >= 4 && x0 + 36 <= g.sx && y0 >= 1 && y0 + 5 <= g.sy && z0 >= 1 &&
                    z0 + 3 <= g.sz;
   if (tma) {
     if (tid == 0) {
@@ -450,16 +460,16 @@ __device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, con
       asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
       asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(mb), "r"(kTileTxBytes)
                    : "memory");
-      tma_box<VelBox>(vs, &maps.vel[in_buf], x0, y0, z0, 1, mb);
-      tma_box<XYF>(bs + 4 * kXY, &maps.xy, x0, y0, z0, 5, mb);
-      tma_box<YXF>(bs + 4 * kYX, &maps.yx, x0, y0, z0, 13, mb);
-      tma_box<XZF>(bs + 4 * kXZ, &maps.xz, x0, y0, z0, 6, mb);
-      tma_box<ZXF>(bs + 4 * kZX, &maps.zx, x0, y0, z0, 19, mb);
-      tma_box<YZF>(bs + 4 * kYZ, &maps.yz, x0, y0, z0, 12, mb);
-      tma_box<ZYF>(bs + 4 * kZY, &maps.zy, x0, y0, z0, 20, mb);
-      tma_box<BXs>(ws + 4 * fBX, &maps.bx[base_buf], x0, y0, z0, 5, mb);
-      tma_box<BYs>(ws + 4 * fBY, &maps.by[base_buf], x0, y0, z0, 6, mb);
-      tma_box<BZs>(ws + 4 * fBZ, &maps.bz[base_buf], x0, y0, z0, 7, mb);
+      tma_box<VelBox>(vs, &maps->vel[in_buf], x0, y0, z0, 1, mb);
+      tma_box<XYF>(bs + 4 * kXY, &maps->xy, x0, y0, z0, 5, mb);
+      tma_box<YXF>(bs + 4 * kYX, &maps->yx, x0, y0, z0, 13, mb);
+      tma_box<XZF>(bs + 4 * kXZ, &maps->xz, x0, y0, z0, 6, mb);
+      tma_box<ZXF>(bs + 4 * kZX, &maps->zx, x0, y0, z0, 19, mb);
+      tma_box<YZF>(bs + 4 * kYZ, &maps->yz, x0, y0, z0, 12, mb);
+      tma_box<ZYF>(bs + 4 * kZY, &maps->zy, x0, y0, z0, 20, mb);
+      tma_box<BXs>(ws + 4 * fBX, &maps->bx[base_buf], x0, y0, z0, 5, mb);
+      tma_box<BYs>(ws + 4 * fBY, &maps->by[base_buf], x0, y0, z0, 6, mb);
+      tma_box<BZs>(ws + 4 * fBZ, &maps->bz[base_buf], x0, y0, z0, 7, mb);
     }
   } else {
     if (tid < 34) s.gx[tid] = wrap_any(x0 - 1 + tid, g.sx);
@@ -484,27 +494,25 @@ __device__ __forceinline__ float tile_epilogue(Smem &s, const GridParams &g, con
     // every thread has passed the wait: the barrier's word is released
     if (tid == 0) asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(mb) : "memory");
   } else {
-    // whole 16-byte row chunks: no periodic wrap in x (the padded rows span
-    // x0 - 4 .. x0 + 35) and 16-byte aligned rows
-    const bool vec = x0 >= 1 && x0 + 32 < g.sx && (g.sx & 3) == 0;
-    load_box<VelBox, 3>(s, vs, win + N, N, x0, vec, tid);
-    load_box<XYF, 1>(s, bs + 4 * kXY, flux + 5 * N, N, x0, vec, tid);
-    load_box<YXF, 1>(s, bs + 4 * kYX, flux + 13 * N, N, x0, vec, tid);
-    load_box<XZF, 1>(s, bs + 4 * kXZ, flux + 6 * N, N, x0, vec, tid);
-    load_box<ZXF, 1>(s, bs + 4 * kZX, flux + 19 * N, N, x0, vec, tid);
-    load_box<YZF, 1>(s, bs + 4 * kYZ, flux + 12 * N, N, x0, vec, tid);
-    load_box<ZYF, 1>(s, bs + 4 * kZY, flux + 20 * N, N, x0, vec, tid);
-    load_box<BXs, 1>(s, ws + 4 * fBX, wb + 5 * N, N, x0, vec, tid);
-    load_box<BYs, 1>(s, ws + 4 * fBY, wb + 6 * N, N, x0, vec, tid);
-    load_box<BZs, 1>(s, ws + 4 * fBZ, wb + 7 * N, N, x0, vec, tid);
+    // whole 16-byte row chunks where rows are 16-byte aligned
+    const bool vec = (g.sx & 3) == 0;
+    load_box<VelBox, 3>(s, vs, win + N, N, x0, g.sx, vec, tid);
+    load_box<XYF, 1>(s, bs + 4 * kXY, flux + 5 * N, N, x0, g.sx, vec, tid);
+    load_box<YXF, 1>(s, bs + 4 * kYX, flux + 13 * N, N, x0, g.sx, vec, tid);
+    load_box<XZF, 1>(s, bs + 4 * kXZ, flux + 6 * N, N, x0, g.sx, vec, tid);
+    load_box<ZXF, 1>(s, bs + 4 * kZX, flux + 19 * N, N, x0, g.sx, vec, tid);
+    load_box<YZF, 1>(s, bs + 4 * kYZ, flux + 12 * N, N, x0, g.sx, vec, tid);
+    load_box<ZYF, 1>(s, bs + 4 * kZY, flux + 20 * N, N, x0, g.sx, vec, tid);
+    load_box<BXs, 1>(s, ws + 4 * fBX, wb + 5 * N, N, x0, g.sx, vec, tid);
+    load_box<BYs, 1>(s, ws + 4 * fBY, wb + 6 * N, N, x0, g.sx, vec, tid);
+    load_box<BZs, 1>(s, ws + 4 * fBZ, wb + 7 * N, N, x0, g.sx, vec, tid);
     cp_async_wait_all();
     __syncthreads();
   }
-  corner_emfs(s, threadIdx.x, threadIdx.y, threadIdx.z, warp, lane, tid);
+  corner_emfs(s, a, b, c, warp, lane, tid);
   __syncthreads();
-  face_b<kPow2>(s, g, threadIdx.x, threadIdx.y, threadIdx.z, warp, lane, dt);
+  face_b<kPow2>(s, g, a, b, c, warp, lane, dt);
   __syncthreads();
-  const int a = threadIdx.x, b = threadIdx.y, c = threadIdx.z;
   const int x = x0 + a, y = y0 + b, z = z0 + c;
   if (x < g.sx && y < g.sy && z < g.sz)
     return finish_cell<kPow2>(s, g, wb, wo, flux, a, b, c, x, y, z, dt, final_stage, bad);

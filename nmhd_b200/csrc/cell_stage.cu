@@ -135,7 +135,7 @@ __global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
   const float *win = pick(ctl, in_sel, w0, w1, wp), *wb = pick(ctl, 0, w0, w1, wp);
   float *wo = const_cast<float *>(pick(ctl, out_sel, w0, w1, wp));
   int bad = 0, timed_out = 0;
-  const float tcfl = epi::tile_epilogue<kPow2>(s, g, maps, pick_index(ctl, in_sel), pick_index(ctl, 0), win, wb, wo,
+  const float tcfl = epi::tile_epilogue<kPow2>(s, g, &maps, pick_index(ctl, in_sel), pick_index(ctl, 0), win, wb, wo,
                                                flux, blockIdx.x * BX, blockIdx.y * BY, blockIdx.z * BZ, dt,
                                                final_stage != 0, &bad, &timed_out);
   if (timed_out && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
