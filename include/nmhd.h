@@ -179,10 +179,14 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
  * per-cell kernels on 32x4x2 blocks; variant 3: the variant-2
  * kernels as a pipeline over chunks of z_chunk planes, so each chunk's face
  * fluxes are read back from L2 (nmhd_profile then times each whole stage as
- * its flux class); variant 4 (the default): the variant-2 flux kernel, then
+ * its flux class); variant 4: the variant-2 flux kernel, then
  * constrained transport and the conserved update fused in one kernel per
  * stage (corner EMFs and new face B of a 32x4x2 tile in shared memory, its
- * inputs staged by tensor copies).  tile_rows is used
+ * inputs staged by tensor copies); variant 5 (the default): the variant-4
+ * update after a flux kernel that first copies each 32x4x2 tile's stencil of
+ * the stage input (all 8 fields, two cells around) into shared memory.  With
+ * NMHD_FLAG_FAST_ARITHMETIC variants 2, 4 and 5 run the fast flux kernel
+ * (5 is then 4) and the others are refused.  tile_rows is used
  * by variant 0 only, z_chunk by variants 0 and 3.  Every variant gives
  * bitwise identical results. */
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk);

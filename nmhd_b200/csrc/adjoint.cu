@@ -314,13 +314,15 @@ void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl,
     nmhd::launch_fill(g, w.ctl, b0, b1, st);
     if (cfl) nmhd::launch_cfl_margin(g, w.ctl, b0, b1, st);
   }
+  // the default kernels (variant 5), staging by cp.async: the tape's
+  // buffers change from step to step, so no tensor maps
   if (s->cfg.time_order == 1) {
-    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, st);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, nullptr, st);
     nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, nullptr, st);
   } else {
-    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, st);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, nullptr, st);
     nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, nullptr, st);
-    nmhd::launch_cell_flux(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, st);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, nullptr, st);
     nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, nullptr, st);
   }
   w.parity ^= 1;

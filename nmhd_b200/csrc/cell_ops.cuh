@@ -66,42 +66,53 @@ __device__ __forceinline__ float step_dt(const StepCtl *c, bool *last) {
   return dt;
 }
 
+// Loads of face_flux's inputs: read-only global memory (the stage input in
+// HBM) or a plain load (a shared-memory copy of it).
+struct GlobalLd {
+  __device__ static __forceinline__ float ld(const float *p) { return __ldg(p); }
+};
+struct SharedLd {
+  __device__ static __forceinline__ float ld(const float *p) { return *p; }
+};
+
 // Flux through the lower face of cell o along runtime axis `ax` (one HLLD
-// instance serves all three axes).  m2, m1, p1: offsets of the stencil cells
-// -2, -1, +1 along ax; t1, t2: +1 offsets along the transverse axes ax+1 and
-// ax+2 (mod 3).  The 7 results go to flux + (7*ax + k)*N + o: mass, momentum
-// x/y/z (absolute components), energy, F(B_t1), F(B_t2)
+// instance serves all three axes).  The inputs are read at w + f*NW + o + d
+// (field f, stencil offset d): m2, m1, p1 are the offsets of the stencil
+// cells -2, -1, +1 along ax; t1, t2 the +1 offsets along the transverse axes
+// ax+1 and ax+2 (mod 3).  The 7 results go to flux + (7*ax + k)*N + oo:
+// mass, momentum x/y/z (absolute components), energy, F(B_t1), F(B_t2)
 // (calc_flux_kernel<EX>, src/library/mhd_solver.inlrb:562-636).
-__device__ __forceinline__ void face_flux(const GridParams &g, const float *__restrict__ w, size_t N, int o,
-                                          int ax, int m2, int m1, int p1, int t1, int t2, int yidx,
-                                          float dt, float *__restrict__ flux) {
+template <class L = GlobalLd, class S = size_t>
+__device__ __forceinline__ void face_flux(const GridParams &g, const float *__restrict__ w, S NW, int o, int ax,
+                                          int m2, int m1, int p1, int t1, int t2, int yidx, float dt,
+                                          float *__restrict__ flux, size_t N, int oo) {
   const int e1 = ax == 2 ? 0 : ax + 1, e2 = ax == 0 ? 2 : ax - 1;
-  const float *rho = w, *p = w + 4 * N;
-  const float *vn = w + (1 + ax) * N, *v1 = w + (1 + e1) * N, *v2 = w + (1 + e2) * N;
-  const float *bn = w + (5 + ax) * N, *b1 = w + (5 + e1) * N, *b2 = w + (5 + e2) * N;
+  const float *rho = w, *p = w + 4 * NW;
+  const float *vn = w + (1 + ax) * NW, *v1 = w + (1 + e1) * NW, *v2 = w + (1 + e2) * NW;
+  const float *bn = w + (5 + ax) * NW, *b1 = w + (5 + e1) * NW, *b2 = w + (5 + e2) * NW;
   const int s[4] = {m2, m1, 0, p1};
   float bc1[4], bc2[4];
 #pragma unroll
   for (int t = 0; t < 4; ++t) {
     const int c = o + s[t];
-    bc1[t] = 0.5f * (__ldg(b1 + c) + __ldg(b1 + c + t1));
-    bc2[t] = 0.5f * (__ldg(b2 + c) + __ldg(b2 + c + t2));
+    bc1[t] = 0.5f * (L::ld(b1 + c) + L::ld(b1 + c + t1));
+    bc2[t] = 0.5f * (L::ld(b2 + c) + L::ld(b2 + c + t2));
   }
   HlldIn in;
   if (g.order2) {
-    reconstruct4(__ldg(rho + o + m2), __ldg(rho + o + m1), __ldg(rho + o), __ldg(rho + o + p1), in.dl, in.dr);
-    reconstruct4(__ldg(vn + o + m2), __ldg(vn + o + m1), __ldg(vn + o), __ldg(vn + o + p1), in.ul, in.ur);
-    reconstruct4(__ldg(v1 + o + m2), __ldg(v1 + o + m1), __ldg(v1 + o), __ldg(v1 + o + p1), in.vl, in.vr);
-    reconstruct4(__ldg(v2 + o + m2), __ldg(v2 + o + m1), __ldg(v2 + o), __ldg(v2 + o + p1), in.wl, in.wr);
-    reconstruct4(__ldg(p + o + m2), __ldg(p + o + m1), __ldg(p + o), __ldg(p + o + p1), in.pl, in.pr);
+    reconstruct4(L::ld(rho + o + m2), L::ld(rho + o + m1), L::ld(rho + o), L::ld(rho + o + p1), in.dl, in.dr);
+    reconstruct4(L::ld(vn + o + m2), L::ld(vn + o + m1), L::ld(vn + o), L::ld(vn + o + p1), in.ul, in.ur);
+    reconstruct4(L::ld(v1 + o + m2), L::ld(v1 + o + m1), L::ld(v1 + o), L::ld(v1 + o + p1), in.vl, in.vr);
+    reconstruct4(L::ld(v2 + o + m2), L::ld(v2 + o + m1), L::ld(v2 + o), L::ld(v2 + o + p1), in.wl, in.wr);
+    reconstruct4(L::ld(p + o + m2), L::ld(p + o + m1), L::ld(p + o), L::ld(p + o + p1), in.pl, in.pr);
     reconstruct4(bc1[0], bc1[1], bc1[2], bc1[3], in.byl, in.byr);
     reconstruct4(bc2[0], bc2[1], bc2[2], bc2[3], in.bzl, in.bzr);
   } else {
-    in.dl = __ldg(rho + o + m1); in.dr = __ldg(rho + o);
-    in.ul = __ldg(vn + o + m1); in.ur = __ldg(vn + o);
-    in.vl = __ldg(v1 + o + m1); in.vr = __ldg(v1 + o);
-    in.wl = __ldg(v2 + o + m1); in.wr = __ldg(v2 + o);
-    in.pl = __ldg(p + o + m1); in.pr = __ldg(p + o);
+    in.dl = L::ld(rho + o + m1); in.dr = L::ld(rho + o);
+    in.ul = L::ld(vn + o + m1); in.ur = L::ld(vn + o);
+    in.vl = L::ld(v1 + o + m1); in.vr = L::ld(v1 + o);
+    in.wl = L::ld(v2 + o + m1); in.wr = L::ld(v2 + o);
+    in.pl = L::ld(p + o + m1); in.pr = L::ld(p + o);
     in.byl = bc1[1]; in.byr = bc1[2];
     in.bzl = bc2[1]; in.bzr = bc2[2];
   }
@@ -109,10 +120,10 @@ __device__ __forceinline__ void face_flux(const GridParams &g, const float *__re
     // face-centred Kepler acceleration, half a stage kick on the normal velocity
     float acc;
     if (ax == 0) {
-      const float vY = 0.5f * (__ldg(w + 2 * N + o + m1) + __ldg(w + 2 * N + o));
+      const float vY = 0.5f * (L::ld(w + 2 * NW + o + m1) + L::ld(w + 2 * NW + o));
       acc = -2.0f * g.omega * vY;
     } else if (ax == 1) {
-      const float vX = 0.5f * (__ldg(w + N + o + m1) + __ldg(w + N + o));
+      const float vX = 0.5f * (L::ld(w + NW + o + m1) + L::ld(w + NW + o));
       acc = 2.0f * g.omega * vX + 2.0f * g.q * (g.omega * g.omega) * (g.corner_y + g.dy * ((float)yidx + 0.5f));
     } else {
       acc = 0.0f;
@@ -122,8 +133,8 @@ __device__ __forceinline__ void face_flux(const GridParams &g, const float *__re
     in.ur += mbv;
   }
   float f[7];
-  hlld_flux(g.gamma, __ldg(bn + o), in, f);
-  float *out = flux + (size_t)(7 * ax) * N + o;
+  hlld_flux(g.gamma, L::ld(bn + o), in, f);
+  float *out = flux + (size_t)(7 * ax) * N + oo;
   out[0] = f[0];
   out[(1 + ax) * N] = f[1];
   out[(1 + e1) * N] = f[2];
@@ -146,7 +157,7 @@ __device__ __forceinline__ void flux_cell(const GridParams &g, const float *__re
     const int p1 = ax == 0 ? f.xp1 : ax == 1 ? f.yp1 : f.zp1;
     const int t1 = ax == 0 ? f.yp1 : ax == 1 ? f.zp1 : f.xp1;
     const int t2 = ax == 0 ? f.zp1 : ax == 1 ? f.xp1 : f.yp1;
-    face_flux(g, w, N, o, ax, m2, m1, p1, t1, t2, y, dt, flux);
+    face_flux(g, w, N, o, ax, m2, m1, p1, t1, t2, y, dt, flux, N, o);
   }
 }
 

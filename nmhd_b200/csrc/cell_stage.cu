@@ -19,7 +19,7 @@
 #include <cstring>
 #include <mutex>
 
-#include "cell_epilogue.cuh"
+#include "cell_flux_staged.cuh"
 
 // Resident CTAs per SM asked of the compiler (register budget) for the two
 // update kernels, both bound by memory latency: measured on the 128x256x64
@@ -43,12 +43,22 @@
 #ifndef NMHD_EPI_MIN_BLOCKS
 #define NMHD_EPI_MIN_BLOCKS 5
 #endif
+// The staged flux kernel holds 44 KB of shared memory per CTA (4 CTAs/SM).
+#ifndef NMHD_SFLUX_MIN_BLOCKS
+#define NMHD_SFLUX_MIN_BLOCKS 4
+#endif
 
 namespace nmhd {
 
 namespace {
 
 using namespace cell;
+
+// Buffer index (0 w0, 1 w1, 2 predictor) that pick() selects.
+__device__ __forceinline__ int pick_index(const StepCtl *c, int sel) {
+  if (sel == 2) return 2;
+  return (sel == 0) == (c->parity == 0) ? 0 : 1;
+}
 
 // Every kernel covers the z planes [z0, z1) (the whole box, or one chunk of
 // the chunked pipeline).
@@ -117,11 +127,6 @@ __global__ void __launch_bounds__(kThreads, NMHD_PRIM_MIN_BLOCKS) k_cell_prim(Gr
 // Constrained transport and conserved update of one stage in one pass
 // (variant 4); ntiles: the CTAs of this launch (the last one to finish the
 // final stage advances the clock).
-// Buffer index (0 w0, 1 w1, 2 predictor) that pick() selects.
-__device__ __forceinline__ int pick_index(const StepCtl *c, int sel) {
-  if (sel == 2) return 2;
-  return (sel == 0) == (c->parity == 0) ? 0 : 1;
-}
 
 template <bool kPow2>
 __global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
@@ -141,6 +146,26 @@ __global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
   if (timed_out && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
     atomicOr(&ctl->status, kStatusTimeout);
   if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, s.red);
+}
+
+// Face fluxes of one stage from a shared copy of the stage input (variant
+// 5, cell_flux_staged.cuh).
+__global__ void __launch_bounds__(kThreads, NMHD_SFLUX_MIN_BLOCKS)
+    k_cell_flux_staged(const __grid_constant__ sfx::FluxMaps maps, GridParams g, StepCtl *ctl, const float *w0,
+                       const float *w1, const float *wp, float *__restrict__ flux, int in_sel, int half) {
+  __shared__ sfx::Smem s;
+  if (ctl->done) return;
+  float dt = step_dt(ctl, nullptr);
+  if (half) dt = dt / 2.0f;
+  const int tid = (threadIdx.z * BY + threadIdx.y) * BX + threadIdx.x;
+  const int x0 = blockIdx.x * BX, y0 = blockIdx.y * BY, z0 = blockIdx.z * BZ;
+  if (!sfx::stage(s, g, &maps, pick_index(ctl, in_sel), pick(ctl, in_sel, w0, w1, wp), x0, y0, z0, tid)) {
+    if (tid == 0) atomicOr(&ctl->status, kStatusTimeout);
+    return;
+  }
+  const int x = x0 + threadIdx.x, y = y0 + threadIdx.y, z = z0 + threadIdx.z;
+  if (x < g.sx && y < g.sy && z < g.sz)
+    sfx::flux_cell_staged(g, s, flux, threadIdx.x, threadIdx.y, threadIdx.z, x, y, z, dt);
 }
 
 dim3 cell_grid(const GridParams &g, int nz) {
@@ -179,6 +204,7 @@ void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1,
 
 struct EpilogueMaps {
   epi::EpiMaps m;
+  sfx::FluxMaps f;  // the staged flux kernel's
 };
 
 // Tensor maps of the fused epilogue's staged boxes for one solver's buffers
@@ -227,15 +253,24 @@ EpilogueMaps *make_epilogue_maps(const GridParams &g, float *w0, float *w1, floa
   make(&out->m.zx, flux, kFluxFields, ZXF::P, ZXF::NJ, ZXF::NK, 1);
   make(&out->m.yz, flux, kFluxFields, YZF::P, YZF::NJ, YZF::NK, 1);
   make(&out->m.zy, flux, kFluxFields, ZYF::P, ZYF::NJ, ZYF::NK, 1);
+  for (int b = 0; b < 3; ++b) make(&out->f.w[b], w[b], 8, sfx::P, sfx::NJ, sfx::NK, 8);
   if (!ok) {
     delete out;
     return nullptr;
   }
   out->m.enabled = 1;
+  out->f.enabled = 1;
   return out;
 }
 
 void free_epilogue_maps(EpilogueMaps *m) { delete m; }
+
+void launch_cell_flux_staged(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                             int in_sel, int half, const EpilogueMaps *maps, cudaStream_t st) {
+  static const EpilogueMaps kNone = {};  // enabled = 0: cp.async staging only
+  k_cell_flux_staged<<<cell_grid(g, g.sz), dim3(BX, BY, BZ), 0, st>>>(maps ? maps->f : kNone.f, g, ctl, w0, w1,
+                                                                      wp, flux, in_sel, half);
+}
 
 void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                               float *dt_hist, int in_sel, int out_sel, int half, int final_stage,

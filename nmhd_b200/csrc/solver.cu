@@ -156,12 +156,14 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
     float *unew = s->flux, *bflux = s->flux + (size_t)5 * g.n;
     nmhd::launch_tile_stage(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, s->dt_hist, in_sel, out_sel,
                             half, final_stage, s->shape, st);
-  } else if (s->variant == 2 || s->variant == 4) {
+  } else if (s->variant == 2 || s->variant == 4 || s->variant == 5) {
     if (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)
       nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
+    else if (s->variant == 5)
+      nmhd::launch_cell_flux_staged(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, st);
     else
       nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
-    if (s->variant == 4)
+    if (s->variant == 4 || s->variant == 5)
       nmhd::launch_cell_update_fused(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel, half,
                                      final_stage, s->epi_maps, st);
     else
@@ -589,8 +591,10 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       if (s->variant == 3) return;
       if (s->variant == 0)
         nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
-      else if ((s->variant == 2 || s->variant == 4) && (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC))
+      else if ((s->variant == 2 || s->variant == 4 || s->variant == 5) && (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC))
         nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
+      else if (s->variant == 5)
+        nmhd::launch_cell_flux_staged(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, q);
       else if (s->variant == 2 || s->variant == 4)
         nmhd::launch_cell_flux(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
       else
@@ -604,7 +608,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       else if (s->variant == 2)
         nmhd::launch_cell_update(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel,
                                  half, fin, q);
-      else if (s->variant == 4)
+      else if (s->variant == 4 || s->variant == 5)
         nmhd::launch_cell_update_fused(g, s->ctl, s->w0, s->w1, s->wp, s->flux, s->dt_hist, in_sel, out_sel,
                                        half, fin, s->epi_maps, q);
       else
@@ -644,15 +648,15 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
     }
     // kernel launches of each class: fill (Y and Z margins), margin CFL, and
     // per stage the flux class (variant 3: the whole chunked stage) and the
-    // update class (variant 2: CT + conserved update, variant 4: the two
-    // fused; the per-stage predictor refill is timed with the first stage's
-    // update)
+    // update class (variant 2: CT + conserved update, variants 4 and 5: the
+    // two fused; the per-stage predictor refill is timed with the first
+    // stage's update)
     const int fills = (g.my > 0) + (g.mz > 0);
     const int nch = s->variant == 3 ? (g.sz + (s->shape.zc < 1 ? g.sz : s->shape.zc) - 1) /
                                           (s->shape.zc < 1 ? g.sz : s->shape.zc)
                                     : 0;
     const int flux_n = s->variant == 3 ? 3 * nch : 1;
-    const int upd_n = s->variant == 3 ? 0 : (s->variant == 2 ? 2 : 1);  // variants 0, 1, 4: one
+    const int upd_n = s->variant == 3 ? 0 : (s->variant == 2 ? 2 : 1);  // variants 0, 1, 4, 5: one
     cnt[0] += fills;
     cnt[1] += margins;
     cnt[2] += midpoint ? flux_n : 0;
@@ -675,9 +679,9 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
 
 nmhd_status nmhd_set_kernel(nmhd_solver *s, int variant, int tile_rows, int z_chunk) {
   if (!s) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "NULL solver");
-  if (variant < 0 || variant > 4) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0, 1, 2, 3 or 4");
-  if ((s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC) && variant != 2 && variant != 4)
-    return fail(s, NMHD_ERR_NOT_SUPPORTED, "fast arithmetic exists for kernel variants 2 and 4 only");
+  if (variant < 0 || variant > 5) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "variant must be 0 to 5");
+  if ((s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC) && variant != 2 && variant != 4 && variant != 5)
+    return fail(s, NMHD_ERR_NOT_SUPPORTED, "fast arithmetic exists for kernel variants 2, 4 and 5 only");
   if (variant == 0 && tile_rows != 4 && tile_rows != 8 && tile_rows != 16)
     return fail(s, NMHD_ERR_INVALID_ARGUMENT, "tile_rows must be 4, 8 or 16");
   if (z_chunk < 0) return fail(s, NMHD_ERR_INVALID_ARGUMENT, "z_chunk must be >= 0");
@@ -737,9 +741,13 @@ int nmhd_autotune(nmhd_solver *s, int steps, double *trials_out, int max_trials)
   const GridParams &g = s->g;
   const TuneKey key = tune_key(s);
   std::vector<TuneChoice> cands;
+  // with fast arithmetic variants 2, 4 and 5 run the fast flux kernel
+  // (5 is then 4) and the others do not exist
+  const bool fast = (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC) != 0;
+  if (!fast) cands.push_back({5, 8, 0});
   cands.push_back({4, 8, 0});
   cands.push_back({2, 8, 0});
-  if (!(s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)) {  // the fast flux kernel exists for variants 2 and 4 only
+  if (!fast) {
     cands.push_back({1, 8, 0});
     for (int zc : {4, 8, 16})
       if (zc < g.sz) cands.push_back({3, 8, zc});

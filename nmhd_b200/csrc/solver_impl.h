@@ -21,9 +21,10 @@ struct nmhd_solver {
   double *diag = nullptr;
   bool cfl_ready = false;  // ctl->cfl_cur holds the CFL time of the current state
   // 0: z-marching tiled kernels, 1: per-cell 1-D, 2: per-cell 3-D blocks,
-  // 3: variant 2 as a z-chunk pipeline, 4 (the default): the variant-2 flux
-  // kernel with the fused stage epilogue
-  int variant = 4;
+  // 3: variant 2 as a z-chunk pipeline, 4: the variant-2 flux kernel with the
+  // fused stage epilogue, 5 (the default): the staged flux kernel with the
+  // fused stage epilogue
+  int variant = 5;
   nmhd::TileShape shape = {8, 16};
   std::map<int, cudaGraphExec_t> graphs;
   // Pinned copies of the control block after each of the (at most two) step
@@ -32,7 +33,8 @@ struct nmhd_solver {
   cudaEvent_t batch_done[2] = {nullptr, nullptr};
   std::string err;
   void *adjoint = nullptr;  // differentiation workspace (adjoint.cu), allocated on first use
-  // tensor maps of the fused epilogue (variant 4) over w0, w1, wp and flux
+  // tensor maps of the fused epilogue and the staged flux kernel (variants
+  // 4 and 5) over w0, w1, wp and flux
   nmhd::EpilogueMaps *epi_maps = nullptr;
 };
 

@@ -121,6 +121,11 @@ void free_epilogue_maps(EpilogueMaps *m);
 void launch_cell_update_fused(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                               float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
                               const EpilogueMaps *maps, cudaStream_t stream);
+// The face fluxes of a stage from a shared-memory copy of each tile's
+// stencil (variant 5), the same fluxes as launch_cell_flux; `maps` as above
+// (interior tiles copy with one tensor copy).
+void launch_cell_flux_staged(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
+                             int in_sel, int half, const EpilogueMaps *maps, cudaStream_t stream);
 // One RK stage with the per-cell kernels as a pipeline over chunks of z_chunk
 // planes (variant 3), so each chunk's face fluxes are consumed from L2.
 void launch_cell_stage_chunked(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,

@@ -116,13 +116,13 @@ SCHEMES = [
 ]
 
 
-@pytest.mark.parametrize("variant", [4, 2])
+@pytest.mark.parametrize("variant", [4, 2, 5])
 @pytest.mark.parametrize("case", range(len(SCHEMES)))
 def test_scheme_variants_match_the_reference_expansions(gpu, case, variant):
     """Piecewise-constant reconstruction and Euler stepping, 60 steps, against
     the reference's own piecewiseconst1 / euler1 code (its template's rules
-    applied to the shipped expansion), for the default and the three-kernel
-    variant."""
+    applied to the shipped expansion), for the default, the three-kernel and
+    the staged-flux variant."""
     name, make, so, to = SCHEMES[case]
     needs_ref(name)
     cfg, s = make()

@@ -116,7 +116,7 @@ def test_gpu_large_box_matches_oracle_and_keeps_div_b(gpu):
 
 
 @pytest.mark.parametrize("case", ["ot_m2", "shear_m2", "shear_m4_mz2"])
-@pytest.mark.parametrize("variant", [2, 0, 4])
+@pytest.mark.parametrize("variant", [2, 0, 4, 5])
 def test_per_stage_margin_fill_matches_oracle(gpu, case, variant):
     """NMHD_FLAG_HALO_PER_STAGE: the predictor's margins refilled before the
     second stage; bitwise the oracle's mode, for the default and the tiled
@@ -262,7 +262,7 @@ def test_goal_time_semantics(gpu):
 
 @pytest.mark.parametrize("variant,rows,zc", [(2, 8, 0), (1, 8, 0), (0, 4, 0), (0, 8, 16), (0, 16, 5),
                                              (0, 8, 3), (3, 8, 1), (3, 8, 2), (3, 8, 3), (3, 8, 4),
-                                             (3, 8, 64), (4, 8, 0)])
+                                             (3, 8, 64), (4, 8, 0), (5, 8, 0)])
 @pytest.mark.parametrize("case", ["ot_ragged", "shear_ragged", "shear_mz"])
 def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
     """Every kernel variant and tile shape, on boxes whose sizes are not
@@ -270,13 +270,14 @@ def test_kernel_variants_and_tile_shapes_bitwise(gpu, variant, rows, zc, case):
     _variant_case(variant, rows, zc, case)
 
 
-@pytest.mark.parametrize("variant", [2, 4])
-@pytest.mark.parametrize("case", ["tiny", "ot_2d", "euler_order1"])
+@pytest.mark.parametrize("variant", [2, 4, 5])
+@pytest.mark.parametrize("case", ["tiny", "ot_2d", "euler_order1", "shear_tma"])
 def test_cell_kernels_on_tiny_flat_and_first_order_boxes(gpu, variant, case):
-    """The per-cell kernels and the fused epilogue (whose shared-memory tile
-    with its halo is larger than these boxes: every halo entry wraps
-    periodically) on a 5 x 9 x 1 box, a single-plane box, and Euler stepping
-    with piecewise-constant reconstruction."""
+    """The per-cell kernels, the fused epilogue and the staged flux kernel
+    (whose shared-memory tiles with their halos are larger than these boxes:
+    every halo entry wraps periodically) on a 5 x 9 x 1 box, a single-plane
+    box, Euler stepping with piecewise-constant reconstruction, and a box
+    with interior tiles (staged by tensor copies) beside edge tiles."""
     _variant_case(variant, 8, 0, case)
 
 
@@ -298,6 +299,9 @@ def _variant_case(variant, rows, zc, case):
     elif case == "ot_2d":
         cfg, s = orszag_tang_3d(40, ny=24, nz=1)
         steps = 10
+    elif case == "shear_tma":  # 96 x 24 x 8: tiles at x0 = 32, 2 <= y0 <= 19, z0 = 2 lie inside
+        cfg, s = shearing_box(n_radial=16, n_azimuthal=96, n_vertical=8, l_azimuthal=6.0, seed=9)
+        steps = 8
     else:  # Euler stepping with piecewise-constant reconstruction
         cfg, s = shearing_box(n_radial=12, n_azimuthal=40, n_vertical=5, l_azimuthal=2.0, seed=10)
         cfg.time_order, cfg.space_order = 1, 1
@@ -334,7 +338,7 @@ def test_autotune_restores_state_and_keeps_results_bitwise(gpu):
         assert again.kernel() == best[:3]
     other, _ = shearing_box(n_radial=16, n_azimuthal=64, n_vertical=12, l_azimuthal=4.0, seed=13)
     with MHDSolver(other) as fresh:
-        assert fresh.kernel()[0] == 4
+        assert fresh.kernel()[0] == 5
 
 
 @pytest.mark.parametrize("zc", [1, 2, 5])
@@ -392,7 +396,7 @@ def test_monitor_hook_runs_before_every_step(gpu):
 
 
 @pytest.mark.parametrize("variant,zc,mz,expect", [(2, 0, 0, 8), (2, 0, 2, 9), (0, 0, 0, 6), (3, 4, 0, 2 + 2 * 3 * 2),
-                                                 (4, 0, 0, 6), (4, 0, 2, 7)])
+                                                 (4, 0, 0, 6), (4, 0, 2, 7), (5, 0, 0, 6)])
 def test_profile_counts_kernel_launches(gpu, variant, zc, mz, expect):
     """nmhd_profile reports each class's kernel launches per step (the bench's
     gpu_launches): fill (Y, Z), margin CFL, flux and update of each stage;
