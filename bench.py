@@ -517,10 +517,10 @@ def ensemble_measure(workload, steps, warmup, dev, rank=0, world=1, dist=None, n
     batch.step(warmup)
     # schedule of each stage kernel (persistent or one tile per CTA), timed on these boxes
     tuning = batch.autotune(reps=3)
-    names = ("flux", "ct", "update", "fused")
+    names = ("flux", "ct", "update", "fused", "staged_flux")
 
     def sched(k, p, s):
-        if k == 3:
+        if k >= 3:
             return ("persistent" if p else "per_tile") if s else "off"
         return ("persistent" if p else "per_tile") + ("_split" if s else "")
 

@@ -290,18 +290,23 @@ int nmhd_batch_launches_per_step(const nmhd_batch *b);
  * kernel = 3 is the fused pass: split = 1 runs constrained transport and the
  * conserved update of the 32 x 4 x 2 boxes as one kernel (the single-box fused
  * epilogue; it takes effect while kernels 1 and 2 are split), persistent its
- * schedule; split = 0 (the default) turns it off. */
+ * schedule; split = 0 (the default) turns it off.  kernel = 4 is the staged
+ * flux pass: split = 1 computes the face fluxes of the 32 x 4 x 2 boxes from a
+ * shared-memory copy of each tile's stencil (the single-box variant-5 flux
+ * kernel; it takes effect while kernel 0 is split), persistent its schedule. */
 nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split);
 /* Schedule autotuner of the batch (the batched counterpart of nmhd_autotune).
  * Times `reps` launches of each stage kernel (face fluxes, constrained
  * transport, conserved update) in every schedule (persistent or not, split or
  * not) on the boxes' current states with CUDA events, keeps the fastest per
- * kernel, then times the stage update (kernels 1 and 2) against the fused
- * pass, one tile per CTA and persistent, and keeps the fastest; states and
- * clocks are left unchanged.  trials_out (may be NULL) receives up to
- * max_trials rows of (kernel, persistent, split, ms per launch), the fused
- * comparison as rows (3, persistent, fused, ms per stage update).  Returns the
- * number of rows written or a negative nmhd_status.
+ * kernel, then times the face fluxes against the staged flux pass and the
+ * stage update (kernels 1 and 2) against the fused pass, each one tile per
+ * CTA and persistent, and keeps the fastest; states and clocks are left
+ * unchanged.  trials_out (may be NULL) receives up to max_trials rows of
+ * (kernel, persistent, split, ms per launch), the two comparisons as rows
+ * (4, persistent, staged, ms per flux launch) and (3, persistent, fused, ms
+ * per stage update).  Returns the number of rows written or a negative
+ * nmhd_status.
  * Every schedule gives bitwise the same result. */
 int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_trials);
 const char *nmhd_batch_last_error(const nmhd_batch *b);

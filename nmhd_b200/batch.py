@@ -142,18 +142,23 @@ class BatchSolver:
         ``split`` the boxes with 32 x 4 x 2 tiles run in a launch of their own.
         ``kernel`` 3 is the fused pass (constrained transport and conserved
         update of the 32 x 4 x 2 boxes in one kernel): ``split`` turns it on
-        (it then needs kernels 1 and 2 split), ``persistent`` its schedule."""
+        (it then needs kernels 1 and 2 split), ``persistent`` its schedule.
+        ``kernel`` 4 is the staged flux pass of the 32 x 4 x 2 boxes (their
+        fluxes from a shared copy of each tile's stencil; needs kernel 0
+        split), turned on and scheduled the same way."""
         self._check(self._L.nmhd_batch_set_schedule(self._h, int(kernel), int(bool(persistent)),
                                                     int(bool(split))))
 
     def autotune(self, reps=5):
         """Pick each stage kernel's schedule (persistent or one tile per CTA,
         split or not) by timing all of them on the current states, then the
-        stage update with and without the fused pass; states and clocks are
-        left unchanged.  Returns rows (kernel, persistent, split, ms per
-        launch); kernel 3 rows are (3, persistent, fused, ms per stage update)."""
-        out = np.zeros((16, 4), dtype=np.float64)
-        k = self._check(self._L.nmhd_batch_autotune(self._h, int(reps), out.ctypes.data, 16))
+        face fluxes with and without the staged flux pass and the stage
+        update with and without the fused pass; states and clocks are left
+        unchanged.  Returns rows (kernel, persistent, split, ms per launch);
+        kernel 4 rows are (4, persistent, staged, ms per flux launch), kernel
+        3 rows (3, persistent, fused, ms per stage update)."""
+        out = np.zeros((20, 4), dtype=np.float64)
+        k = self._check(self._L.nmhd_batch_autotune(self._h, int(reps), out.ctypes.data, 20))
         return [(int(a), bool(b), bool(c), float(d)) for a, b, c, d in out[:k]]
 
     @property

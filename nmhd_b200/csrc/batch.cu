@@ -22,7 +22,7 @@
 #include <vector>
 
 #include "../../include/nmhd.h"
-#include "cell_epilogue.cuh"
+#include "cell_flux_staged.cuh"
 #include "margin_ops.cuh"
 
 namespace nmhd {
@@ -227,6 +227,49 @@ __global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_EPI)
   }
 }
 
+// Face fluxes of the boxes with 32 x 4 x 2 tiles from a shared copy of each
+// tile's stencil: the single-box staged flux kernel (cell_flux_staged.cuh,
+// staging with cp.async), tiles [tb, te) of the group, persistent or one
+// tile per CTA.
+#ifndef NMHD_BATCH_MIN_BLOCKS_SFLUX
+#define NMHD_BATCH_MIN_BLOCKS_SFLUX 4
+#endif
+template <bool kPersist>
+__global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_SFLUX)
+    k_batch_flux_staged(const __grid_constant__ BatchGroup p, int tb, int te, int in_sel, int half) {
+  __shared__ cell::sfx::Smem s;
+  const int tid = threadIdx.x;
+  const int a = tid % BX, b = tid / BX % BY, c = tid / (BX * BY);
+  auto tile = [&](const BoxDesc &d, int t) {
+    const GridParams &g = d.g;
+    StepCtl *ctl = d.ctl;
+    const int lt = t - d.tile_begin;
+    const int x0 = lt % d.tiles_x << 5, y0 = lt / d.tiles_x % d.tiles_y << 2, z0 = lt / (d.tiles_x * d.tiles_y) << 1;
+    float dt = step_dt(ctl, nullptr);
+    if (half) dt = dt / 2.0f;
+    cell::sfx::stage(s, g, nullptr, 0, pick(ctl, in_sel, d.w0, d.w1, d.wp), x0, y0, z0, tid);
+    const int x = x0 + a, y = y0 + b, z = z0 + c;
+    if (x < g.sx && y < g.sy && z < g.sz) cell::sfx::flux_cell_staged(g, s, d.flux, a, b, c, x, y, z, dt);
+  };
+  if (!kPersist) {
+    const int t = tb + blockIdx.x;
+    const BoxDesc &d = p.box[group_box(p, t)];
+    if (d.ctl->done) return;
+    tile(d, t);
+    return;
+  }
+  const int t0 = tb + (int)((long long)(te - tb) * blockIdx.x / gridDim.x);
+  const int t1 = tb + (int)((long long)(te - tb) * (blockIdx.x + 1) / gridDim.x);
+  int bx = group_box(p, t0);
+  for (int t = t0; t < t1; ++t) {
+    while (t >= p.tile_begin[bx + 1]) ++bx;
+    const BoxDesc &d = p.box[bx];
+    if (d.ctl->done) continue;
+    tile(d, t);
+    __syncthreads();  // the next tile overwrites the shared copy
+  }
+}
+
 // Shearing-periodic Y-margin fill of every box (margin_ops.cuh).
 __global__ void __launch_bounds__(256) k_batch_fill(const BoxDesc *__restrict__ boxes, int nb, long long total) {
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < total; i += (long long)gridDim.x * blockDim.x) {
@@ -297,7 +340,10 @@ struct nmhd_batch {
   // with split constrained transport and update: the 32 x 4 x 2 boxes take
   // both in one fused pass (k_batch_epilogue), persistent or one tile per CTA
   bool fuse = false, persist_fused = false;
-  int ctas[4] = {0, 0, 0, 0};               // resident CTAs of each persistent stage kernel ([3]: fused)
+  // with split face fluxes: the 32 x 4 x 2 boxes' fluxes from a shared copy
+  // of each tile's stencil (k_batch_flux_staged), persistent or per tile
+  bool sflux = false, persist_sflux = false;
+  int ctas[5] = {0, 0, 0, 0, 0};  // resident CTAs of each persistent stage kernel ([3]: fused, [4]: staged flux)
   int device = 0;
   cudaStream_t stream = nullptr;
   bool own_stream = true;
@@ -373,6 +419,7 @@ void launch_stage(const nmhd::BatchGroup &p, bool persist, bool split, int ctas,
 }
 
 bool fused(const nmhd_batch *b) { return b->fuse && b->split[1] && b->split[2]; }
+bool staged(const nmhd_batch *b) { return b->sflux && b->split[0]; }
 
 // Kernel `kind` of one stage over every group.  Fused: kind 1 covers the
 // boxes with general tiles only, kind 2 the fused pass of the 32 x 4 x 2
@@ -380,7 +427,22 @@ bool fused(const nmhd_batch *b) { return b->fuse && b->split[1] && b->split[2]; 
 void launch_kind(nmhd_batch *b, int kind, int in_sel, int out_sel, int half, int fin) {
   const dim3 blk(nmhd::cell::kThreads);
   for (const BatchGroup &p : b->groups) {
-    if (kind == 0) {
+    if (kind == 0 && staged(b)) {
+      const int tb = p.fixed_tiles, te = p.total_tiles;
+      if (tb > 0) {
+        if (b->persist_sflux)
+          nmhd::k_batch_flux_staged<true><<<std::min(b->ctas[4], tb), blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
+        else
+          nmhd::k_batch_flux_staged<false><<<tb, blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
+      }
+      if (te > tb) {
+        if (b->persist[0])
+          nmhd::k_batch_stage<0, true, false><<<std::min(b->ctas[0], te - tb), blk, 0, b->stream>>>(
+              p, tb, te, in_sel, out_sel, half, fin);
+        else
+          nmhd::k_batch_stage<0, false, false><<<te - tb, blk, 0, b->stream>>>(p, tb, te, in_sel, out_sel, half, fin);
+      }
+    } else if (kind == 0) {
       launch_stage<0>(p, b->persist[0], b->split[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
     } else if (fused(b)) {
       const int tb = p.fixed_tiles, te = p.total_tiles;
@@ -549,12 +611,13 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
   // persistent schedule: as many CTAs as fit on the GPU at once
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
-  int occ[4] = {1, 1, 1, 1};
+  int occ[5] = {1, 1, 1, 1, 1};
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], nmhd::k_batch_stage<0, true, false>, nmhd::cell::kThreads, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], nmhd::k_batch_stage<1, true, false>, nmhd::cell::kThreads, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], nmhd::k_batch_stage<2, true, false>, nmhd::cell::kThreads, 0);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], nmhd::k_batch_epilogue<true>, nmhd::cell::kThreads, 0);
-  for (int k = 0; k < 4; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], nmhd::k_batch_flux_staged<true>, nmhd::cell::kThreads, 0);
+  for (int k = 0; k < 5; ++k) b->ctas[k] = sms * std::max(1, occ[k]);
   // launch groups: consecutive boxes, tiles numbered from 0 within a group,
   // the boxes with 32 x 4 x 2 tiles first
   for (int i0 = 0; i0 < n; i0 += nmhd::kGroupBoxes) {
@@ -825,12 +888,15 @@ nmhd_status nmhd_batch_tile_shape(const nmhd_batch *b, int box, int *tile_x, int
 }
 
 nmhd_status nmhd_batch_set_schedule(nmhd_batch *b, int kernel, int persistent, int split) {
-  if (!b || kernel < 0 || kernel > 3 || (persistent != 0 && persistent != 1) || (split != 0 && split != 1))
-    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..3, persistent and split 0 or 1");
+  if (!b || kernel < 0 || kernel > 4 || (persistent != 0 && persistent != 1) || (split != 0 && split != 1))
+    return bfail(b, NMHD_ERR_INVALID_ARGUMENT, "kernel must be 0..4, persistent and split 0 or 1");
   BATCH_CUDA(b, cudaStreamSynchronize(b->stream));
   if (kernel == 3) {  // the fused pass: on (split = 1) or off, and its schedule
     b->fuse = split != 0;
     b->persist_fused = persistent != 0;
+  } else if (kernel == 4) {  // the staged flux pass: on (split = 1) or off, and its schedule
+    b->sflux = split != 0;
+    b->persist_sflux = persistent != 0;
   } else {
     b->persist[kernel] = persistent != 0;
     b->split[kernel] = split != 0;
@@ -870,7 +936,9 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
   const bool saved[3] = {b->persist[0], b->persist[1], b->persist[2]};
   const bool saved_split[3] = {b->split[0], b->split[1], b->split[2]};
   const bool saved_fuse = b->fuse, saved_pf = b->persist_fused;
-  b->fuse = false;  // each kernel alone first; the fused pass is compared last
+  const bool saved_sflux = b->sflux, saved_ps = b->persist_sflux;
+  b->fuse = false;  // each kernel alone first; the fused passes are compared last
+  b->sflux = false;
   cudaEvent_t e0 = nullptr, e1 = nullptr;
   cudaError_t e = cudaEventCreate(&e0);
   if (e == cudaSuccess) e = cudaEventCreate(&e1);
@@ -907,6 +975,47 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
     }
     b->persist[kind] = choice;
     b->split[kind] = choice_split;
+  }
+  // The face fluxes with the chosen schedule against the staged flux pass for
+  // the 32 x 4 x 2 boxes (fluxes split), one tile per CTA or persistent:
+  // rows (4, persistent, staged, ms per launch).
+  {
+    const bool keep_split = b->split[0];
+    double best = 1e30;
+    bool best_on = false, best_p = false, any_fixed = false;
+    for (const BatchGroup &p : b->groups) any_fixed = any_fixed || p.fixed_tiles > 0;
+    for (int trial = 0; trial < 3 && e == cudaSuccess; ++trial) {
+      const int on = trial > 0, ps = trial == 2;
+      if (on && !any_fixed) break;
+      b->sflux = on != 0;
+      b->persist_sflux = ps != 0;
+      if (on) b->split[0] = true;
+      launch_kind(b, 0, 0, 2, 1, 0);  // warm-up
+      e = cudaEventRecord(e0, b->stream);
+      for (int r = 0; r < reps && e == cudaSuccess; ++r) launch_kind(b, 0, 0, 2, 1, 0);
+      if (e == cudaSuccess) e = cudaEventRecord(e1, b->stream);
+      if (e == cudaSuccess) e = cudaEventSynchronize(e1);
+      float ms = 0.f;
+      if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, e0, e1);
+      if (e != cudaSuccess) break;
+      const double per = ms / reps;
+      if (trials_out && written < max_trials) {
+        trials_out[4 * written + 0] = 4;
+        trials_out[4 * written + 1] = ps;
+        trials_out[4 * written + 2] = on;
+        trials_out[4 * written + 3] = per;
+        ++written;
+      }
+      if (per < best) {
+        best = per;
+        best_on = on != 0;
+        best_p = ps != 0;
+      }
+      if (on) b->split[0] = keep_split;
+    }
+    b->sflux = best_on;
+    b->persist_sflux = best_p;
+    if (best_on) b->split[0] = true;
   }
   // The stage's update (constrained transport, then conserved update) with
   // the chosen schedules, against the fused pass for the 32 x 4 x 2 boxes
@@ -961,6 +1070,8 @@ int nmhd_batch_autotune(nmhd_batch *b, int reps, double *trials_out, int max_tri
     for (int k = 0; k < 3; ++k) b->persist[k] = saved[k], b->split[k] = saved_split[k];
     b->fuse = saved_fuse;
     b->persist_fused = saved_pf;
+    b->sflux = saved_sflux;
+    b->persist_sflux = saved_ps;
     return bfail(b, NMHD_ERR_CUDA, std::string("nmhd_batch_autotune: ") + cudaGetErrorString(e));
   }
   // the graphs hold the previous schedules

@@ -41,7 +41,7 @@ def test_batch_rejects_unsupported_configs_on_cpu():
 
 @pytest.mark.gpu
 @pytest.mark.parametrize("schedule", ["per_tile", "persistent", "mixed", "unsplit", "unsplit_persistent",
-                                      "fused", "fused_persistent"])
+                                      "fused", "fused_persistent", "staged", "staged_persistent"])
 def test_batch_boxes_equal_single_box_runs(gpu, schedule):
     """Every box of a batch equals its single-box run, in each schedule of the
     stage kernels (persistent tile ranges or one tile per CTA, and the fused
@@ -49,7 +49,8 @@ def test_batch_boxes_equal_single_box_runs(gpu, schedule):
     from nmhd_b200.batch import BatchSolver
     from nmhd_b200.solver import MHDSolver
     persist = {"per_tile": (0, 0, 0), "persistent": (1, 1, 1), "mixed": (1, 0, 1), "unsplit": (0, 0, 0),
-               "unsplit_persistent": (1, 1, 1), "fused": (0, 0, 0), "fused_persistent": (1, 1, 1)}[schedule]
+               "unsplit_persistent": (1, 1, 1), "fused": (0, 0, 0), "fused_persistent": (1, 1, 1),
+               "staged": (0, 0, 0), "staged_persistent": (1, 1, 1)}[schedule]
     split = not schedule.startswith("unsplit")
     boxes, _ = small_ensemble()
     # add two non-shearing boxes of other shapes (power-of-two and not)
@@ -71,6 +72,8 @@ def test_batch_boxes_equal_single_box_runs(gpu, schedule):
             launches = batch.launches_per_step()
             batch.set_schedule(3, schedule == "fused_persistent", True)
             assert batch.launches_per_step() != launches
+        if schedule.startswith("staged"):
+            batch.set_schedule(4, schedule == "staged_persistent", True)
         for i, (c, s) in enumerate(boxes):
             batch.set_state(i, s)
         batch.step(4)
@@ -151,8 +154,9 @@ def test_batch_autotune_keeps_states_clocks_and_results(gpu):
         # the fused pass against the update kernels: off, and where boxes have
         # 32 x 4 x 2 tiles, per tile and persistent
         fixed = any(batch.tile_shape(i) == (32, 4, 2) for i in range(len(boxes)))
-        assert sorted((p, s) for k, p, s, _ in trials if k == 3) == (
-            [(False, False), (False, True), (True, True)] if fixed else [(False, False)])
+        for kk in (3, 4):  # fused update, staged fluxes
+            assert sorted((p, s) for k, p, s, _ in trials if k == kk) == (
+                [(False, False), (False, True), (True, True)] if fixed else [(False, False)])
         assert all(ms > 0 for _, _, _, ms in trials)
         for i, (clk, st) in enumerate(before):
             assert batch.clock(i) == clk and np.array_equal(batch.get_state(i), st)
