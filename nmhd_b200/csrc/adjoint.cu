@@ -175,9 +175,14 @@ struct Workspace {
   // sweep: control blocks are staged in pinned memory (one per segment, so
   // none is overwritten before its copy runs) and two tape slots alternate,
   // ordered by "slot recomputed" / "slot swept" events.
-  cudaStream_t stream2 = nullptr;
+  // The reverse sweep itself runs on stream_hi, at the device's highest
+  // stream priority, the recomputation on stream2 at the lowest: the sweep's
+  // thread blocks are scheduled first and the recomputation fills the SMs
+  // they leave free.
+  cudaStream_t stream2 = nullptr, stream_hi = nullptr;
   StepCtl *hstage = nullptr;  // pinned, NMHD_ADJOINT_MAX_STEPS entries
-  cudaEvent_t slot_ready[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr}, fwd_done = nullptr;
+  cudaEvent_t slot_ready[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr}, fwd_done = nullptr,
+              sweep_done = nullptr;
 };
 
 Workspace &workspace(nmhd_solver *s) {
@@ -218,13 +223,17 @@ nmhd_status reserve(nmhd_solver *s, Workspace &w, size_t bytes) {
     AD_CUDA(cudaMalloc(&w.dt_dev, sizeof(float) * nmhd::kDtHistCap));
     AD_CUDA(cudaMalloc(&w.hist_dummy, sizeof(float) * nmhd::kDtHistCap));
     for (auto &e : w.ev) AD_CUDA(cudaEventCreate(&e));
-    AD_CUDA(cudaStreamCreateWithFlags(&w.stream2, cudaStreamNonBlocking));
+    int prio_low = 0, prio_high = 0;
+    AD_CUDA(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    AD_CUDA(cudaStreamCreateWithPriority(&w.stream2, cudaStreamNonBlocking, prio_low));
+    AD_CUDA(cudaStreamCreateWithPriority(&w.stream_hi, cudaStreamNonBlocking, prio_high));
     AD_CUDA(cudaMallocHost(&w.hstage, sizeof(StepCtl) * NMHD_ADJOINT_MAX_STEPS));
     for (int i = 0; i < 2; ++i) {
       AD_CUDA(cudaEventCreateWithFlags(&w.slot_ready[i], cudaEventDisableTiming));
       AD_CUDA(cudaEventCreateWithFlags(&w.slot_free[i], cudaEventDisableTiming));
     }
     AD_CUDA(cudaEventCreateWithFlags(&w.fwd_done, cudaEventDisableTiming));
+    AD_CUDA(cudaEventCreateWithFlags(&w.sweep_done, cudaEventDisableTiming));
   }
   if (w.bytes >= bytes) return NMHD_OK;
   if (w.mem) {
@@ -486,7 +495,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
 
   // ---- reverse sweep ---------------------------------------------------------------
   // Segments [0, nrec) are recomputed from their checkpoints on a second
-  // stream while the reverse sweep runs on the solver's: recomputed segment
+  // stream while the reverse sweep runs on a third (high priority): recomputed segment
   // j (from the last, nrec-1, down) lands in slot X for even j and in tape
   // slot 0 for odd j, so the recomputation of a segment overlaps the adjoint
   // of the one after it.  Slot 0 first holds the earliest kept segment; a
@@ -526,22 +535,26 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
     AD_CUDA(cudaEventRecord(w.slot_ready[si], q2));
     return NMHD_OK;
   };
+  cudaStream_t qs = w.stream_hi;
+  GpuExec exs{qs};
   auto sweep = [&](int seg, R *segtape) -> nmhd_status {
     const int n0 = seg * K, n1 = std::min(n0 + K, nsteps);
     for (int i = n1 - 1; i >= n0; --i) {
       const StepTape<R> t = tape_at(segtape + (size_t)(i - n0) * kTapeFields * n, n, fscr);
-      if (in_window(L, i + 1)) ex.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
-      adj_step(ex, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
+      if (in_window(L, i + 1)) exs.cells(gg, OpAStress<R>{gg, t.wo, lamA, scale});
+      adj_step(exs, gg, s->cfg.time_order, tn[i], (R)dts[i], t, lamA, lamS, lamF, sc);
       std::swap(lamA, lamF);
     }
     return NMHD_OK;
   };
   AD_CUDA(cudaEventRecord(w.ev[2], q));
-  // the recomputation reads the checkpoints and frozen time steps written on q
+  // the recomputation and the sweep read the checkpoints, frozen time steps
+  // and adjoint state written on q
   AD_CUDA(cudaEventRecord(w.fwd_done, q));
   AD_CUDA(cudaStreamWaitEvent(q2, w.fwd_done, 0));
+  AD_CUDA(cudaStreamWaitEvent(qs, w.fwd_done, 0));
   // neither slot holds a segment still to be swept yet
-  for (int i = 0; i < 2; ++i) AD_CUDA(cudaEventRecord(w.slot_free[i], q));
+  for (int i = 0; i < 2; ++i) AD_CUDA(cudaEventRecord(w.slot_free[i], qs));
   if (nrec > 0) {
     st = recompute(nrec - 1);
     if (st != NMHD_OK) return st;
@@ -551,7 +564,7 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
     if (n0 >= kept0) {  // taped by the forward run
       st = sweep(seg, tape + (size_t)(n0 - kept0) * kTapeFields * n);
       if (st != NMHD_OK) return st;
-      if (n0 == kept0) AD_CUDA(cudaEventRecord(w.slot_free[1], q));  // tape slot 0 swept
+      if (n0 == kept0) AD_CUDA(cudaEventRecord(w.slot_free[1], qs));  // tape slot 0 swept
       continue;
     }
     const int si = (nrec - 1 - seg) % 2;
@@ -559,12 +572,14 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
       st = recompute(seg - 1);
       if (st != NMHD_OK) return st;
     }
-    AD_CUDA(cudaStreamWaitEvent(q, w.slot_ready[si], 0));
+    AD_CUDA(cudaStreamWaitEvent(qs, w.slot_ready[si], 0));
     st = sweep(seg, slots[si]);
     if (st != NMHD_OK) return st;
-    AD_CUDA(cudaEventRecord(w.slot_free[si], q));
+    AD_CUDA(cudaEventRecord(w.slot_free[si], qs));
   }
   AD_CUDA(cudaGetLastError());
+  AD_CUDA(cudaEventRecord(w.sweep_done, qs));
+  AD_CUDA(cudaStreamWaitEvent(q, w.sweep_done, 0));
   AD_CUDA(cudaEventRecord(w.ev[3], q));
   AD_CUDA(cudaEventSynchronize(w.ev[3]));
   double ms_re = 0.0;
@@ -597,6 +612,11 @@ void nmhd_adjoint_release(nmhd_solver *s) {
     cudaStreamSynchronize(w->stream2);
     cudaStreamDestroy(w->stream2);
   }
+  if (w->stream_hi) {
+    cudaStreamSynchronize(w->stream_hi);
+    cudaStreamDestroy(w->stream_hi);
+  }
+  if (w->sweep_done) cudaEventDestroy(w->sweep_done);
   if (w->hstage) cudaFreeHost(w->hstage);
   for (int i = 0; i < 2; ++i) {
     if (w->slot_ready[i]) cudaEventDestroy(w->slot_ready[i]);
