@@ -135,4 +135,12 @@ __device__ __forceinline__ void flux_cell_staged(const GridParams &g, const Smem
 
 }  // namespace sfx
 }  // namespace cell
+
+// The tensor maps of one solver's buffers (make_epilogue_maps): the fused
+// epilogue's and the staged flux kernels'.
+struct EpilogueMaps {
+  cell::epi::EpiMaps m;
+  cell::sfx::FluxMaps f;
+};
+
 }  // namespace nmhd

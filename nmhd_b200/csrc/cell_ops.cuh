@@ -486,5 +486,11 @@ __device__ __forceinline__ const float *pick(const StepCtl *c, int sel, const fl
   return (sel == 0) == (c->parity == 0) ? w0 : w1;
 }
 
+// Buffer index (0 w0, 1 w1, 2 predictor) that pick() selects.
+__device__ __forceinline__ int pick_index(const StepCtl *c, int sel) {
+  if (sel == 2) return 2;
+  return (sel == 0) == (c->parity == 0) ? 0 : 1;
+}
+
 }  // namespace cell
 }  // namespace nmhd

@@ -54,11 +54,6 @@ namespace {
 
 using namespace cell;
 
-// Buffer index (0 w0, 1 w1, 2 predictor) that pick() selects.
-__device__ __forceinline__ int pick_index(const StepCtl *c, int sel) {
-  if (sel == 2) return 2;
-  return (sel == 0) == (c->parity == 0) ? 0 : 1;
-}
 
 // Every kernel covers the z planes [z0, z1) (the whole box, or one chunk of
 // the chunked pipeline).
@@ -201,11 +196,6 @@ void launch_cell_update(const GridParams &g, StepCtl *ctl, float *w0, float *w1,
     update_range<false>(g, ctl, w0, w1, wp, flux, dt_hist, in_sel, out_sel, half, final_stage, 0, g.sz, ntiles,
                         true, true, st);
 }
-
-struct EpilogueMaps {
-  epi::EpiMaps m;
-  sfx::FluxMaps f;  // the staged flux kernel's
-};
 
 // Tensor maps of the fused epilogue's staged boxes for one solver's buffers
 // (cuTensorMapEncodeTiled through the runtime's driver entry point): 4-D

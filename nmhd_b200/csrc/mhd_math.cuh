@@ -56,8 +56,6 @@ __host__ __device__ __forceinline__ void hlld_flux(const float gamma, const floa
   const float pres_L = s.pl, pres_R = s.pr, By_L = s.byl, By_R = s.byr;
   const float Bz_L = s.bzl, Bz_R = s.bzr;
 
-  float signBx = 0.0f;
-  if (fabsf(Bx) > 0.0f) signBx = Bx / fabsf(Bx);
 
   const float momx_L = dens_L * velx_L, momy_L = dens_L * vely_L, momz_L = dens_L * velz_L;
   const float momx_R = dens_R * velx_R, momy_R = dens_R * vely_R, momz_R = dens_R * velz_R;
@@ -198,6 +196,11 @@ __host__ __device__ __forceinline__ void hlld_flux(const float gamma, const floa
   const float velz_L_s = left ? ws_ : wso, velz_R_s = left ? wso : ws_;
   const float By_L_s = left ? bys_ : byso, By_R_s = left ? byso : bys_;
   const float Bz_L_s = left ? bzs_ : bzso, Bz_R_s = left ? bzso : bzs_;
+  // sign(Bx) as the reference computes it, Bx / |Bx| for |Bx| > 0, else 0:
+  // the quotient is exactly +-1 for finite Bx and NaN for infinite Bx, so it
+  // is written without the division
+  float signBx = 0.0f;
+  if (fabsf(Bx) > 0.0f) signBx = isinf(Bx) ? __builtin_nanf("") : copysignf(1.0f, Bx);
   // double-star states (hlld.inl:172-193)
   const float fr = 1.0f / (sdL + sdR);
   const float vely_ss = fr * (sdL * vely_L_s + sdR * vely_R_s + (By_R_s - By_L_s) * signBx);

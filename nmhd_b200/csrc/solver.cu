@@ -158,7 +158,7 @@ void enqueue_stage(nmhd_solver *s, int in_sel, int out_sel, int half, int final_
                             half, final_stage, s->shape, st);
   } else if (s->variant == 2 || s->variant == 4 || s->variant == 5) {
     if (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC)
-      nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, st);
+      nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, st);
     else if (s->variant == 5)
       nmhd::launch_cell_flux_staged(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, st);
     else
@@ -592,7 +592,7 @@ int nmhd_profile(nmhd_solver *s, int steps, double *ms_out, double *launches_out
       if (s->variant == 0)
         nmhd::launch_tile_flux(g, s->ctl, s->w0, s->w1, s->wp, unew, bflux, in_sel, half, s->shape, q);
       else if ((s->variant == 2 || s->variant == 4 || s->variant == 5) && (s->cfg.flags & NMHD_FLAG_FAST_ARITHMETIC))
-        nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, q);
+        nmhd::launch_cell_flux_fast(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, q);
       else if (s->variant == 5)
         nmhd::launch_cell_flux_staged(g, s->ctl, s->w0, s->w1, s->wp, s->flux, in_sel, half, s->epi_maps, q);
       else if (s->variant == 2 || s->variant == 4)

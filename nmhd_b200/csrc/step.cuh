@@ -102,9 +102,11 @@ struct TileShape {
 void launch_tile_stage(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *unew,
                        float *bflux, float *dt_hist, int in_sel, int out_sel, int half, int final_stage,
                        const TileShape &shape, cudaStream_t stream);
-// The flux kernel with fast arithmetic (NMHD_FLAG_FAST_ARITHMETIC, cell_fast.cu).
+// The staged flux kernel with fast arithmetic (NMHD_FLAG_FAST_ARITHMETIC,
+// cell_fast.cu); `maps` as for launch_cell_flux_staged.
+struct EpilogueMaps;
 void launch_cell_flux_fast(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
-                           int in_sel, int half, cudaStream_t stream);
+                           int in_sel, int half, const EpilogueMaps *maps, cudaStream_t stream);
 // Per-cell stage kernels with 32x4x2 CTAs (flux: 21 fields of scratch).
 void launch_cell_flux(const GridParams &g, StepCtl *ctl, float *w0, float *w1, float *wp, float *flux,
                       int in_sel, int half, cudaStream_t stream);
