@@ -31,6 +31,9 @@ struct __align__(8) BoxDesc {
   GridParams g;
   float *w0, *w1, *wp, *flux, *dt_hist;
   StepCtl *ctl;
+  // tensor maps of this box's buffers in device memory (boxes with 32 x 4 x 2
+  // tiles and Sx % 4 == 0), or NULL: the staged passes then copy by cp.async
+  const EpilogueMaps *maps;
   int tile_begin;                 // first tile of this box in the flattened list
   int tiles_x, tiles_y, tiles_z;  // tiles per axis
   int lx, ly, lz;                 // tile of 2^lx x 2^ly x 2^lz cells (256 threads)
@@ -200,12 +203,15 @@ __global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_EPI)
     const float *win = pick(ctl, in_sel, d.w0, d.w1, d.wp), *wb = pick(ctl, 0, d.w0, d.w1, d.wp);
     float *wo = const_cast<float *>(pick(ctl, out_sel, d.w0, d.w1, d.wp));
     int bad = 0, timed_out = 0;
+    const cell::epi::EpiMaps *maps = d.maps ? &d.maps->m : nullptr;
+    const int ib = pick_index(ctl, in_sel), bb = pick_index(ctl, 0);
     const float tcfl =
         d.g.pow2_spacing
-            ? cell::epi::tile_epilogue<true>(s, d.g, nullptr, 0, 0, win, wb, wo, d.flux, x0, y0, z0, dt,
+            ? cell::epi::tile_epilogue<true>(s, d.g, maps, ib, bb, win, wb, wo, d.flux, x0, y0, z0, dt,
                                             final_stage != 0, &bad, &timed_out)
-            : cell::epi::tile_epilogue<false>(s, d.g, nullptr, 0, 0, win, wb, wo, d.flux, x0, y0, z0, dt,
+            : cell::epi::tile_epilogue<false>(s, d.g, maps, ib, bb, win, wb, wo, d.flux, x0, y0, z0, dt,
                                              final_stage != 0, &bad, &timed_out);
+    if (timed_out && threadIdx.x == 0) atomicOr(&ctl->status, kStatusTimeout);
     if (final_stage) finish_tile(ctl, (unsigned)(d.tiles_x * d.tiles_y * d.tiles_z), tcfl, bad, d.dt_hist, s.red);
   };
   if (!kPersist) {
@@ -247,7 +253,11 @@ __global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_SFLUX)
     const int x0 = lt % d.tiles_x << 5, y0 = lt / d.tiles_x % d.tiles_y << 2, z0 = lt / (d.tiles_x * d.tiles_y) << 1;
     float dt = step_dt(ctl, nullptr);
     if (half) dt = dt / 2.0f;
-    cell::sfx::stage(s, g, nullptr, 0, pick(ctl, in_sel, d.w0, d.w1, d.wp), x0, y0, z0, tid);
+    if (!cell::sfx::stage(s, g, d.maps ? &d.maps->f : nullptr, pick_index(ctl, in_sel),
+                          pick(ctl, in_sel, d.w0, d.w1, d.wp), x0, y0, z0, tid)) {
+      if (tid == 0) atomicOr(&ctl->status, kStatusTimeout);
+      return;
+    }
     const int x = x0 + a, y = y0 + b, z = z0 + c;
     if (x < g.sx && y < g.sy && z < g.sz) cell::sfx::flux_cell_staged(g, s, d.flux, a, b, c, x, y, z, dt);
   };
@@ -329,6 +339,7 @@ struct nmhd_batch {
   std::vector<nmhd_config> cfg;
   std::vector<BoxDesc> boxes;
   BoxDesc *d_boxes = nullptr;
+  nmhd::EpilogueMaps *d_maps = nullptr;  // per box (used by the boxes whose BoxDesc points here)
   float *pool = nullptr;  // per box: w0, w1, wp (8 fields each), flux (21 fields)
   float *hist = nullptr;
   StepCtl *ctls = nullptr;
@@ -608,6 +619,34 @@ nmhd_status nmhd_batch_create(const nmhd_config *cfgs, int n, nmhd_batch **out) 
     h[i].goal = INFINITY;
     h[i].hist_cap = nmhd::kDtHistCap;
   }
+  // tensor maps of the 32 x 4 x 2 boxes' buffers, in device memory: their
+  // interior tiles stage by tensor copies as in the single-box kernels
+  {
+    std::vector<nmhd::EpilogueMaps> hm(n);
+    std::memset(hm.data(), 0, sizeof(nmhd::EpilogueMaps) * n);
+    std::vector<char> has(n, 0);
+    for (int i = 0; i < n; ++i) {
+      BoxDesc &d = b->boxes[i];
+      d.maps = nullptr;
+      if (!(d.lx == 5 && d.ly == 2 && d.lz == 1)) continue;
+      nmhd::EpilogueMaps *m = nmhd::make_epilogue_maps(d.g, d.w0, d.w1, d.wp, d.flux);
+      if (m) {
+        hm[i] = *m;
+        has[i] = 1;
+        nmhd::free_epilogue_maps(m);
+      }
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&b->d_maps, sizeof(nmhd::EpilogueMaps) * n);
+    if (e == cudaSuccess)
+      e = cudaMemcpy(b->d_maps, hm.data(), sizeof(nmhd::EpilogueMaps) * n, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess)
+      for (int i = 0; i < n; ++i)
+        if (has[i]) b->boxes[i].maps = b->d_maps + i;
+    if (e != cudaSuccess) {
+      nmhd_batch_destroy(b);
+      return bfail(nullptr, NMHD_ERR_CUDA, std::string("nmhd_batch_create: ") + cudaGetErrorString(e));
+    }
+  }
   // persistent schedule: as many CTAs as fit on the GPU at once
   int sms = 148;
   cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
@@ -660,6 +699,7 @@ void nmhd_batch_destroy(nmhd_batch *b) {
   cudaFree(b->hist);
   cudaFree(b->ctls);
   cudaFree(b->d_boxes);
+  cudaFree(b->d_maps);
   if (b->hctl) cudaFreeHost(b->hctl);
   for (cudaEvent_t ev : b->batch_done)
     if (ev) cudaEventDestroy(ev);
