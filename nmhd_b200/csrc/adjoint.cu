@@ -18,9 +18,11 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <string>
 #include <vector>
 
@@ -183,6 +185,14 @@ struct Workspace {
   StepCtl *hstage = nullptr;  // pinned, NMHD_ADJOINT_MAX_STEPS entries
   cudaEvent_t slot_ready[2] = {nullptr, nullptr}, slot_free[2] = {nullptr, nullptr}, fwd_done = nullptr,
               sweep_done = nullptr;
+  // Tensor maps of the production kernels for each (w0, w1, predictor, flux)
+  // buffer set a taped step runs on, made on first use: the sets are fixed
+  // while the arena stays, so repeated runs reuse them.
+  std::map<std::array<const void *, 4>, nmhd::EpilogueMaps *> maps;
+  void clear_maps() {
+    for (auto &kv : maps) nmhd::free_epilogue_maps(kv.second);
+    maps.clear();
+  }
 };
 
 Workspace &workspace(nmhd_solver *s) {
@@ -241,6 +251,7 @@ nmhd_status reserve(nmhd_solver *s, Workspace &w, size_t bytes) {
     cudaFree(w.mem);
     w.mem = nullptr;
     w.bytes = 0;
+    w.clear_maps();  // they name the old arena's buffers
   }
   AD_CUDA(cudaMalloc(&w.mem, bytes));
   w.bytes = bytes;
@@ -315,6 +326,17 @@ nmhd_status write_ctl_async(nmhd_solver *s, Workspace &w, double time, long long
 // kernels take the current state as buffer `parity` of (w0, w1) and the final
 // stage flips the device parity; the pair is passed in the order that makes
 // t.wf the current buffer, so the parity needs no reset between steps.
+// Tensor maps for the buffer set (b0, b1, ws, flux), made on first use (NULL
+// where they cannot be made: the kernels then stage by cp.async).
+const nmhd::EpilogueMaps *maps_for(nmhd_solver *s, Workspace &w, float *b0, float *b1, float *ws, float *flux) {
+  const std::array<const void *, 4> key = {b0, b1, ws, flux};
+  auto it = w.maps.find(key);
+  if (it != w.maps.end()) return it->second;
+  nmhd::EpilogueMaps *m = nmhd::make_epilogue_maps(s->g, b0, b1, ws, flux);
+  w.maps[key] = m;
+  return m;
+}
+
 void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl, cudaStream_t st) {
   const GridParams &g = s->g;
   float *hist = cfl ? w.dt_dev : w.hist_dummy;
@@ -323,16 +345,18 @@ void prod_step(nmhd_solver *s, Workspace &w, const StepTape<float> &t, bool cfl,
     nmhd::launch_fill(g, w.ctl, b0, b1, st);
     if (cfl) nmhd::launch_cfl_margin(g, w.ctl, b0, b1, st);
   }
-  // the default kernels (variant 5), staging by cp.async: the tape's
-  // buffers change from step to step, so no tensor maps
+  // the default kernels (variant 5), with the tensor maps of this step's
+  // buffers (the tape's buffers change from step to step)
+  const nmhd::EpilogueMaps *m1 = maps_for(s, w, b0, b1, t.ws, t.f1);
   if (s->cfg.time_order == 1) {
-    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, nullptr, st);
-    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, nullptr, st);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 0, m1, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 1, 0, 1, m1, st);
   } else {
-    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, nullptr, st);
-    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, nullptr, st);
-    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, nullptr, st);
-    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, nullptr, st);
+    const nmhd::EpilogueMaps *m2 = t.f2 == t.f1 ? m1 : maps_for(s, w, b0, b1, t.ws, t.f2);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f1, 0, 1, m1, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f1, hist, 0, 2, 1, 0, m1, st);
+    nmhd::launch_cell_flux_staged(g, w.ctl, b0, b1, t.ws, t.f2, 2, 0, m2, st);
+    nmhd::launch_cell_update_fused(g, w.ctl, b0, b1, t.ws, t.f2, hist, 2, 1, 0, 1, m2, st);
   }
   w.parity ^= 1;
 }
@@ -602,6 +626,8 @@ nmhd_status run(nmhd_solver *s, int nsteps, int K, const nmhd_loss_spec &L, cons
 void nmhd_adjoint_release(nmhd_solver *s) {
   if (!s || !s->adjoint) return;
   Workspace *w = static_cast<Workspace *>(s->adjoint);
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  w->clear_maps();
   cudaFree(w->mem);
   cudaFree(w->ctl);
   cudaFree(w->dt_dev);
