@@ -1,17 +1,21 @@
-// Per-cell stage kernels (variant 2, the default) of the B200 ideal-MHD time
-// step, sm_100a: one thread per cell on 32 x 4 x 2 CTAs.
+// Per-cell stage kernels of the B200 ideal-MHD time step, sm_100a: one thread
+// per cell on 32 x 4 x 2 CTAs.  Variant 5 (the default): k_cell_flux_staged
+// then k_cell_epilogue; variant 4: k_cell_flux then k_cell_epilogue; variant
+// 2: k_cell_flux, k_cell_ct, k_cell_prim.
 //
 //  k_cell_flux  reconstruction + HLLD on the cell's lower x-, y- and z-face
 //               (calc_flux_kernel<X,Y,Z>, src/library/mhd_solver.inlrb:562-636);
 //               21 flux values per cell go to scratch.
+//  k_cell_flux_staged  the same fluxes from a shared-memory copy of the
+//               tile's stencil (cell_flux_staged.cuh).
 //  k_cell_ct    corner EMFs and the face-B update (:641-714), written into the
 //               output state.
 //  k_cell_prim  flux divergence (add_flux_kernel :689-693), conserved update
 //               (:762-835), primitive recovery (:779-795), the Kepler kick
 //               (:837-848), and in the final stage the CFL reduction and clock
 //               update (:496-521, 870-901, 981).
-//  k_cell_epilogue  (variant 4) k_cell_ct and k_cell_prim fused: one pass per
-//               tile with the corner EMFs and new face B in shared memory
+//  k_cell_epilogue  k_cell_ct and k_cell_prim fused: one pass per tile with
+//               the corner EMFs and new face B in shared memory
 //               (cell_epilogue.cuh).
 // The per-cell work lives in cell_ops.cuh, shared with the batch kernels.
 #include <cudaTypedefs.h>
