@@ -24,6 +24,7 @@
 #include <cstring>
 #include <map>
 #include <string>
+#include <utility>
 #include <vector>
 
 #include "../../include/nmhd.h"
@@ -70,8 +71,19 @@ struct MinBlocks<OpABface<float>> {
   static constexpr int value = NMHD_AD_GATHER_MIN_BLOCKS;
 };
 
+// Programmatic dependent launch: the executor launches each pass so that it
+// may be scheduled while the previous pass's last blocks still run; every
+// pass lets its own successor be scheduled at once, then waits until the
+// previous grid has completed and its memory is visible, before its first
+// global access.  (Both are no-ops for a launch without the attribute.)
+__device__ __forceinline__ void pdl_enter() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 template <class F, int kMinBlocks>
 __global__ void __launch_bounds__(BX *BY *BZ, kMinBlocks) k_ad_cells(F f, int sx, int sy, int sz) {
+  pdl_enter();
   const int x = blockIdx.x * BX + threadIdx.x;
   const int y = blockIdx.y * BY + threadIdx.y;
   const int z = blockIdx.z * BZ + threadIdx.z;
@@ -80,6 +92,7 @@ __global__ void __launch_bounds__(BX *BY *BZ, kMinBlocks) k_ad_cells(F f, int sx
 
 template <class F>
 __global__ void __launch_bounds__(256) k_ad_items(F f, int n) {
+  pdl_enter();
   const int i = blockIdx.x * 256 + threadIdx.x;
   if (i < n) f(i);
 }
@@ -90,6 +103,7 @@ template <class D, class F>
 __global__ void __launch_bounds__(256) k_ad_reduce(F f, int sx, int sy, int sz, D *partial) {
   __shared__ double raw[256 * sizeof(D) / sizeof(double)];
   D *sh = reinterpret_cast<D *>(raw);
+  pdl_enter();
   const int tid = threadIdx.x;
   const long long i = (long long)blockIdx.x * 256 + tid;
   const long long n = (long long)sx * sy * sz;
@@ -111,6 +125,7 @@ template <class D>
 __global__ void __launch_bounds__(256) k_ad_reduce_final(const D *partial, int nb, D *acc, double scale) {
   __shared__ double raw[256 * sizeof(D) / sizeof(double)];
   D *sh = reinterpret_cast<D *>(raw);
+  pdl_enter();
   const int tid = threadIdx.x;
   D v = to<D>(0.0);
   for (int i = tid; i < nb; i += 256) v = v + partial[i];
@@ -138,16 +153,32 @@ NMHD_HD void OpWiden<Dual<double>>::operator()(int i) const {
   dst[i] = dir ? Dual<double>((double)src[i] + shift * dir[i], dir[i]) : Dual<double>((double)src[i], 0.0);
 }
 
+// Launch with programmatic stream serialization (see pdl_enter).
+template <class... KArgs, class... Args>
+void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st, Args &&...args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = st;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...);
+}
+
 struct GpuExec {
   cudaStream_t st;
   template <class R, class F>
   void cells(const GGrid<R> &g, const F &f) {
     const dim3 grid((g.sx + BX - 1) / BX, (g.sy + BY - 1) / BY, (g.sz + BZ - 1) / BZ);
-    k_ad_cells<F, MinBlocks<F>::value><<<grid, dim3(BX, BY, BZ), 0, st>>>(f, g.sx, g.sy, g.sz);
+    launch_pdl(k_ad_cells<F, MinBlocks<F>::value>, grid, dim3(BX, BY, BZ), st, f, g.sx, g.sy, g.sz);
   }
   template <class F>
   void items(int n, const F &f) {
-    if (n > 0) k_ad_items<<<(n + 255) / 256, 256, 0, st>>>(f, n);
+    if (n > 0) launch_pdl(k_ad_items<F>, dim3((n + 255) / 256), dim3(256), st, f, n);
   }
   template <class T>
   void zero(T *p, size_t n) {
@@ -157,8 +188,8 @@ struct GpuExec {
   void reduce(const GGrid<R> &g, const F &f, D *partial, D *acc, double scale) {
     const long long n = (long long)g.sx * g.sy * g.sz;
     const int nb = (int)((n + 255) / 256);
-    k_ad_reduce<D, F><<<nb, 256, 0, st>>>(f, g.sx, g.sy, g.sz, partial);
-    k_ad_reduce_final<D><<<1, 256, 0, st>>>(partial, nb, acc, scale);
+    launch_pdl(k_ad_reduce<D, F>, dim3(nb), dim3(256), st, f, g.sx, g.sy, g.sz, partial);
+    launch_pdl(k_ad_reduce_final<D>, dim3(1), dim3(256), st, (const D *)partial, nb, acc, scale);
   }
 };
 
