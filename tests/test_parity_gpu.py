@@ -156,8 +156,8 @@ def _rel_by_quantity(a, b):
 def test_fast_arithmetic_within_tolerance(gpu, case):
     """NMHD_FLAG_FAST_ARITHMETIC on the noisy MRI boxes: one step from the
     reference's own state (the oracle's) is within 1e-5 of the reference's,
-    relative to each quantity's scale (the north star's per-step FP32
-    tolerance); after 20 steps mass is conserved and div B stays at roundoff.
+    relative to each quantity's scale (the per-step FP32 tolerance this mode
+    is held to); after 20 steps mass is conserved and div B stays at roundoff.
     (Not on flows with exact symmetries: there the reference's corner wind
     sums are exactly zero, CT takes the mean, and rounding-size differences
     in the predictor pick one side instead.)"""
