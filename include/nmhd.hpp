@@ -13,6 +13,7 @@
 #ifndef NMHD_HPP
 #define NMHD_HPP
 
+#include <array>
 #include <chrono>
 #include <cmath>
 #include <cstdio>
@@ -242,6 +243,26 @@ class MHDSolver {
   // Builds the CUDA graphs a later proceed(..., max_steps) launches, without
   // running them (nmhd_prepare).
   void prepare(long long max_steps = 0) { check(nmhd_prepare(s_, max_steps)); }
+  // Kernel selection (nmhd_set_kernel / nmhd_get_kernel; every variant gives
+  // bitwise the same results) and the autotuner, which times every variant on
+  // this box from the current state and keeps the fastest (nmhd_autotune):
+  // returns its rows (variant, tile_rows, z_chunk, ms per step).
+  void set_kernel(int variant, int tile_rows = 8, int z_chunk = 0) {
+    check(nmhd_set_kernel(s_, variant, tile_rows, z_chunk));
+  }
+  int kernel_variant() const {
+    int v = 0;
+    nmhd_get_kernel(s_, &v, nullptr, nullptr);
+    return v;
+  }
+  std::vector<std::array<double, 4>> autotune(int steps = 5) {
+    std::vector<double> rows(4 * 64);
+    const int k = nmhd_autotune(s_, steps, rows.data(), 64);
+    if (k < 0) throw Error((nmhd_status)k, nmhd_last_error(s_));
+    std::vector<std::array<double, 4>> out(k);
+    for (int i = 0; i < k; ++i) out[i] = {rows[4 * i], rows[4 * i + 1], rows[4 * i + 2], rows[4 * i + 3]};
+    return out;
+  }
   // The application's monitor() (e.g. src/application/kepler_disk_demo/
   // mhd_solver.curb:107-130); an empty function removes it.
   void set_monitor(std::function<int(MHDSolver &)> m) { monitor_ = std::move(m); }
@@ -361,6 +382,14 @@ class Batch {
     const int k = nmhd_batch_autotune(b_, reps, nullptr, 0);
     if (k < 0) throw Error((nmhd_status)k, nmhd_batch_last_error(b_));
   }
+  // One schedule pinned (nmhd_batch_set_schedule: kernel 0-2 the stage
+  // kernels, 3 the fused update pass, 4 the staged flux pass).
+  void set_schedule(int kernel, bool persistent, bool split) {
+    check(nmhd_batch_set_schedule(b_, kernel, persistent ? 1 : 0, split ? 1 : 0));
+  }
+  // Builds the CUDA graphs a later proceed(..., max_steps) launches
+  // (nmhd_batch_prepare).
+  void prepare(long long max_steps = 0) { check(nmhd_batch_prepare(b_, max_steps)); }
   long long last_steps() const { return last_steps_; }
   nmhd_batch *handle() { return b_; }
 

@@ -103,7 +103,8 @@ def test_cpp_mirror_compiles_and_links(tmp_path):
     src.write_text('#include "nmhd.hpp"\n'
                    'int main() { std::vector<nmhd_config> b(1); '
                    'if (b.size() == 7) { nmhd::Batch x(b); nmhd::MHDSolver y(b[0]); x.autotune(); y.proceed(1.f); '
-                   'x.initialize_states(x.states()); } '
+                   'x.initialize_states(x.states()); x.set_schedule(4, false, true); x.prepare(16); '
+                   'y.set_kernel(5); y.prepare(16); if (y.autotune(2).size() > 0 && y.kernel_variant() < 0) return 1; } '
                    'return 0; }\n')
     lib = os.path.join(root, "nmhd_b200")
     subprocess.run(["g++", "-std=c++17", "-Wall", "-Werror", "-I" + os.path.join(root, "include"), str(src),

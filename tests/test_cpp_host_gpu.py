@@ -28,6 +28,10 @@ int main(int argc, char **argv) {
   c.q = 1.5f; c.omega = 1.0f; c.space_order = 2; c.time_order = 2;
   const int stop = std::atoi(argv[3]);
   nmhd::MHDSolver solver(c);
+  if (argc > 4) {  // a kernel variant other than the default
+    solver.set_kernel(std::atoi(argv[4]));
+    if (solver.kernel_variant() != std::atoi(argv[4])) return 6;
+  }
   if (!solver.read(argv[1])) return 3;
   std::vector<int> seen;
   solver.set_monitor([&](nmhd::MHDSolver &s) {
@@ -44,7 +48,8 @@ int main(int argc, char **argv) {
 '''
 
 
-def test_cpp_host_program_matches_python_front_end(gpu, tmp_path):
+@pytest.mark.parametrize("variant", [None, 4, 2])
+def test_cpp_host_program_matches_python_front_end(gpu, tmp_path, variant):
     src = tmp_path / "app.cpp"
     src.write_text(SRC)
     exe = tmp_path / "app"
@@ -53,8 +58,8 @@ def test_cpp_host_program_matches_python_front_end(gpu, tmp_path):
                     "-lnmhd", "-Wl,-rpath," + lib, "-o", str(exe)], check=True)
     cfg, s = shearing_box(n_radial=16, n_azimuthal=32, n_vertical=8, l_azimuthal=4.0, seed=41)
     write_bin(str(tmp_path / "in.bin"), s)
-    r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "9"],
-                       capture_output=True, text=True)
+    r = subprocess.run([str(exe), str(tmp_path / "in.bin"), str(tmp_path / "out.bin"), "9"] +
+                       ([str(variant)] if variant is not None else []), capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     reached, gen, calls = (int(v) for v in r.stdout.split())
     assert (reached, gen, calls) == (0, 9, 10)
@@ -89,6 +94,12 @@ int main(int argc, char **argv) {
     batch.initialize_state(i, s);
   }
   batch.autotune(2);
+  if (argc > 3) {  // the staged flux and fused update passes pinned, graphs built first
+    batch.set_schedule(0, false, true);
+    batch.set_schedule(4, false, true);
+    batch.set_schedule(3, true, true);
+    batch.prepare(7);
+  }
   const bool reached = batch.proceed(1e30f, 7);
   const std::vector<std::vector<float>> all = batch.states();
   for (int i = 0; i < 2; ++i) {
@@ -104,9 +115,11 @@ int main(int argc, char **argv) {
 '''
 
 
-def test_cpp_batch_program_matches_single_box_runs(gpu, tmp_path):
+@pytest.mark.parametrize("pinned", [False, True])
+def test_cpp_batch_program_matches_single_box_runs(gpu, tmp_path, pinned):
     """nmhd::Batch (include/nmhd.hpp) advances two boxes of different shapes
-    bitwise as the single-box solver does."""
+    bitwise as the single-box solver does (autotuned schedules, or the staged
+    and fused passes pinned with the graphs prepared first)."""
     src = tmp_path / "batch.cpp"
     src.write_text(BATCH_SRC)
     exe = tmp_path / "batch"
@@ -118,7 +131,8 @@ def test_cpp_batch_program_matches_single_box_runs(gpu, tmp_path):
     paths = [tmp_path / f"box{i}.raw" for i in range(2)]
     for (cfg, s), p in zip(cases, paths):
         np.ascontiguousarray(s, dtype=np.float32).tofile(p)
-    r = subprocess.run([str(exe)] + [str(p) for p in paths], capture_output=True, text=True)
+    r = subprocess.run([str(exe)] + [str(p) for p in paths] + (["pinned"] if pinned else []),
+                       capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
     assert r.stdout.split() == ["0", "7", "7", "7"]
     for (cfg, s), p in zip(cases, paths):
