@@ -224,9 +224,10 @@ const char *nmhd_kernel_name(int i);
  *   time, generation  in: the clock of state_in; out: the clock of the result
  * Boxes larger than NMHD_NOALLOC_MAX_CELLS are rejected with
  * NMHD_ERR_INVALID_ARGUMENT.  Calls no cudaMalloc/cudaFree.  The first call on
- * a device looks up the array's device address (set-up).  All calls share the
- * array and it keeps the
- * last call's contents: calls that overlap on the GPU race.  Runs on
+ * a device does the set-up: it looks up the array's device address with that
+ * device current; make that first call before any stream capture.  All calls
+ * share the array and it keeps the last call's contents: calls that overlap on
+ * the GPU race.  Runs on
  * `cuda_stream` (NULL: the default stream), reads the control block back
  * every 16 steps (stopping once the goal is reached or the state is bad) and
  * returns when done.  A CUDA error pending from earlier work is reported as

@@ -11,7 +11,9 @@
 // loads the library holds it (kNoAllocScratchFloats floats, about 28 MB)
 // until the process exits.  All calls share it and it keeps the last call's
 // contents, so calls that overlap on the GPU race; the control block at its
-// start is rewritten by every call.
+// start is rewritten by every call.  The first call on a device does the
+// set-up (the array's device address, looked up with that device current);
+// it should come before any stream capture.
 #include <cuda_runtime.h>
 
 #include <atomic>
