@@ -24,8 +24,8 @@ def build():
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            build()
+        # make rebuilds the library when a product header it compiles changed
+        build()
         L = ctypes.CDLL(LIB)
         f32, f64, P = ctypes.c_float, ctypes.c_double, ctypes.c_void_p
         L.adh_hlld_f32.argtypes = [f32, f32, P, P]

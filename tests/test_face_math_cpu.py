@@ -29,8 +29,8 @@ _lib = None
 def lib():
     global _lib
     if _lib is None:
-        if not os.path.exists(LIB):
-            subprocess.run(["make", "-s", "-C", os.path.join(HERE, "native")], check=True)
+        # make rebuilds the library when mhd_math.cuh changed
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "native")], check=True)
         L = ctypes.CDLL(LIB)
         P = ctypes.c_void_p
         L.cellh_hlld_many_f32.argtypes = [ctypes.c_float, P, P, P, ctypes.c_long]
