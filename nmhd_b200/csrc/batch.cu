@@ -215,7 +215,10 @@ __global__ void __launch_bounds__(kThreads, NMHD_BATCH_MIN_BLOCKS_EPI)
     if (final_stage) finish_tile(ctl, (unsigned)(d.tiles_x * d.tiles_y * d.tiles_z), tcfl, bad, d.dt_hist, s.red);
   };
   if (!kPersist) {
-    const int t = tb + blockIdx.x;
+    // tiles in the reverse of the flux pass's order (grid = te - tb CTAs,
+    // dispatched in block order): the first tiles read the fluxes written
+    // last, which are still in L2
+    const int t = te - 1 - (int)blockIdx.x;
     const BoxDesc &d = p.box[group_box(p, t)];
     if (d.ctl->done) return;
     tile(d, t);

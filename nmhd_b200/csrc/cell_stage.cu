@@ -139,9 +139,13 @@ __global__ void __launch_bounds__(kThreads, NMHD_EPI_MIN_BLOCKS)
   const float *win = pick(ctl, in_sel, w0, w1, wp), *wb = pick(ctl, 0, w0, w1, wp);
   float *wo = const_cast<float *>(pick(ctl, out_sel, w0, w1, wp));
   int bad = 0, timed_out = 0;
+  // tiles in the reverse of the flux kernel's order: CTAs are dispatched in
+  // block order, so the first tiles read the fluxes written last, which are
+  // still in L2
+  const int tx = gridDim.x - 1 - blockIdx.x, ty = gridDim.y - 1 - blockIdx.y, tz = gridDim.z - 1 - blockIdx.z;
   const float tcfl = epi::tile_epilogue<kPow2>(s, g, &maps, pick_index(ctl, in_sel), pick_index(ctl, 0), win, wb, wo,
-                                               flux, blockIdx.x * BX, blockIdx.y * BY, blockIdx.z * BZ, dt,
-                                               final_stage != 0, &bad, &timed_out);
+                                               flux, tx * BX, ty * BY, tz * BZ, dt, final_stage != 0, &bad,
+                                               &timed_out);
   if (timed_out && threadIdx.x == 0 && threadIdx.y == 0 && threadIdx.z == 0)
     atomicOr(&ctl->status, kStatusTimeout);
   if (final_stage) finish_tile(ctl, ntiles, tcfl, bad, dt_hist, s.red);
