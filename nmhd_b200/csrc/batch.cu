@@ -3,12 +3,17 @@
 // No counterpart in the reference (one box per process, sizes fixed at compile
 // time).  Every box keeps its own configuration, state buffers, control block
 // (clock, CFL minimum, status) and therefore its own time step from its own CFL
-// reduction.  Each kernel of a step is ONE persistent launch over all boxes: a
-// CTA walks a flattened list of 32 x 4 x 2-cell tiles, finds the tile's box in
-// a descriptor table and runs the same per-cell code as the single-box path
-// (cell_ops.cuh, margin_ops.cuh), so every box is bitwise the box advanced
-// alone.  A step is 8 launches whatever the number of boxes, and batches of
-// steps are one CUDA graph.
+// reduction.  Each stage kernel of a step is launched over all boxes of a
+// launch group (up to 128 boxes, their descriptors in the kernel parameter
+// block): a CTA takes a tile of the flattened tile list (or, in the persistent
+// schedule, a contiguous range of tiles), finds the tile's box and runs the
+// same per-cell code as the single-box path (cell_ops.cuh, margin_ops.cuh,
+// cell_flux_staged.cuh, cell_epilogue.cuh), so every box is bitwise the box
+// advanced alone.  Each box has its own tile shape; the boxes with the
+// single-box kernels' 32 x 4 x 2 tile can run in launches of their own
+// (split), through the staged flux and fused update passes.  The launches of
+// a step depend on the schedules, not on the number of boxes in a group
+// (nmhd_batch_launches_per_step), and batches of steps are one CUDA graph.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -442,19 +447,21 @@ void launch_kind(nmhd_batch *b, int kind, int in_sel, int out_sel, int half, int
   const dim3 blk(nmhd::cell::kThreads);
   for (const BatchGroup &p : b->groups) {
     if (kind == 0 && staged(b)) {
+      // the other boxes first: the staged pass's fluxes, written last, are
+      // the ones the fused pass reads first
       const int tb = p.fixed_tiles, te = p.total_tiles;
-      if (tb > 0) {
-        if (b->persist_sflux)
-          nmhd::k_batch_flux_staged<true><<<std::min(b->ctas[4], tb), blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
-        else
-          nmhd::k_batch_flux_staged<false><<<tb, blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
-      }
       if (te > tb) {
         if (b->persist[0])
           nmhd::k_batch_stage<0, true, false><<<std::min(b->ctas[0], te - tb), blk, 0, b->stream>>>(
               p, tb, te, in_sel, out_sel, half, fin);
         else
           nmhd::k_batch_stage<0, false, false><<<te - tb, blk, 0, b->stream>>>(p, tb, te, in_sel, out_sel, half, fin);
+      }
+      if (tb > 0) {
+        if (b->persist_sflux)
+          nmhd::k_batch_flux_staged<true><<<std::min(b->ctas[4], tb), blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
+        else
+          nmhd::k_batch_flux_staged<false><<<tb, blk, 0, b->stream>>>(p, 0, tb, in_sel, half);
       }
     } else if (kind == 0) {
       launch_stage<0>(p, b->persist[0], b->split[0], b->ctas[0], b->stream, in_sel, out_sel, half, fin);
